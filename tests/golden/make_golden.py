@@ -1,0 +1,112 @@
+"""Generate the golden fixtures under tests/golden/ from the reference's own source text.
+
+The reference (Fortran 90 + PETSc) cannot be compiled or run here, so the only numeric
+ground truth it ships is tabulated in its source files.  This script parses those tables
+and evaluates them, writing small .npy/.json fixtures that the CPU test-suite compares the
+oracle (and the library's host code) against.  It is run once in a container that has the
+reference checkout; the fixtures are committed so nothing at test time reads the reference.
+
+Fixtures written:
+  ke08_table_nu{NU}.npy   mod_linfe.f90:161-776  Hexe08 C_FE(24,24) table before `* factor`
+                          (factor = E*a/(144*(2nu^2+nu-1)), mod_linfe.f90:182)
+  ke20_table_nu{NU}.npy   mod_linfe.f90:890-4509 Hexe20 C_FE(60,60) table before `* factor`
+                          (factor = E*a*2nu/(256*(2nu^2+nu-1)*2nu), mod_linfe.f90:904)
+  uu_hexe8_eps1e-6.npy    mod_write_deck.f90:63-116 init_displ_hexe8, uu(8,3,24)
+  vv_lin_eps1e-6.npy      mod_struct_calcmat.f90:1684-1770 init_loadcase_el_order_lin, vv(24,24)
+  golden_meta.json        the source line ranges and the evaluation parameters
+
+Usage:  python tests/golden/make_golden.py [/path/to/reference]
+"""
+import json
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+OUT = Path(__file__).resolve().parent
+
+
+def _fortran_expr(expr: str) -> str:
+    expr = expr.replace("_rk", "").replace("_8", "")
+    expr = re.sub(r"(\d)\.(?!\d)", r"\1.0", expr)  # "0." -> "0.0"
+    expr = expr.replace("**", "^^").replace("^^", "**")
+    return expr
+
+
+def ke_table(lines, lo, hi, n, nu):
+    K = np.full((n, n), np.nan)
+    pat = re.compile(r"^\s*C_FE\((\d+),(\d+)\)\s*=\s*(.+?)\s*$")
+    for ln in lines[lo - 1:hi]:
+        m = pat.match(ln)
+        if m:
+            K[int(m.group(1)) - 1, int(m.group(2)) - 1] = eval(_fortran_expr(m.group(3)), {"nu": nu})
+    assert np.isfinite(K).all(), "table not completely filled"
+    return K
+
+
+def joined_statements(lines, lo, hi):
+    """Join Fortran free-form continuation lines ('&' at end) into statements."""
+    out, cur = [], ""
+    for ln in lines[lo - 1:hi]:
+        s = ln.split("!")[0].rstrip()
+        if s.endswith("&"):
+            cur += s[:-1] + " "
+            continue
+        s = s.lstrip()
+        if s.startswith("&"):
+            s = s[1:]
+        cur += s
+        out.append(cur)
+        cur = ""
+    return out
+
+
+def uu_hexe8(lines, eps):
+    uu = np.zeros((8, 3, 24))
+    pat = re.compile(r"uu\(:,\s*(\d+),\s*(\d+)\)\s*=\s*\[(.*)\]")
+    for st in joined_statements(lines, 63, 116):
+        m = pat.search(st)
+        if m:
+            vals = [eval(_fortran_expr(v.strip()), {"eps": eps}) for v in m.group(3).split(",")]
+            assert len(vals) == 8
+            uu[:, int(m.group(1)) - 1, int(m.group(2)) - 1] = vals
+    return uu
+
+
+def vv_lin(lines, eps):
+    vv = np.zeros((24, 24))
+    pat = re.compile(r"vv\(\s*(\d+),:\)\s*=\s*\[(.*)\]")
+    env = {"eps": eps, "eps2": 2 * eps, "eps3": 3 * eps, "eps4": 4 * eps}
+    n = 0
+    for st in joined_statements(lines, 1684, 1770):
+        m = pat.search(st)
+        if m:
+            vals = [eval(_fortran_expr(v.strip()), env) for v in m.group(2).split(",")]
+            assert len(vals) == 24
+            vv[int(m.group(1)) - 1, :] = vals
+            n += 1
+    assert n == 24
+    return vv
+
+
+def main():
+    linfe = (REF / "f-src/mod_linfe.f90").read_text().splitlines()
+    deck = (REF / "f-src/mod_write_deck.f90").read_text().splitlines()
+    calc = (REF / "f-src/mod_struct_calcmat.f90").read_text().splitlines()
+    meta = {"reference_files": {
+        "ke08": "f-src/mod_linfe.f90:161-776", "ke20": "f-src/mod_linfe.f90:890-4509",
+        "uu": "f-src/mod_write_deck.f90:63-116", "vv": "f-src/mod_struct_calcmat.f90:1684-1770"},
+        "nu": [0.3, 0.25], "eps": 1e-6}
+    for nu in meta["nu"]:
+        np.save(OUT / f"ke08_table_nu{nu}.npy", ke_table(linfe, 161, 776, 24, nu))
+        np.save(OUT / f"ke20_table_nu{nu}.npy", ke_table(linfe, 890, 4509, 60, nu))
+    np.save(OUT / "uu_hexe8_eps1e-6.npy", uu_hexe8(deck, 1e-6))
+    np.save(OUT / "vv_lin_eps1e-6.npy", vv_lin(calc, 1e-6))
+    (OUT / "golden_meta.json").write_text(json.dumps(meta, indent=1) + "\n")
+    print("fixtures written to", OUT)
+
+
+if __name__ == "__main__":
+    main()
