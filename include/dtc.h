@@ -1,0 +1,180 @@
+/*
+ * dtc.h -- C ABI of the B200 direct-tensor-computation solver.
+ *
+ * Drop-in for the per-domain solve of the reference's exec_single_domain
+ * (f-src/mod_dtc_main_subroutines.f90:52-1337): the block from MatCreate (:426) to
+ * calc_effective_material_parameters (:1257), together with the meshing and boundary
+ * generation it calls (f-src/mod_struct_preprocess.f90:23-738,
+ * f-src/mod_gen_quadmesh.f90:22-679, f-src/mod_write_deck.f90:22-279) and the
+ * homogenisation + rotation search (f-src/mod_struct_calcmat.f90:23-1673).
+ * The MPI domain loop of the driver (f-src_main/struct_process.f90:960-1070,1240-1395)
+ * becomes one call with many domains.
+ *
+ * Plain C types only: int64_t / double / pointers.  All arrays are caller-owned host
+ * memory.  Matrices are column-major with the reference's Fortran layout (entry (i,j),
+ * 1-based, at [(i-1) + n*(j-1)]), i.e. exactly the order of the reference's result leaves
+ * (reshape(ff,[no_lc*no_lc]) etc., f-src/mod_struct_calcmat.f90:289-1664).
+ * Functions return dtc_status; per-domain outcomes are in dtc_domain_out.status.
+ * Nothing aborts the process and no device code traps.
+ *
+ * Threading: a handle is used by one host thread at a time; distinct handles are
+ * independent.  The library owns all device memory it allocates inside a handle.
+ */
+#ifndef DTC_H
+#define DTC_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTC_ABI_VERSION 1
+
+typedef enum dtc_status {
+  DTC_OK = 0,
+  DTC_ERR_INVALID_ARGUMENT = 1, /* a pointer, size or parameter failed validation */
+  DTC_ERR_CUDA = 2,             /* a CUDA runtime call failed; see dtc_last_error */
+  DTC_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed */
+  DTC_ERR_NO_DEVICE = 4,        /* no usable CUDA device */
+  DTC_ERR_ABI_MISMATCH = 5,     /* dtc_options.abi_version != DTC_ABI_VERSION */
+  DTC_ERR_INTERNAL = 6
+} dtc_status;
+
+/* Per-domain status, same meaning as the reference's skip paths. */
+enum {
+  DTC_DOMAIN_OK = 0,
+  DTC_DOMAIN_EMPTY = 1,        /* max(phi) < llimit: no mesh (mod_gen_quadmesh.f90:142-164) */
+  DTC_DOMAIN_NO_STRUCTURE = 2, /* no nodes or elements (mod_struct_preprocess.f90:358-361) */
+  DTC_DOMAIN_FEW_NODES = 3,    /* the "< 6" test on the node-count leaf (mod_struct_preprocess.f90:471-473) */
+  DTC_DOMAIN_MAX_IT = 4,       /* a load case reached max_it (KSP_DIVERGED_ITS) */
+  DTC_DOMAIN_BREAKDOWN = 5,    /* p'Ap <= 0 or an indefinite preconditioner in CG */
+  DTC_DOMAIN_NONFINITE = 6     /* NaN/Inf residual or divergence (KSP_DIVERGED_NANORINF/DTOL) */
+};
+
+enum { DTC_HEX08 = 8, DTC_HEX20 = 20 };
+
+enum {
+  DTC_PREC_FP64 = 0,  /* plain FP64 Jacobi-PCG, PETSc KSPCG semantics per load case */
+  DTC_PREC_MIXED = 1  /* FP32 Jacobi-PCG inner solves inside FP64 iterative refinement */
+};
+
+typedef struct dtc_options {
+  int32_t abi_version;     /* must be DTC_ABI_VERSION */
+  int32_t precision;       /* DTC_PREC_* */
+  double rtol;             /* relative tolerance on ||D^-1 r|| / ||D^-1 b|| per load case;
+                              the reference's PETSc option -ksp_rtol (f-src/mod_parameters.f90:31) */
+  int64_t max_it;          /* CG iteration cap per load case (-ksp_max_it, :32); for the mixed
+                              path the cap on the summed inner iterations */
+  double inner_rtol;       /* mixed path: reduction asked of each FP32 inner solve (0 -> 1e-5) */
+  int32_t max_refine;      /* mixed path: cap on FP64 refinement steps (0 -> 12) */
+  int32_t rotation_search; /* 1: run the CR1/CR2 rotation search (mod_struct_calcmat.f90:533-1603) */
+  int32_t device;          /* CUDA device ordinal */
+  int32_t host_threads;    /* threads for host-side meshing (0 -> hardware concurrency) */
+  int32_t keep_displacements; /* 1: keep the converged displacements on the device for
+                                 dtc_energy_grad (the adjoint); 0: release them */
+  int32_t reserved[8];
+} dtc_options;
+
+typedef struct dtc_domain_in {
+  int64_t L[3];            /* x_D: voxels per domain edge (mod_decomp.f90:290) */
+  int64_t xa_n[3];         /* 1-based first voxel of the domain in the volume
+                              (mod_struct_preprocess.f90:89-91) */
+  int64_t domain_number;   /* copied to the output record */
+  int32_t elem_type;       /* DTC_HEX08 or DTC_HEX20 (MICRO_ELMNT_TYPE) */
+  int32_t phi_type;        /* bytes per gray value: 1, 2 or 4 (TYPE_RAW ik1/ik2/ik4) */
+  const void* phi;         /* L0*L1*L2 signed gray values, x fastest */
+  int64_t llimit;          /* BINARIZE_LO: voxel is bone iff phi >= llimit (mod_gen_quadmesh.f90:296) */
+  const float* E_voxel;    /* optional per-voxel Young's modulus (MPa), L0*L1*L2, x fastest.
+                              NULL: every element uses E, which is the reference behaviour */
+  double delta[3];         /* SPACING: voxel edge (mm); must be equal in x, y, z */
+  double phdsize[3];       /* SIZE_DOMAIN (mm); the element scale is a = phdsize(1)*delta(1) */
+  double E;                /* YOUNG_MODULUS (MPa) */
+  double nu;               /* POISSON_RATIO; all domains of one call share it */
+  double rve_strain;       /* RVE_STRAIN: eps of the load-case matrix vv */
+} dtc_domain_in;
+
+typedef struct dtc_domain_out {
+  int32_t status;          /* DTC_DOMAIN_* */
+  int32_t refine_steps;    /* mixed path: FP64 refinement steps taken */
+  int64_t domain_number;
+  int64_t ne, nn, nb;      /* elements, nodes, constrained nodes of the reference mesh */
+  int64_t n_free_dof;      /* unconstrained DOFs the solver iterates on */
+  int64_t iters[24];       /* CG iterations per load case (summed inner iterations for mixed) */
+  double relres[24];       /* final ||D^-1 r|| / ||D^-1 b|| evaluated in FP64 */
+  double ff[576];          /* "Domain forces" ff(24,24) */
+  double kmacro[576];      /* "Effective numerical stiffness" ff * vv^-1 */
+  double sym_k;            /* symmetry deviation max|A-A^T|/max|A| of kmacro */
+  double c[36];            /* "Effective stiffness" fv * meps */
+  double sym_c;
+  double ee[36];           /* "Averaged Effective stiffness" (C + C^T)/2 */
+  double sym_ee;
+  double cr1_angle, cr1_n[3], cr1_aa[9], cr1_ee[36], cr1_crit;  /* CR1 (monotropic) */
+  double cr2_angle, cr2_n[3], cr2_aa[9], cr2_ee[36], cr2_crit;  /* CR2 (orthotropic) */
+  int32_t cr1_iters, cr2_iters;  /* refinement iterations jj */
+  double density;          /* ne / (L0*L1*L2) (mod_struct_calcmat.f90:1642-1651) */
+  double* displ;           /* optional (NULL to skip): 24 x 3nn displacements incl. boundary
+                              values, load-case major, reference DOF numbering 3*(node-1)+comp */
+  double* force;           /* optional: 24 x 3nn reaction forces AA_org*u, same layout */
+} dtc_domain_out;
+
+typedef struct dtc_mesh_out {
+  int64_t ne, nn, nb;      /* filled always */
+  int32_t status;          /* DTC_DOMAIN_OK / EMPTY / NO_STRUCTURE / FEW_NODES */
+  int32_t last_elem_partial; /* 1 when the mesher kept its last element although its region
+                                was dropped (mod_gen_quadmesh.f90:598-613) */
+  int64_t cap_elems, cap_nodes; /* capacities of the arrays below */
+  int64_t* elems;          /* optional: elem_type*ne node ids, 1-based, 0 = dropped node */
+  double* nodes;           /* optional: 3*nn coordinates */
+  int64_t* bnode_ids;      /* optional: nb constrained node ids in node order */
+  double* bnode_vals;      /* optional: 24 x 3nb prescribed displacements, column-major */
+} dtc_mesh_out;
+
+typedef struct dtc_handle dtc_handle;
+
+/* Version of this header the library was built with. */
+int32_t dtc_abi_version(void);
+
+/* Fill *opt with defaults: FP64, rtol 1e-3 and max_it 500000 (the reference's PETSc
+ * options, f-src/mod_parameters.f90:23-32), rotation search on. */
+void dtc_default_options(dtc_options* opt);
+
+/* Create a solver bound to one CUDA device.  Replaces the per-domain
+ * PetscInitialize/KSPCreate set-up of mod_dtc_main_subroutines.f90:144-148,995-1023. */
+dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt);
+
+/* Release every device and host resource of the handle (PetscFinalize, :1220-1238). */
+dtc_status dtc_destroy(dtc_handle* handle);
+
+/* Mesh, solve and homogenise n domains.  Replaces, per domain, exec_single_domain's
+ * generate_geometry (:247) + assembly (:516-579) + RHS/BC (:674-951) + 24 KSPSolve
+ * (:1072-1078) + reactions (:1092-1123) + calc_effective_material_parameters (:1257).
+ * in[i] and out[i] are caller-owned; out[i].displ/force may be NULL. */
+dtc_status dtc_solve_batch(dtc_handle* handle, const dtc_domain_in* in, int64_t n,
+                           dtc_domain_out* out);
+
+/* Host-only: the reference mesh and boundary conditions of one domain (element order,
+ * node numbering and constrained-node list bit-identical to gen_quadmesh_from_phi and
+ * generate_boundaries).  Needs no device. */
+dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out);
+
+/* Adjoint of the last dtc_solve_batch on this handle (which must have run with
+ * keep_displacements = 1 and E_voxel given): for each domain i, dL/dE_voxel given
+ * dL/dC = dloss_dc[36*i .. 36*i+35] (column-major 6x6, C = out.c).  Writes
+ * L0*L1*L2 floats per domain into grad_e[i] (caller-owned).  No reference counterpart:
+ * the reference has no gradient; this is the element-energy contraction
+ * dff(r,lc)/dE_e = sum_a vv^-1(a,r) u_a,e^T (Ke/E) u_lc,e at the converged solution. */
+dtc_status dtc_energy_grad(dtc_handle* handle, const double* dloss_dc, float* const* grad_e,
+                           int64_t n);
+
+/* Timing and work counters of the last dtc_solve_batch: device solve wall time (ms),
+ * kernels launched, and sum over domains of free DOFs x load cases x CG iterations. */
+dtc_status dtc_get_stats(const dtc_handle* handle, double* ms_solve, int64_t* kernel_launches,
+                         double* dof_iterations);
+
+/* Message describing the last error on this handle (never NULL). */
+const char* dtc_last_error(const dtc_handle* handle);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DTC_H */

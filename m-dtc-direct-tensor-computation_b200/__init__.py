@@ -1,0 +1,185 @@
+"""B200-native direct tensor computation: per-domain homogenisation of voxel bone domains.
+
+Python mirror of the C ABI in include/dtc.h.  One call meshes, solves the 24 macro load
+cases and homogenises many domains at once on one GPU, the way the reference's MPI driver
+calls exec_single_domain per domain (f-src_main/struct_process.f90:1293).
+
+    import dtc_b200 as dtc
+    solver = dtc.Solver(precision="mixed", rtol=1e-8)
+    results = solver.solve([dtc.Domain(phi) for phi in volumes])
+    results[0]["c"]          # 6x6 effective stiffness (MPa)
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi, synth
+from .capi import (DOMAIN_BREAKDOWN, DOMAIN_EMPTY, DOMAIN_FEW_NODES, DOMAIN_MAX_IT, DOMAIN_NO_STRUCTURE,
+                   DOMAIN_NONFINITE, DOMAIN_OK, HEX08, HEX20, PREC_FP64, PREC_MIXED, DTCError)
+
+__all__ = ["Domain", "Solver", "mesh_domain", "solve_batch", "DTCError", "HEX08", "HEX20",
+           "DOMAIN_OK", "DOMAIN_EMPTY", "DOMAIN_NO_STRUCTURE", "DOMAIN_FEW_NODES", "DOMAIN_MAX_IT",
+           "DOMAIN_BREAKDOWN", "DOMAIN_NONFINITE"]
+
+
+class Domain:
+    """One control volume: gray values phi[z, y, x] plus the meta parameters the reference
+    reads for it (BINARIZE_LO, SPACING, SIZE_DOMAIN, YOUNG_MODULUS, POISSON_RATIO, RVE_STRAIN,
+    MICRO_ELMNT_TYPE) and its position xa_n in the volume."""
+
+    def __init__(self, phi, *, llimit=1, elem_type=HEX08, delta=0.05, phdsize=None, E=5600.0, nu=0.3,
+                 rve_strain=1e-6, xa_n=(2, 2, 2), E_voxel=None, domain_number=0):
+        phi = np.asarray(phi)
+        if phi.ndim != 3:
+            raise ValueError("phi must be a 3-D array indexed [z, y, x]")
+        if phi.dtype == np.uint16:
+            if phi.size and phi.max() > 32767:
+                raise ValueError("uint16 gray values above 32767 do not fit the reference's signed ik2")
+            phi = phi.astype(np.int16)
+        if phi.dtype not in (np.int8, np.int16, np.int32):
+            phi = phi.astype(np.int32)
+        self.phi = np.ascontiguousarray(phi)
+        self.L = (phi.shape[2], phi.shape[1], phi.shape[0])
+        self.E_voxel = None if E_voxel is None else np.ascontiguousarray(E_voxel, dtype=np.float32)
+        if self.E_voxel is not None and self.E_voxel.shape != phi.shape:
+            raise ValueError("E_voxel must have the shape of phi")
+        d = (float(delta),) * 3 if np.isscalar(delta) else tuple(map(float, delta))
+        if phdsize is None:
+            ph = tuple(self.L[i] * d[i] for i in range(3))
+        else:
+            ph = (float(phdsize),) * 3 if np.isscalar(phdsize) else tuple(map(float, phdsize))
+        self.struct = capi.DomainIn()
+        s = self.struct
+        s.L[:] = self.L
+        s.xa_n[:] = xa_n
+        s.domain_number = domain_number
+        s.elem_type = elem_type
+        s.phi_type = self.phi.dtype.itemsize
+        s.phi = self.phi.ctypes.data
+        s.llimit = llimit
+        s.E_voxel = (self.E_voxel.ctypes.data_as(C.POINTER(C.c_float)) if self.E_voxel is not None
+                     else C.POINTER(C.c_float)())
+        s.delta[:] = d
+        s.phdsize[:] = ph
+        s.E, s.nu, s.rve_strain = float(E), float(nu), float(rve_strain)
+        self.elem_type = elem_type
+
+
+def _result(o, fields):
+    r = {
+        "status": o.status, "refine_steps": o.refine_steps, "domain_number": o.domain_number,
+        "ne": o.ne, "nn": o.nn, "nb": o.nb, "n_free_dof": o.n_free_dof,
+        "iters": np.array(o.iters[:]), "relres": np.array(o.relres[:]),
+        "ff": np.array(o.ff[:]).reshape(24, 24, order="F"),
+        "kmacro": np.array(o.kmacro[:]).reshape(24, 24, order="F"), "sym_k": o.sym_k,
+        "c": np.array(o.c[:]).reshape(6, 6, order="F"), "sym_c": o.sym_c,
+        "ee": np.array(o.ee[:]).reshape(6, 6, order="F"), "sym_ee": o.sym_ee,
+        "density": o.density,
+    }
+    for k in ("cr1", "cr2"):
+        r[k] = {"angle": getattr(o, k + "_angle"), "n": np.array(getattr(o, k + "_n")[:]),
+                "aa": np.array(getattr(o, k + "_aa")[:]).reshape(3, 3, order="F"),
+                "ee": np.array(getattr(o, k + "_ee")[:]).reshape(6, 6, order="F"),
+                "crit": getattr(o, k + "_crit"), "iters": getattr(o, k + "_iters")}
+    if fields is not None:
+        nn = o.nn
+        r["displ"] = fields[0][: 24 * 3 * nn].reshape(24, 3 * nn)
+        r["force"] = fields[1][: 24 * 3 * nn].reshape(24, 3 * nn)
+    return r
+
+
+class Solver:
+    """A handle on one GPU (dtc_create / dtc_destroy)."""
+
+    def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=1e-5, max_refine=12,
+                 rotation_search=True, device=0, host_threads=0, keep_displacements=False):
+        self.lib = capi.load()
+        o = capi.Options()
+        self.lib.dtc_default_options(C.byref(o))
+        o.precision = {"fp64": PREC_FP64, "mixed": PREC_MIXED}[precision]
+        o.rtol, o.max_it, o.inner_rtol, o.max_refine = float(rtol), int(max_it), float(inner_rtol), int(max_refine)
+        o.rotation_search, o.device, o.host_threads = int(bool(rotation_search)), int(device), int(host_threads)
+        o.keep_displacements = int(bool(keep_displacements))
+        self.options = o
+        h = C.c_void_p()
+        rc = self.lib.dtc_create(C.byref(h), C.byref(o))
+        if rc != capi.DTC_OK:
+            raise DTCError(rc, "dtc_create failed")
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.dtc_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != capi.DTC_OK:
+            raise DTCError(rc, (self.lib.dtc_last_error(self.handle) or b"").decode())
+
+    def solve(self, domains, want_fields=False):
+        n = len(domains)
+        ins = (capi.DomainIn * n)(*[d.struct for d in domains])
+        outs = (capi.DomainOut * n)()
+        keep = []
+        if want_fields:
+            for i, d in enumerate(domains):
+                cap = 24 * 3 * (d.L[0] + 1) * (d.L[1] + 1) * (d.L[2] + 1)
+                fd, ff_ = np.zeros(cap), np.zeros(cap)
+                keep.append((fd, ff_))
+                outs[i].displ = fd.ctypes.data_as(C.POINTER(C.c_double))
+                outs[i].force = ff_.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.dtc_solve_batch(self.handle, ins, n, outs))
+        return [_result(outs[i], keep[i] if want_fields else None) for i in range(n)]
+
+    def stats(self):
+        ms, launches, dofit = C.c_double(), C.c_int64(), C.c_double()
+        self._check(self.lib.dtc_get_stats(self.handle, C.byref(ms), C.byref(launches), C.byref(dofit)))
+        return {"ms_solve": ms.value, "kernel_launches": launches.value, "dof_iterations": dofit.value}
+
+    def energy_grad(self, dloss_dc, grads):
+        """dL/dE_voxel of the last solve; grads: list of float32 arrays shaped like phi."""
+        dl = np.ascontiguousarray(np.asarray(dloss_dc, dtype=np.float64).reshape(-1, 6, 6).transpose(0, 2, 1))
+        n = dl.shape[0]
+        ptrs = (C.POINTER(C.c_float) * n)(*[g.ctypes.data_as(C.POINTER(C.c_float)) for g in grads])
+        self._check(self.lib.dtc_energy_grad(self.handle, dl.ctypes.data_as(C.POINTER(C.c_double)), ptrs, n))
+
+
+def solve_batch(domains, want_fields=False, **options):
+    with Solver(**options) as s:
+        return s.solve(domains, want_fields=want_fields)
+
+
+def mesh_domain(domain):
+    """Reference mesh + boundary conditions of one domain (host only, no GPU needed)."""
+    lib = capi.load()
+    L = domain.L
+    nen = domain.elem_type
+    m = 1 if nen == HEX08 else 2
+    max_nodes = (m * L[0] + 1) * (m * L[1] + 1) * (m * L[2] + 1)
+    max_elems = L[0] * L[1] * L[2]
+    elems = np.zeros(nen * max_elems, np.int64)
+    nodes = np.zeros(3 * max_nodes)
+    bids = np.zeros(max_nodes, np.int64)
+    bvals = np.zeros(24 * 3 * max_nodes)
+    o = capi.MeshOut()
+    o.cap_elems, o.cap_nodes = max_elems, max_nodes
+    o.elems = elems.ctypes.data_as(C.POINTER(C.c_int64))
+    o.nodes = nodes.ctypes.data_as(C.POINTER(C.c_double))
+    o.bnode_ids = bids.ctypes.data_as(C.POINTER(C.c_int64))
+    o.bnode_vals = bvals.ctypes.data_as(C.POINTER(C.c_double))
+    rc = lib.dtc_mesh_domain(C.byref(domain.struct), C.byref(o))
+    if rc != capi.DTC_OK:
+        raise DTCError(rc, "dtc_mesh_domain failed")
+    ne, nn, nb = o.ne, o.nn, o.nb
+    return {"status": o.status, "ne": ne, "nn": nn, "nb": nb, "last_elem_partial": bool(o.last_elem_partial),
+            "elems": elems[: nen * ne].reshape(ne, nen), "nodes": nodes[: 3 * nn].reshape(nn, 3),
+            "bnode_ids": bids[:nb], "bnode_vals": bvals[: 24 * 3 * nb].reshape(24, 3 * nb, order="F")}

@@ -1,0 +1,288 @@
+// capi.cpp -- the extern "C" boundary (include/dtc.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/dtc.h"
+#include "fe.h"
+#include "mesher.h"
+#include "solver.h"
+
+struct dtc_handle {
+  dtc_options opt;
+  dtc::DeviceSolver solver;
+  std::string err;
+  dtc::SolverStats last;
+};
+
+namespace {
+
+using namespace dtc;
+
+int validate_domain(const dtc_domain_in& in, std::string& msg) {
+  if (in.elem_type != DTC_HEX08 && in.elem_type != DTC_HEX20) { msg = "elem_type must be 8 or 20"; return 1; }
+  if (!in.phi) { msg = "phi is NULL"; return 1; }
+  if (in.phi_type != 1 && in.phi_type != 2 && in.phi_type != 4) { msg = "phi_type must be 1, 2 or 4"; return 1; }
+  for (int d = 0; d < 3; ++d) {
+    if (in.L[d] < 1 || in.L[d] > 1024) { msg = "L out of range [1, 1024]"; return 1; }
+    if (!(in.delta[d] > 0) || !(in.phdsize[d] > 0)) { msg = "delta and phdsize must be > 0"; return 1; }
+  }
+  if (in.delta[0] != in.delta[1] || in.delta[0] != in.delta[2]) { msg = "voxels must be cubic (delta equal in x, y, z)"; return 1; }
+  if (!(in.E > 0) || !(in.nu > -1.0 && in.nu < 0.5) || !(in.rve_strain != 0)) { msg = "E > 0, -1 < nu < 0.5, rve_strain != 0 required"; return 1; }
+  return 0;
+}
+
+void plan_all(const dtc_domain_in* in, int64_t n, std::vector<MeshPlan>& plans, bool numbering, int threads) {
+  plans.resize(n);
+  int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
+  std::atomic<int64_t> next(0);
+  auto work = [&]() {
+    for (;;) {
+      int64_t i = next.fetch_add(1);
+      if (i >= n) break;
+      plan_mesh(in[i], numbering, plans[i]);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+}
+
+// The last element kept only by the compaction quirk contributes its 3x3 diagonal block at
+// its surviving node; that node is decoupled, so its displacement is the prescribed value
+// on the boundary and 0 inside, and its reaction Ke_ll * u enters ff like any other node.
+void quirk_correction(const dtc_domain_in& in, const MeshPlan& mp, double nu, dtc_domain_out* o) {
+  if (!mp.last_partial || !mp.last_on_boundary) return;
+  const int nen = mp.nen, nd = 3 * nen;
+  std::vector<double> kh(nd * nd);
+  voxel_stiffness(nen, nu, kh.data());
+  const double a = in.phdsize[0] * in.delta[0];
+  const double E = in.E_voxel ? (double)in.E_voxel[mp.last_voxel] : in.E;
+  const double s = E * a;
+  double x[3], lo[3], hi[3], xi[3], N[8], uu[8 * 3 * 24];
+  grid_coordinate(in, nen, mp.last_grid, x);
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = (double)(in.xa_n[d] - 1) * in.delta[d];
+    hi[d] = (double)(in.xa_n[d] + in.L[d] - 1) * in.delta[d];
+  }
+  geom_to_xi(x, lo, hi, xi);
+  macro_shape8(xi, N);
+  macro_modes(1e-6, uu);
+  const int ln = mp.last_local;
+  for (int lc = 0; lc < 24; ++lc) {
+    double g[3], F[3];
+    for (int c = 0; c < 3; ++c) g[c] = boundary_value(uu, N, c, lc);
+    for (int c = 0; c < 3; ++c) {
+      F[c] = 0.0;
+      for (int cj = 0; cj < 3; ++cj) F[c] += s * kh[(3 * ln + c) + nd * (3 * ln + cj)] * g[cj];
+    }
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 8; ++l) o->ff[(k * 8 + l) + 24 * lc] += F[k] * N[l];
+    if (o->displ || o->force) {
+      const int64_t id = mp.nn - 1;  // the last node keeps the last id
+      for (int c = 0; c < 3; ++c) {
+        if (o->displ) o->displ[(size_t)lc * 3 * mp.nn + 3 * id + c] = g[c];
+        if (o->force) o->force[(size_t)lc * 3 * mp.nn + 3 * id + c] = F[c];
+      }
+    }
+  }
+}
+
+int64_t device_bytes_per_node() { return 72 * (4 * 8 + 4 * 4) + 64; }
+
+}  // namespace
+
+namespace dtc {
+int rotation_search_device(const std::vector<const double*>& ees, std::vector<int64_t>& ang, std::vector<int>& jj,
+                           std::vector<double>& crit, cudaStream_t s, int64_t& launches, std::string& msg);
+}
+
+extern "C" {
+
+int32_t dtc_abi_version(void) { return DTC_ABI_VERSION; }
+
+void dtc_default_options(dtc_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->abi_version = DTC_ABI_VERSION;
+  opt->precision = DTC_PREC_FP64;
+  opt->rtol = 1e-3;       // -ksp_rtol 1.e-03 (f-src/mod_parameters.f90:31)
+  opt->max_it = 500000;   // -ksp_max_it 500000 (:32)
+  opt->inner_rtol = 1e-5;
+  opt->max_refine = 12;
+  opt->rotation_search = 1;
+  opt->device = 0;
+}
+
+dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
+  if (!handle) return DTC_ERR_INVALID_ARGUMENT;
+  *handle = nullptr;
+  dtc_options o;
+  dtc_default_options(&o);
+  if (opt) {
+    if (opt->abi_version != DTC_ABI_VERSION) return DTC_ERR_ABI_MISMATCH;
+    o = *opt;
+  }
+  if (!(o.rtol > 0 && o.rtol < 1) || o.max_it < 1 || (o.precision != DTC_PREC_FP64 && o.precision != DTC_PREC_MIXED))
+    return DTC_ERR_INVALID_ARGUMENT;
+  dtc_handle* h = new (std::nothrow) dtc_handle();
+  if (!h) return DTC_ERR_OUT_OF_MEMORY;
+  h->opt = o;
+  int rc = h->solver.init(o.device, h->err);
+  if (rc != DTC_OK) { delete h; return (dtc_status)rc; }
+  h->solver.set_keep(o.keep_displacements != 0);
+  *handle = h;
+  return DTC_OK;
+}
+
+dtc_status dtc_destroy(dtc_handle* handle) {
+  delete handle;
+  return DTC_OK;
+}
+
+const char* dtc_last_error(const dtc_handle* handle) {
+  if (!handle) return "invalid handle";
+  return handle->err.c_str();
+}
+
+dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out) {
+  if (!in || !out) return DTC_ERR_INVALID_ARGUMENT;
+  std::string msg;
+  if (validate_domain(*in, msg)) return DTC_ERR_INVALID_ARGUMENT;
+  MeshPlan mp;
+  if (plan_mesh(*in, true, mp) != DTC_OK) return DTC_ERR_INVALID_ARGUMENT;
+  out->ne = mp.ne; out->nn = mp.nn; out->nb = mp.nb;
+  out->status = mp.status;
+  out->last_elem_partial = mp.last_partial ? 1 : 0;
+  if (mp.status == DTC_DOMAIN_EMPTY || mp.status == DTC_DOMAIN_NO_STRUCTURE) return DTC_OK;
+  const int nen = mp.nen;
+  if (out->elems) {
+    if (out->cap_elems < mp.ne) return DTC_ERR_INVALID_ARGUMENT;
+    std::memcpy(out->elems, mp.elems.data(), sizeof(int64_t) * mp.elems.size());
+  }
+  if (out->nodes || out->bnode_ids || out->bnode_vals) {
+    if (out->cap_nodes < mp.nn) return DTC_ERR_INVALID_ARGUMENT;
+    double lo[3], hi[3], uu[8 * 3 * 24];
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = (double)(in->xa_n[d] - 1) * in->delta[d];
+      hi[d] = (double)(in->xa_n[d] + in->L[d] - 1) * in->delta[d];
+    }
+    macro_modes(1e-6, uu);
+    int64_t b = 0;
+    for (int64_t id = 0; id < mp.nn; ++id) {
+      double x[3];
+      grid_coordinate(*in, nen, mp.node_grid[id], x);
+      if (out->nodes) for (int d = 0; d < 3; ++d) out->nodes[3 * id + d] = x[d];
+      if (!grid_on_boundary(in->L, nen, mp.node_grid[id])) continue;
+      if (out->bnode_ids) out->bnode_ids[b] = id + 1;
+      if (out->bnode_vals) {
+        double xi[3], N[8];
+        geom_to_xi(x, lo, hi, xi);
+        macro_shape8(xi, N);
+        for (int c = 0; c < 3; ++c)
+          for (int lc = 0; lc < 24; ++lc) out->bnode_vals[lc + 24 * (3 * b + c)] = boundary_value(uu, N, c, lc);
+      }
+      ++b;
+    }
+  }
+  return DTC_OK;
+}
+
+dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dtc_domain_out* out) {
+  if (!h) return DTC_ERR_INVALID_ARGUMENT;
+  h->err.clear();
+  if (n < 0 || (n > 0 && (!in || !out))) { h->err = "in/out must be non-NULL for n > 0"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (n == 0) return DTC_OK;
+  if (cudaSetDevice(h->opt.device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
+  for (int64_t i = 0; i < n; ++i) {
+    std::string msg;
+    if (validate_domain(in[i], msg)) { h->err = "domain " + std::to_string(i) + ": " + msg; return DTC_ERR_INVALID_ARGUMENT; }
+    if (in[i].nu != in[0].nu) { h->err = "all domains of one call must share nu"; return DTC_ERR_INVALID_ARGUMENT; }
+    if (in[i].elem_type != DTC_HEX08) { h->err = "this build solves HEX08 micro elements only"; return DTC_ERR_INVALID_ARGUMENT; }
+  }
+  std::vector<MeshPlan> plans;
+  bool want_fields = false;
+  for (int64_t i = 0; i < n; ++i) want_fields = want_fields || out[i].displ || out[i].force;
+  plan_all(in, n, plans, want_fields, h->opt.host_threads);
+  std::vector<DomainTask> tasks;
+  for (int64_t i = 0; i < n; ++i) {
+    dtc_domain_out* o = &out[i];
+    double* keep_d = o->displ;
+    double* keep_f = o->force;
+    std::memset(o, 0, sizeof(*o));
+    o->displ = keep_d; o->force = keep_f;
+    o->domain_number = in[i].domain_number;
+    o->status = plans[i].status;
+    o->ne = plans[i].ne; o->nn = plans[i].nn; o->nb = plans[i].nb;
+    o->n_free_dof = plans[i].n_free_dof;
+    if (plans[i].status == DTC_DOMAIN_OK) tasks.push_back(DomainTask{&in[i], &plans[i], o});
+  }
+  // memory-bounded chunks
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { h->err = "cudaMemGetInfo failed"; return DTC_ERR_CUDA; }
+  const double budget = 0.80 * (double)free_b;
+  h->last = SolverStats();
+  size_t k = 0;
+  while (k < tasks.size()) {
+    std::vector<DomainTask> chunk;
+    double bytes = 0;
+    while (k < tasks.size()) {
+      const dtc_domain_in& d = *tasks[k].in;
+      const double nb = (double)(d.L[0] + 1) * (d.L[1] + 1) * (d.L[2] + 1) * device_bytes_per_node();
+      if (!chunk.empty() && bytes + nb > budget) break;
+      bytes += nb;
+      chunk.push_back(tasks[k++]);
+    }
+    int rc = h->solver.solve(chunk, h->opt, in[0].nu, h->err);
+    if (rc != DTC_OK) return (dtc_status)rc;
+    h->last.ms_solve += h->solver.stats().ms_solve;
+    h->last.kernel_launches += h->solver.stats().kernel_launches;
+    h->last.dof_iterations += h->solver.stats().dof_iterations;
+  }
+  std::vector<const double*> ees;
+  std::vector<dtc_domain_out*> rot_out;
+  for (DomainTask& t : tasks) {
+    quirk_correction(*t.in, *t.plan, in[0].nu, t.out);
+    homogenise(t.out->ff, t.in->L, t.in->delta, t.in->rve_strain, t.out);
+    t.out->density = (double)t.plan->ne / ((double)t.in->L[0] * (double)t.in->L[1] * (double)t.in->L[2]);
+    bool finite = true;
+    for (int q = 0; q < 36; ++q) finite = finite && std::isfinite(t.out->ee[q]);
+    if (h->opt.rotation_search && finite) { ees.push_back(t.out->ee); rot_out.push_back(t.out); }
+  }
+  if (!ees.empty()) {
+    std::vector<int64_t> ang;
+    std::vector<int> jj;
+    std::vector<double> crit;
+    cudaStream_t s = nullptr;
+    int rc = rotation_search_device(ees, ang, jj, crit, s, h->last.kernel_launches, h->err);
+    if (rc != DTC_OK) return (dtc_status)rc;
+    for (size_t d = 0; d < ees.size(); ++d) {
+      finish_rotation(ees[d], 1, &ang[6 * d], jj[2 * d], crit[2 * d], rot_out[d]);
+      finish_rotation(ees[d], 2, &ang[6 * d + 3], jj[2 * d + 1], crit[2 * d + 1], rot_out[d]);
+    }
+  }
+  return DTC_OK;
+}
+
+dtc_status dtc_energy_grad(dtc_handle* h, const double* dloss_dc, float* const* grad_e, int64_t n) {
+  if (!h || !dloss_dc || !grad_e || n < 0) return DTC_ERR_INVALID_ARGUMENT;
+  return (dtc_status)h->solver.energy_grad(dloss_dc, grad_e, n, h->err);
+}
+
+dtc_status dtc_get_stats(const dtc_handle* h, double* ms_solve, int64_t* kernel_launches, double* dof_iterations) {
+  if (!h) return DTC_ERR_INVALID_ARGUMENT;
+  if (ms_solve) *ms_solve = h->last.ms_solve;
+  if (kernel_launches) *kernel_launches = h->last.kernel_launches;
+  if (dof_iterations) *dof_iterations = h->last.dof_iterations;
+  return DTC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,958 @@
+// kernels.cu -- sm_100a kernels of the batched voxel solver and its host driver.
+//
+// Operator: the assembled stiffness of the reference (MatSetValues of one Ke per element,
+// f-src/mod_dtc_main_subroutines.f90:516-579) is never formed.  K*u is applied matrix-free
+// as a node-centric sweep: the output at node n sums, over the <= 8 kept voxels around n,
+// s_v * Khat[rows of n's corner, :] * u_v, where s_v = E_v * a and Khat the unit voxel
+// stiffness.  Constrained DOFs (all nodes on the domain box, mod_struct_preprocess.f90:
+// 564-592) are excluded from the unknowns exactly like MatZeroRowsColumns with diag 0
+// (:945-951), so the iteration runs on the interior nodes only.
+//
+// Solver: per (domain, load case) the Jacobi-PCG recurrence of PETSc's KSPSolve_CG with
+// KSPConvergedDefault (zero initial guess, preconditioned 2-norm, ttol = max(rtol*||D^-1 b||,
+// 1e-50), divergence at 1e5*||D^-1 b||) -- four launches per iteration for the whole batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fe.h"
+#include "kernels.cuh"
+#include "solver.h"
+
+namespace dtc {
+
+__constant__ double c_khat64[576];   // unit voxel stiffness, column-major (symmetric)
+__constant__ float c_khat32[576];
+__constant__ double c_uu[8 * 3 * kNLC];  // macro modes uu(8,3,24) for eps = 1e-6
+
+template <typename T> struct KhatC;
+template <> struct KhatC<float> {
+  static __device__ __forceinline__ float at(int i) { return c_khat32[i]; }
+};
+template <> struct KhatC<double> {
+  static __device__ __forceinline__ double at(int i) { return c_khat64[i]; }
+};
+
+// -------------------------------------------------------------------------------------
+// Matrix-free K*u on one tile.  Window w[px][py][pz][c] holds u at x-1+px, y-1+py, z-1+pz;
+// sv[a][b][c] the scale of voxel (x-1+a, y-1+b, z-1+c).
+template <typename T>
+__device__ __forceinline__ void apply_node(const T (&w)[3][3][3][3], const float (&sv)[2][2][2], T (&acc)[3]) {
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const float s = sv[a][b][c];
+        if (s != 0.0f) {
+          const int ln = corner_local(1 - a, 1 - b, 1 - c);
+          T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+          for (int mz = 0; mz < 2; ++mz)
+#pragma unroll
+            for (int my = 0; my < 2; ++my)
+#pragma unroll
+              for (int mx = 0; mx < 2; ++mx) {
+                const int lm = corner_local(mx, my, mz);
+#pragma unroll
+                for (int cj = 0; cj < 3; ++cj) {
+                  const T v = w[a + mx][b + my][c + mz][cj];
+                  const int col = 24 * (3 * lm + cj);
+                  t0 = fma(KhatC<T>::at(col + 3 * ln + 0), v, t0);
+                  t1 = fma(KhatC<T>::at(col + 3 * ln + 1), v, t1);
+                  t2 = fma(KhatC<T>::at(col + 3 * ln + 2), v, t2);
+                }
+              }
+          const T ts = (T)s;
+          acc[0] = fma(ts, t0, acc[0]);
+          acc[1] = fma(ts, t1, acc[1]);
+          acc[2] = fma(ts, t2, acc[2]);
+        }
+      }
+}
+
+template <typename T, bool GUARD>
+__device__ __forceinline__ void load_plane(T (&pl)[3][3][3], const T* __restrict__ u, const DomDev& D, int x, int y,
+                                           int z, int lc) {
+#pragma unroll
+  for (int py = 0; py < 3; ++py)
+#pragma unroll
+    for (int pz = 0; pz < 3; ++pz) {
+      const int yy = y + py - 1, zz = z + pz - 1;
+      bool ok = true;
+      if (GUARD) ok = (x >= 0 && x < D.n[0] && yy >= 0 && yy < D.n[1] && zz >= 0 && zz < D.n[2]);
+      const int64_t base = ok ? vec_index(node_index(D, x, yy, zz), 0, lc) : 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pl[py][pz][c] = ok ? __ldg(u + base + c * kNLC) : T(0);
+    }
+}
+
+template <bool GUARD>
+__device__ __forceinline__ void load_voxels(float (&sp)[2][2], const float* __restrict__ svox, const DomDev& D, int vx,
+                                            int y, int z) {
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int vy = y - 1 + b, vz = z - 1 + c;
+      bool ok = true;
+      if (GUARD) ok = (vx >= 0 && vx < D.L[0] && vy >= 0 && vy < D.L[1] && vz >= 0 && vz < D.L[2]);
+      const int64_t off = ok ? vx + (int64_t)D.L[0] * (vy + (int64_t)D.L[1] * vz) : 0;
+      sp[b][c] = ok ? __ldg(svox + D.vox_off + off) : 0.0f;
+    }
+}
+
+// y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
+// in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
+// node of the grid (reaction forces).
+template <typename T, bool ALL, bool DOT>
+__global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                     const float* __restrict__ svox, const T* __restrict__ u,
+                                                     T* __restrict__ y, double scale, double* __restrict__ acc,
+                                                     const int* __restrict__ dom_active) {
+  __shared__ double red[32];
+  const Tile t = tiles[blockIdx.x];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int lc = blockIdx.y * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  const int lo = ALL ? 0 : 1;
+  const int xhi = ALL ? D.L[0] : D.L[0] - 1, yhi = ALL ? D.L[1] : D.L[1] - 1, zhi = ALL ? D.L[2] : D.L[2] - 1;
+  double dot = 0.0;
+  if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi) {
+    T w[3][3][3][3];
+    float sv[2][2][2];
+    load_plane<T, ALL>(w[0], u, D, t.x0 - 1, yy, zz, lc);
+    load_plane<T, ALL>(w[1], u, D, t.x0, yy, zz, lc);
+    load_voxels<ALL>(sv[0], svox, D, t.x0 - 1, yy, zz);
+#pragma unroll 1
+    for (int i = 0; i < kTileX; ++i) {
+      const int x = t.x0 + i;
+      if (x > xhi) break;
+      load_plane<T, ALL>(w[2], u, D, x + 1, yy, zz, lc);
+      load_voxels<ALL>(sv[1], svox, D, x, yy, zz);
+      const bool any = (sv[0][0][0] != 0.f) | (sv[0][0][1] != 0.f) | (sv[0][1][0] != 0.f) | (sv[0][1][1] != 0.f) |
+                       (sv[1][0][0] != 0.f) | (sv[1][0][1] != 0.f) | (sv[1][1][0] != 0.f) | (sv[1][1][1] != 0.f);
+      if (any) {
+        T a3[3] = {0, 0, 0};
+        apply_node<T>(w, sv, a3);
+        const int64_t b = vec_index(node_index(D, x, yy, zz), 0, lc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T v = (T)(scale * D.scale * (double)a3[c]);
+          y[b + c * kNLC] = v;
+          if (DOT) dot += (double)w[1][1][1][c] * (double)v;
+        }
+      }
+#pragma unroll
+      for (int py = 0; py < 3; ++py)
+#pragma unroll
+        for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            w[0][py][pz][c] = w[1][py][pz][c];
+            w[1][py][pz][c] = w[2][py][pz][c];
+          }
+#pragma unroll
+      for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+        for (int c2 = 0; c2 < 2; ++c2) sv[0][b2][c2] = sv[1][b2][c2];
+    }
+  }
+  if (DOT) {
+    const double s = block_sum_lc<double>(dot, red);
+    if (threadIdx.x < 8) atomicAdd(acc + (int64_t)t.dom * kNLC + lc, s);
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Node set-up: flags and the Jacobi diagonal sum_v s_v Khat(ii) (PCJACOBI of the
+// row-and-column-zeroed matrix; constrained rows are never iterated on).  One thread per
+// node: lane = x offset in the tile, rows as in the matvec.
+__global__ void __launch_bounds__(kThreads) k_node_setup(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                         const float* __restrict__ svox, uint8_t* __restrict__ flags,
+                                                         double* __restrict__ dinv64, float* __restrict__ dinv32) {
+  const Tile t = tiles[blockIdx.x];
+  const DomDev D = doms[t.dom];
+  const int x = t.x0 + (threadIdx.x & 7), row = threadIdx.x >> 3;
+  const int y = t.y0 + (row & 3), z = t.z0 + (row >> 2);
+  if (x > D.L[0] || y > D.L[1] || z > D.L[2]) return;
+  double d[3] = {0, 0, 0};
+  bool active = false;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 2; ++c) {
+        const int vx = x - 1 + a, vy = y - 1 + b, vz = z - 1 + c;
+        if (vx < 0 || vy < 0 || vz < 0 || vx >= D.L[0] || vy >= D.L[1] || vz >= D.L[2]) continue;
+        const float s = svox[D.vox_off + vx + (int64_t)D.L[0] * (vy + (int64_t)D.L[1] * vz)];
+        if (s == 0.0f) continue;
+        active = true;
+        const int ln = corner_local(1 - a, 1 - b, 1 - c);
+        for (int k = 0; k < 3; ++k) d[k] += (double)s * c_khat64[(3 * ln + k) * 25];
+      }
+  for (int k = 0; k < 3; ++k) d[k] *= D.scale;
+  const bool bnd = (x == 0 || x == D.L[0] || y == 0 || y == D.L[1] || z == 0 || z == D.L[2]);
+  const int64_t n = node_index(D, x, y, z);
+  flags[n] = (active ? kNodeActive : 0) | (bnd ? kNodeBoundary : 0);
+  for (int k = 0; k < 3; ++k) {
+    const double di = (active && !bnd && d[k] != 0.0) ? 1.0 / d[k] : 0.0;
+    dinv64[n * 3 + k] = di;
+    dinv32[n * 3 + k] = (float)di;
+  }
+}
+
+// Prescribed displacements of every load case on the boundary nodes
+// (determine_prescribed_displ, mod_write_deck.f90:22-51): sum_l N_l(xi(x)) uu(l,c,lc).
+__device__ __forceinline__ void node_xi(const DomDev& D, int x, int y, int z, double xi[3]) {
+  const int g[3] = {x, y, z};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double pos = (double)((int64_t)g[k] + (int64_t)D.min_c_off[k]) * D.delta;
+    xi[k] = 2.0 / (D.max_c[k] - D.min_c[k]) * pos - (D.max_c[k] + D.min_c[k]) / (D.max_c[k] - D.min_c[k]);
+  }
+}
+__device__ __forceinline__ void shape8(const double xi[3], double N[8]) {
+  const double g1x = 0.5 * (1.0 - xi[0]), g2x = 0.5 * (1.0 + xi[0]);
+  const double g1y = 0.5 * (1.0 - xi[1]), g2y = 0.5 * (1.0 + xi[1]);
+  const double g1z = 0.5 * (1.0 - xi[2]), g2z = 0.5 * (1.0 + xi[2]);
+  N[0] = g1x * g1y * g1z; N[1] = g2x * g1y * g1z; N[2] = g2x * g2y * g1z; N[3] = g1x * g2y * g1z;
+  N[4] = g1x * g1y * g2z; N[5] = g2x * g1y * g2z; N[6] = g2x * g2y * g2z; N[7] = g1x * g2y * g2z;
+}
+
+__global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __restrict__ tiles,
+                                                              const DomDev* __restrict__ doms,
+                                                              const uint8_t* __restrict__ flags,
+                                                              double* __restrict__ X) {
+  const Tile t = tiles[blockIdx.x];
+  const DomDev D = doms[t.dom];
+  const int x = t.x0 + (threadIdx.x & 7), row = threadIdx.x >> 3;
+  const int y = t.y0 + (row & 3), z = t.z0 + (row >> 2);
+  if (x > D.L[0] || y > D.L[1] || z > D.L[2]) return;
+  const int64_t n = node_index(D, x, y, z);
+  const uint8_t f = flags[n];
+  if (!(f & kNodeActive) || !(f & kNodeBoundary)) return;
+  double xi[3], N[8];
+  node_xi(D, x, y, z, xi);
+  shape8(xi, N);
+  for (int c = 0; c < 3; ++c)
+    for (int lc = 0; lc < kNLC; ++lc) {
+      double s = 0.0;
+      for (int l = 0; l < 8; ++l) s += N[l] * c_uu[l + 8 * c + 24 * lc];
+      X[vec_index(n, c, lc)] = s;
+    }
+}
+
+// -------------------------------------------------------------------------------------
+// CG vector kernels on interior tiles; lane = load case, row = (y,z), sweep x.
+#define DTC_TILE_PROLOGUE                                                      \
+  const Tile t = tiles[blockIdx.x];                                            \
+  if (dom_active && !dom_active[t.dom]) return;                                \
+  const DomDev D = doms[t.dom];                                                \
+  const int lc = blockIdx.y * kLcGroup + (threadIdx.x & 7);                    \
+  const int row = threadIdx.x >> 3;                                            \
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);                     \
+  const bool rowok = yy >= 1 && yy <= D.L[1] - 1 && zz >= 1 && zz <= D.L[2] - 1; \
+  const int64_t col = (int64_t)t.dom * kNLC + lc;
+
+// p = D^-1 r + bfac * p
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_direction(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                        const uint8_t* __restrict__ flags, const T* __restrict__ dinv,
+                                                        const T* __restrict__ r, T* __restrict__ p,
+                                                        const ColState* __restrict__ st,
+                                                        const int* __restrict__ dom_active) {
+  DTC_TILE_PROLOGUE
+  if (!rowok || !st[col].active) return;
+  const T bf = (T)st[col].bfac;
+  for (int i = 0; i < kTileX; ++i) {
+    const int x = t.x0 + i;
+    if (x > D.L[0] - 1) break;
+    const int64_t n = node_index(D, x, yy, zz);
+    if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t k = vec_index(n, c, lc);
+      p[k] = dinv[n * 3 + c] * r[k] + bf * p[k];
+    }
+  }
+}
+
+// x += alpha p ; r -= alpha w ; z = D^-1 r ; acc_zz += z.z ; acc_zr += z.r
+// alpha = beta / (p.w) unless the column stopped or p.w flags an indefinite operator.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_update(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                     const uint8_t* __restrict__ flags, const T* __restrict__ dinv,
+                                                     T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                                                     const T* __restrict__ w, const ColState* __restrict__ st,
+                                                     const double* __restrict__ acc_pw, double* __restrict__ acc_zz,
+                                                     double* __restrict__ acc_zr, const int* __restrict__ dom_active) {
+  __shared__ double red[32];
+  DTC_TILE_PROLOGUE
+  double zz2 = 0.0, zr = 0.0;
+  const ColState s = st[col];
+  const double pw = acc_pw[col];
+  const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0) || pw == 0.0);
+  const bool valid = s.active && pw != 0.0 && !flip;
+  if (rowok && valid) {
+    const T a = (T)(s.beta / pw);
+    for (int i = 0; i < kTileX; ++i) {
+      const int xx = t.x0 + i;
+      if (xx > D.L[0] - 1) break;
+      const int64_t n = node_index(D, xx, yy, zz);
+      if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int64_t k = vec_index(n, c, lc);
+        x[k] = x[k] + a * p[k];
+        const T rn = r[k] - a * w[k];
+        r[k] = rn;
+        const T z = dinv[n * 3 + c] * rn;
+        zz2 += (double)z * (double)z;
+        zr += (double)z * (double)rn;
+      }
+    }
+  }
+  const double s1 = block_sum_lc<double>(zz2, red);
+  __syncthreads();
+  const double s2 = block_sum_lc<double>(zr, red);
+  if (threadIdx.x < 8 && valid) {
+    atomicAdd(acc_zz + col, s1);
+    atomicAdd(acc_zr + col, s2);
+  }
+}
+
+// z = D^-1 r; acc_zz += z.z ; acc_zr += z.r (start of a solve)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_initial_dots(const Tile* __restrict__ tiles,
+                                                           const DomDev* __restrict__ doms,
+                                                           const uint8_t* __restrict__ flags,
+                                                           const T* __restrict__ dinv, const T* __restrict__ r,
+                                                           double* __restrict__ acc_zz, double* __restrict__ acc_zr,
+                                                           const int* __restrict__ dom_active) {
+  __shared__ double red[32];
+  DTC_TILE_PROLOGUE
+  double zz2 = 0.0, zr = 0.0;
+  if (rowok) {
+    for (int i = 0; i < kTileX; ++i) {
+      const int xx = t.x0 + i;
+      if (xx > D.L[0] - 1) break;
+      const int64_t n = node_index(D, xx, yy, zz);
+      if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T rn = r[vec_index(n, c, lc)];
+        const T z = dinv[n * 3 + c] * rn;
+        zz2 += (double)z * (double)z;
+        zr += (double)z * (double)rn;
+      }
+    }
+  }
+  const double s1 = block_sum_lc<double>(zz2, red);
+  __syncthreads();
+  const double s2 = block_sum_lc<double>(zr, red);
+  if (threadIdx.x < 8) {
+    atomicAdd(acc_zz + col, s1);
+    atomicAdd(acc_zr + col, s2);
+  }
+}
+
+// Column state at the start of a solve (KSPSolve_CG before its loop + KSPConvergedDefault
+// at n = 0).  ttol = max(rtol * dp0, floor[col]) with floor = 1e-50 (abstol) when absent.
+__global__ void k_colstate_init(ColState* __restrict__ st, double* __restrict__ acc_zz, double* __restrict__ acc_zr,
+                                int* __restrict__ dom_active, double rtol, const double* __restrict__ floor_abs) {
+  const int d = blockIdx.x, lc = threadIdx.x;
+  int act = 0;
+  if (lc < kNLC) {
+    const int64_t col = (int64_t)d * kNLC + lc;
+    ColState s;
+    const double dp0 = sqrt(acc_zz[col]);
+    s.dp0 = dp0; s.dp = dp0; s.its = 0; s.bfac = 0.0; s.dpi = 0.0; s.betaold = 1.0; s.beta = 0.0; s.pad = 0;
+    const double fl = floor_abs ? fmax(floor_abs[col], 1e-50) : 1e-50;
+    s.ttol = fmax(rtol * dp0, fl);
+    s.active = 0;
+    if (!isfinite(dp0)) s.reason = kNanOrInf;
+    else if (dp0 <= s.ttol) s.reason = kConverged;
+    else {
+      s.beta = acc_zr[col];
+      if (s.beta == 0.0) { s.its = 1; s.reason = kConvergedAtol; }
+      else { s.reason = kIterating; s.active = 1; }
+    }
+    st[col] = s;
+    acc_zz[col] = 0.0; acc_zr[col] = 0.0;
+    act = s.active;
+  }
+  act = __syncthreads_or(act);
+  if (threadIdx.x == 0) dom_active[d] = act;
+}
+
+// End of one CG iteration for every column (the tail of KSPSolve_CG's loop body).
+__global__ void k_colstate(ColState* __restrict__ st, double* __restrict__ acc_pw, double* __restrict__ acc_zz,
+                           double* __restrict__ acc_zr, int* __restrict__ dom_active, int64_t max_it) {
+  const int d = blockIdx.x, lc = threadIdx.x;
+  int act = 0;
+  if (lc < kNLC) {
+    const int64_t col = (int64_t)d * kNLC + lc;
+    ColState s = st[col];
+    if (s.active) {
+      const double pw = acc_pw[col];
+      const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0));
+      s.its += 1;
+      if (pw == 0.0 || flip) { s.reason = kIndefinite; s.active = 0; }
+      else {
+        s.dpi = pw;
+        s.betaold = s.beta;
+        const double dp = sqrt(acc_zz[col]);
+        s.dp = dp;
+        if (!isfinite(dp)) { s.reason = kNanOrInf; s.active = 0; }
+        else if (dp <= s.ttol) { s.reason = kConverged; s.active = 0; }
+        else if (dp >= 1e5 * s.dp0) { s.reason = kDivergedDtol; s.active = 0; }
+        else {
+          s.beta = acc_zr[col];
+          if (s.beta == 0.0) { s.its += 1; s.reason = kConvergedAtol; s.active = 0; }
+          else if (s.beta * s.betaold < 0.0) { s.its += 1; s.reason = kIndefinite; s.active = 0; }
+          else if (s.its >= max_it) { s.reason = kDivergedIts; s.active = 0; }
+          else s.bfac = s.beta / s.betaold;
+        }
+      }
+      st[col] = s;
+    }
+    acc_pw[col] = 0.0; acc_zz[col] = 0.0; acc_zr[col] = 0.0;
+    act = s.active;
+  }
+  act = __syncthreads_or(act);
+  if (threadIdx.x == 0) dom_active[d] = act;
+}
+
+__global__ void k_count_active(const int* __restrict__ dom_active, int ndom, int* __restrict__ count) {
+  __shared__ int sh;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  int c = 0;
+  for (int i = threadIdx.x; i < ndom; i += blockDim.x) c += dom_active[i] ? 1 : 0;
+  atomicAdd(&sh, c);
+  __syncthreads();
+  if (threadIdx.x == 0) *count = sh;
+}
+
+// -------------------------------------------------------------------------------------
+// Mixed precision: outer FP64 residual check, FP64 -> FP32 residual, FP32 correction -> FP64.
+__global__ void k_outer_check(ColState* __restrict__ ost, double* __restrict__ acc_zz, double* __restrict__ target,
+                              int* __restrict__ dom_active, double rtol, int first) {
+  const int d = blockIdx.x, lc = threadIdx.x;
+  int act = 0;
+  if (lc < kNLC) {
+    const int64_t col = (int64_t)d * kNLC + lc;
+    ColState s = ost[col];
+    const double dp = sqrt(acc_zz[col]);
+    if (first) {
+      s.dp0 = dp; s.ttol = fmax(rtol * dp, 1e-50); s.its = 0; s.active = 1; s.reason = kIterating;
+      s.beta = 0; s.betaold = 0; s.dpi = 0; s.bfac = 0; s.pad = 0;
+    }
+    s.dp = dp;
+    if (s.active) {
+      if (!isfinite(dp)) { s.reason = kNanOrInf; s.active = 0; }
+      else if (dp <= s.ttol) { s.reason = kConverged; s.active = 0; }
+    }
+    target[col] = s.active ? 0.5 * s.ttol : 0.0;
+    ost[col] = s;
+    acc_zz[col] = 0.0;
+    act = s.active;
+  }
+  act = __syncthreads_or(act);
+  if (threadIdx.x == 0) dom_active[d] = act;
+}
+
+// acc_zz += ||D^-1 r||^2 over interior nodes (FP64 residual norm)
+__global__ void __launch_bounds__(kThreads) k_residual_norm(const Tile* __restrict__ tiles,
+                                                            const DomDev* __restrict__ doms,
+                                                            const uint8_t* __restrict__ flags,
+                                                            const double* __restrict__ dinv,
+                                                            const double* __restrict__ r, double* __restrict__ acc_zz) {
+  __shared__ double red[32];
+  const int* dom_active = nullptr;
+  DTC_TILE_PROLOGUE
+  double zz2 = 0.0;
+  if (rowok) {
+    for (int i = 0; i < kTileX; ++i) {
+      const int xx = t.x0 + i;
+      if (xx > D.L[0] - 1) break;
+      const int64_t n = node_index(D, xx, yy, zz);
+      if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double z = dinv[n * 3 + c] * r[vec_index(n, c, lc)];
+        zz2 += z * z;
+      }
+    }
+  }
+  const double s1 = block_sum_lc<double>(zz2, red);
+  if (threadIdx.x < 8) atomicAdd(acc_zz + col, s1);
+}
+
+// r32 = (float) r64 for columns still refining, 0 otherwise; x32 = p32 = 0
+__global__ void __launch_bounds__(kThreads) k_start_inner(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                          const uint8_t* __restrict__ flags,
+                                                          const double* __restrict__ r64, float* __restrict__ r32,
+                                                          float* __restrict__ x32, float* __restrict__ p32,
+                                                          const ColState* __restrict__ ost) {
+  const int* dom_active = nullptr;
+  DTC_TILE_PROLOGUE
+  if (!rowok) return;
+  const bool on = ost[col].active != 0;
+  for (int i = 0; i < kTileX; ++i) {
+    const int xx = t.x0 + i;
+    if (xx > D.L[0] - 1) break;
+    const int64_t n = node_index(D, xx, yy, zz);
+    if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t k = vec_index(n, c, lc);
+      r32[k] = on ? (float)r64[k] : 0.0f;
+      x32[k] = 0.0f;
+      p32[k] = 0.0f;
+    }
+  }
+}
+
+// X += (double) x32 for columns still refining; inner iterations added to the outer count
+__global__ void __launch_bounds__(kThreads) k_apply_correction(const Tile* __restrict__ tiles,
+                                                               const DomDev* __restrict__ doms,
+                                                               const uint8_t* __restrict__ flags,
+                                                               const float* __restrict__ x32, double* __restrict__ X,
+                                                               const ColState* __restrict__ ost) {
+  const int* dom_active = nullptr;
+  DTC_TILE_PROLOGUE
+  if (!rowok || !ost[col].active) return;
+  for (int i = 0; i < kTileX; ++i) {
+    const int xx = t.x0 + i;
+    if (xx > D.L[0] - 1) break;
+    const int64_t n = node_index(D, xx, yy, zz);
+    if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t k = vec_index(n, c, lc);
+      X[k] += (double)x32[k];
+    }
+  }
+}
+
+__global__ void k_add_inner_its(ColState* __restrict__ ost, const ColState* __restrict__ ist, int64_t ncol) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncol) return;
+  if (ost[i].active) {
+    ost[i].its += ist[i].its;
+    ost[i].pad += 1;  // refinement steps taken
+    if (ist[i].reason == kIndefinite || ist[i].reason == kNanOrInf || ist[i].reason == kDivergedDtol)
+      ost[i].betaold = 1.0;  // remembers an inner failure
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Projection of the reaction forces on the macro shape functions
+// (mod_struct_calcmat.f90:246-280): ff((k-1)*8+l, lc) += F(k, n) * N_l(xi(x_n)), all nodes.
+__global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                     const uint8_t* __restrict__ flags, const double* __restrict__ F,
+                                                     double* __restrict__ ff) {
+  __shared__ double part[16][8][25];
+  const Tile t = tiles[blockIdx.x];
+  const DomDev D = doms[t.dom];
+  const int lcl = threadIdx.x & 7, lc = blockIdx.y * kLcGroup + lcl;
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  double acc[24];
+#pragma unroll
+  for (int k = 0; k < 24; ++k) acc[k] = 0.0;
+  if (yy <= D.L[1] && zz <= D.L[2]) {
+    for (int i = 0; i < kTileX; ++i) {
+      const int xx = t.x0 + i;
+      if (xx > D.L[0]) break;
+      const int64_t n = node_index(D, xx, yy, zz);
+      if (!(flags[n] & kNodeActive)) continue;
+      double xi[3], N[8];
+      node_xi(D, xx, yy, zz, xi);
+      shape8(xi, N);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double f = F[vec_index(n, k, lc)];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) acc[k * 8 + l] += f * N[l];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 24; ++k) part[row][lcl][k] = acc[k];
+  __syncthreads();
+  for (int j = threadIdx.x; j < 8 * 24; j += kThreads) {
+    const int l8 = j / 24, k = j % 24;
+    double s = 0.0;
+    for (int r2 = 0; r2 < 16; ++r2) s += part[r2][l8][k];
+    const int lcg = blockIdx.y * kLcGroup + l8;
+    atomicAdd(ff + (int64_t)t.dom * 576 + k + 24 * lcg, s);
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Host driver
+struct DeviceSolver::Impl {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  // persistent buffers grown on demand
+  std::vector<std::pair<void**, size_t>> owned;
+  void* bufs[32] = {nullptr};
+  size_t caps[32] = {0};
+  // last solve kept for the adjoint
+  std::vector<DomDev> last_doms;
+  std::vector<int64_t> last_task_index;
+};
+
+namespace {
+
+enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
+           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bNumBufs };
+
+int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
+  if (I.caps[which] >= bytes && I.bufs[which]) return DTC_OK;
+  if (I.bufs[which]) { cudaFree(I.bufs[which]); I.bufs[which] = nullptr; I.caps[which] = 0; }
+  size_t b = std::max<size_t>(bytes, 256);
+  DTC_CUDA(cudaMalloc(&I.bufs[which], b));
+  I.caps[which] = b;
+  return DTC_OK;
+}
+
+template <typename T> T* B(DeviceSolver::Impl& I, int which) { return static_cast<T*>(I.bufs[which]); }
+
+int launch_check(std::string& msg) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { msg = std::string("kernel launch: ") + cudaGetErrorString(e); return DTC_ERR_CUDA; }
+  return DTC_OK;
+}
+
+}  // namespace
+
+DeviceSolver::DeviceSolver() : impl_(new Impl) {}
+DeviceSolver::~DeviceSolver() {
+  if (impl_) {
+    if (impl_->device >= 0) cudaSetDevice(impl_->device);
+    for (int i = 0; i < 32; ++i) if (impl_->bufs[i]) cudaFree(impl_->bufs[i]);
+    if (impl_->stream) cudaStreamDestroy(impl_->stream);
+    delete impl_;
+  }
+}
+
+int DeviceSolver::init(int device, std::string& msg) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { msg = "no CUDA device"; return DTC_ERR_NO_DEVICE; }
+  if (device < 0 || device >= n) { msg = "device ordinal out of range"; return DTC_ERR_INVALID_ARGUMENT; }
+  DTC_CUDA(cudaSetDevice(device));
+  DTC_CUDA(cudaStreamCreateWithFlags(&impl_->stream, cudaStreamNonBlocking));
+  impl_->device = device;
+  return DTC_OK;
+}
+
+namespace {
+
+// CG on one precision: x (interior part), r = b on entry, p = 0 on entry.
+template <typename T>
+int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w, const T* dinv, double rtol,
+           const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
+  cudaStream_t s = I.stream;
+  const Tile* ti = B<Tile>(I, bTilesI);
+  const DomDev* dd = B<DomDev>(I, bDoms);
+  const uint8_t* fl = B<uint8_t>(I, bFlags);
+  ColState* st = B<ColState>(I, bSt);
+  double* pw = B<double>(I, bPw);
+  double* zz = B<double>(I, bZz);
+  double* zr = B<double>(I, bZr);
+  int* act = B<int>(I, bDomAct);
+  int* cnt = B<int>(I, bCount);
+  const dim3 grid((unsigned)nti, 3);
+  DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
+  DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
+  DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
+  if (nti > 0) k_initial_dots<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, zz, zr, nullptr);
+  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs);
+  launches += 2;
+  if (int e = launch_check(msg)) return e;
+  const int chunk = 32;
+  int h_count = 1;
+  for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
+    for (int k = 0; k < chunk; ++k) {
+      if (nti > 0) {
+        k_direction<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
+        k_matvec<T, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+        k_update<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
+      }
+      k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+      launches += 4;
+    }
+    k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
+    launches += 1;
+    if (int e = launch_check(msg)) return e;
+    DTC_CUDA(cudaMemcpyAsync(&h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DTC_CUDA(cudaStreamSynchronize(s));
+  }
+  return DTC_OK;
+}
+
+}  // namespace
+
+int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg) {
+  Impl& I = *impl_;
+  DTC_CUDA(cudaSetDevice(I.device));
+  cudaStream_t s = I.stream;
+  stats_ = SolverStats();
+  // constant tables
+  {
+    double kh[576];
+    float kh32[576];
+    voxel_stiffness(8, nu, kh);
+    for (int i = 0; i < 576; ++i) kh32[i] = (float)kh[i];
+    double uu[8 * 3 * 24];
+    macro_modes(1e-6, uu);   // the hard-coded boundary eps (mod_write_deck.f90:61)
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat64, kh, sizeof(kh), 0, cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
+  }
+  // pack the batch (all solvable tasks at once; chunking by memory happens in the caller)
+  std::vector<DomDev> doms;
+  std::vector<Tile> tiles_i, tiles_a;
+  std::vector<float> svox;
+  std::vector<int64_t> tidx;
+  int64_t node_total = 0;
+  for (size_t k = 0; k < tasks.size(); ++k) {
+    DomainTask& t = tasks[k];
+    const MeshPlan& mp = *t.plan;
+    if (mp.status != DTC_DOMAIN_OK) continue;
+    const dtc_domain_in& in = *t.in;
+    DomDev D{};
+    for (int d = 0; d < 3; ++d) { D.L[d] = (int32_t)in.L[d]; D.n[d] = (int32_t)in.L[d] + 1; }
+    D.vox_off = (int64_t)svox.size();
+    D.node_off = node_total;
+    D.delta = in.delta[0];
+    for (int d = 0; d < 3; ++d) {
+      D.min_c_off[d] = in.xa_n[d] - 1;
+      D.min_c[d] = (double)(in.xa_n[d] - 1) * in.delta[d];
+      D.max_c[d] = (double)(in.xa_n[d] + in.L[d] - 1) * in.delta[d];
+    }
+    const int64_t nvox = in.L[0] * in.L[1] * in.L[2];
+    const double a = in.phdsize[0] * in.delta[0];
+    D.scale = in.E_voxel ? a : a * in.E;
+    const int dom = (int)doms.size();
+    svox.resize(svox.size() + nvox);
+    float* sv = svox.data() + D.vox_off;
+    for (int64_t v = 0; v < nvox; ++v) sv[v] = mp.kept[v] ? (in.E_voxel ? in.E_voxel[v] : 1.0f) : 0.0f;
+    // node activity on the host for the tile lists
+    const int nx = D.n[0], ny = D.n[1], nz = D.n[2];
+    std::vector<uint8_t> act((size_t)nx * ny * nz, 0);
+    for (int64_t v = 0; v < nvox; ++v) {
+      if (sv[v] == 0.0f) continue;
+      const int vx = (int)(v % in.L[0]), vy = (int)((v / in.L[0]) % in.L[1]), vz = (int)(v / (in.L[0] * in.L[1]));
+      for (int c = 0; c < 2; ++c)
+        for (int b = 0; b < 2; ++b)
+          for (int a2 = 0; a2 < 2; ++a2) act[(vx + a2) + (size_t)nx * ((vy + b) + (size_t)ny * (vz + c))] = 1;
+    }
+    auto tile_active = [&](int x0, int y0, int z0, int lo, int hx, int hy, int hz) {
+      for (int z = z0; z < std::min(z0 + kTileZ, hz + 1); ++z)
+        for (int y = y0; y < std::min(y0 + kTileY, hy + 1); ++y)
+          for (int x = x0; x < std::min(x0 + kTileX, hx + 1); ++x)
+            if (x >= lo && y >= lo && z >= lo && act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
+      return false;
+    };
+    for (int z0 = 1; z0 <= (int)in.L[2] - 1; z0 += kTileZ)
+      for (int y0 = 1; y0 <= (int)in.L[1] - 1; y0 += kTileY)
+        for (int x0 = 1; x0 <= (int)in.L[0] - 1; x0 += kTileX)
+          if (tile_active(x0, y0, z0, 1, in.L[0] - 1, in.L[1] - 1, in.L[2] - 1))
+            tiles_i.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+    for (int z0 = 0; z0 <= (int)in.L[2]; z0 += kTileZ)
+      for (int y0 = 0; y0 <= (int)in.L[1]; y0 += kTileY)
+        for (int x0 = 0; x0 <= (int)in.L[0]; x0 += kTileX)
+          if (tile_active(x0, y0, z0, 0, in.L[0], in.L[1], in.L[2]))
+            tiles_a.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+    node_total += (int64_t)nx * ny * nz;
+    doms.push_back(D);
+    tidx.push_back((int64_t)k);
+  }
+  const int ndom = (int)doms.size();
+  if (ndom == 0) return DTC_OK;
+  const int64_t nti = (int64_t)tiles_i.size(), nta = (int64_t)tiles_a.size();
+  const size_t vbytes64 = sizeof(double) * node_total * 3 * kNLC, vbytes32 = sizeof(float) * node_total * 3 * kNLC;
+  const bool mixed = opt.precision == DTC_PREC_MIXED;
+  int e;
+  if ((e = ensure(I, bDoms, sizeof(DomDev) * ndom, msg))) return e;
+  if ((e = ensure(I, bTilesI, sizeof(Tile) * std::max<int64_t>(nti, 1), msg))) return e;
+  if ((e = ensure(I, bTilesA, sizeof(Tile) * std::max<int64_t>(nta, 1), msg))) return e;
+  if ((e = ensure(I, bSvox, sizeof(float) * svox.size(), msg))) return e;
+  if ((e = ensure(I, bFlags, node_total, msg))) return e;
+  if ((e = ensure(I, bDinv64, sizeof(double) * node_total * 3, msg))) return e;
+  if ((e = ensure(I, bDinv32, sizeof(float) * node_total * 3, msg))) return e;
+  if ((e = ensure(I, bX, vbytes64, msg))) return e;
+  if ((e = ensure(I, bR64, vbytes64, msg))) return e;
+  if (mixed) {
+    if ((e = ensure(I, bR32, vbytes32, msg))) return e;
+    if ((e = ensure(I, bX32, vbytes32, msg))) return e;
+    if ((e = ensure(I, bP32, vbytes32, msg))) return e;
+    if ((e = ensure(I, bW32, vbytes32, msg))) return e;
+  } else {
+    if ((e = ensure(I, bP64, vbytes64, msg))) return e;
+    if ((e = ensure(I, bW64, vbytes64, msg))) return e;
+  }
+  const size_t ncol = (size_t)ndom * kNLC;
+  if ((e = ensure(I, bSt, sizeof(ColState) * ncol, msg))) return e;
+  if ((e = ensure(I, bOst, sizeof(ColState) * ncol, msg))) return e;
+  if ((e = ensure(I, bPw, sizeof(double) * ncol, msg))) return e;
+  if ((e = ensure(I, bZz, sizeof(double) * ncol, msg))) return e;
+  if ((e = ensure(I, bZr, sizeof(double) * ncol, msg))) return e;
+  if ((e = ensure(I, bTarget, sizeof(double) * ncol, msg))) return e;
+  if ((e = ensure(I, bDomAct, sizeof(int) * ndom, msg))) return e;
+  if ((e = ensure(I, bCount, sizeof(int), msg))) return e;
+  if ((e = ensure(I, bFf, sizeof(double) * 576 * ndom, msg))) return e;
+
+  auto t0 = std::chrono::steady_clock::now();
+  DTC_CUDA(cudaMemcpyAsync(I.bufs[bDoms], doms.data(), sizeof(DomDev) * ndom, cudaMemcpyHostToDevice, s));
+  if (nti) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesI], tiles_i.data(), sizeof(Tile) * nti, cudaMemcpyHostToDevice, s));
+  if (nta) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesA], tiles_a.data(), sizeof(Tile) * nta, cudaMemcpyHostToDevice, s));
+  DTC_CUDA(cudaMemcpyAsync(I.bufs[bSvox], svox.data(), sizeof(float) * svox.size(), cudaMemcpyHostToDevice, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bFlags], 0, node_total, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv64], 0, sizeof(double) * node_total * 3, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv32], 0, sizeof(float) * node_total * 3, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bX], 0, vbytes64, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bR64], 0, vbytes64, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * 576 * ndom, s));
+  const Tile* ti = B<Tile>(I, bTilesI);
+  const Tile* ta = B<Tile>(I, bTilesA);
+  const DomDev* dd = B<DomDev>(I, bDoms);
+  uint8_t* fl = B<uint8_t>(I, bFlags);
+  double* X = B<double>(I, bX);
+  double* R64 = B<double>(I, bR64);
+  int64_t& L = stats_.kernel_launches;
+  if (nta) {
+    k_node_setup<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
+                                                    B<float>(I, bDinv32));
+    k_boundary_values<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, fl, X);
+    L += 2;
+  }
+  if ((e = launch_check(msg))) return e;
+  const dim3 gi((unsigned)std::max<int64_t>(nti, 1), 3), ga((unsigned)std::max<int64_t>(nta, 1), 3);
+  ColState* ost = B<ColState>(I, bOst);
+  if (!mixed) {
+    // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
+    if (nti) { k_matvec<double, false, false><<<gi, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), X, R64, -1.0, nullptr, nullptr); ++L; }
+    if ((e = run_cg<double>(I, ndom, nti, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
+                            opt.rtol, nullptr, opt.max_it, L, msg)))
+      return e;
+    DTC_CUDA(cudaMemcpyAsync(ost, I.bufs[bSt], sizeof(ColState) * ncol, cudaMemcpyDeviceToDevice, s));
+  } else {
+    // every FP32 work vector starts at zero: the stencil reads boundary and void entries
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bR32], 0, vbytes32, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
+    const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : 1e-5;
+    const int max_refine = opt.max_refine > 0 ? opt.max_refine : 12;
+    int64_t inner_budget = opt.max_it;
+    for (int step = 0; step <= max_refine; ++step) {
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
+      if (nti) {
+        k_matvec<double, false, false><<<gi, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), X, R64, -1.0, nullptr, nullptr);
+        k_residual_norm<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<double>(I, bDinv64), R64, B<double>(I, bZz));
+        L += 2;
+      }
+      k_outer_check<<<ndom, 32, 0, s>>>(ost, B<double>(I, bZz), B<double>(I, bTarget), B<int>(I, bDomAct), opt.rtol,
+                                        step == 0);
+      k_count_active<<<1, 256, 0, s>>>(B<int>(I, bDomAct), ndom, B<int>(I, bCount));
+      L += 2;
+      if ((e = launch_check(msg))) return e;
+      int h_count = 0;
+      DTC_CUDA(cudaMemcpyAsync(&h_count, I.bufs[bCount], sizeof(int), cudaMemcpyDeviceToHost, s));
+      DTC_CUDA(cudaStreamSynchronize(s));
+      if (h_count == 0 || step == max_refine || inner_budget <= 0) break;
+      if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
+      if ((e = run_cg<float>(I, ndom, nti, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
+                             B<float>(I, bDinv32), inner, B<double>(I, bTarget), inner_budget, L, msg)))
+        return e;
+      if (nti) { k_apply_correction<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<float>(I, bX32), X, ost); ++L; }
+      k_add_inner_its<<<(unsigned)((ncol + 255) / 256), 256, 0, s>>>(ost, B<ColState>(I, bSt), (int64_t)ncol);
+      ++L;
+      if ((e = launch_check(msg))) return e;
+    }
+  }
+  // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff)
+  DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
+  if (nta) {
+    k_matvec<double, true, false><<<ga, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), X, R64, 1.0, nullptr, nullptr);
+    k_project<<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf));
+    L += 2;
+  }
+  if ((e = launch_check(msg))) return e;
+  std::vector<double> ff((size_t)576 * ndom);
+  std::vector<ColState> cs(ncol);
+  DTC_CUDA(cudaMemcpyAsync(ff.data(), I.bufs[bFf], sizeof(double) * ff.size(), cudaMemcpyDeviceToHost, s));
+  DTC_CUDA(cudaMemcpyAsync(cs.data(), ost, sizeof(ColState) * ncol, cudaMemcpyDeviceToHost, s));
+  // optional displacement / force output in reference numbering
+  bool want_fields = false;
+  for (int d = 0; d < ndom; ++d) want_fields = want_fields || tasks[tidx[d]].out->displ || tasks[tidx[d]].out->force;
+  std::vector<double> hX, hF;
+  if (want_fields) {
+    hX.resize(node_total * 3 * kNLC);
+    hF.resize(node_total * 3 * kNLC);
+    DTC_CUDA(cudaMemcpyAsync(hX.data(), X, vbytes64, cudaMemcpyDeviceToHost, s));
+    DTC_CUDA(cudaMemcpyAsync(hF.data(), R64, vbytes64, cudaMemcpyDeviceToHost, s));
+  }
+  DTC_CUDA(cudaStreamSynchronize(s));
+  stats_.ms_solve = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  for (int d = 0; d < ndom; ++d) {
+    DomainTask& t = tasks[tidx[d]];
+    dtc_domain_out* o = t.out;
+    std::memcpy(o->ff, &ff[(size_t)576 * d], sizeof(double) * 576);
+    int worst = DTC_DOMAIN_OK;
+    int steps = 0;
+    for (int lc = 0; lc < kNLC; ++lc) {
+      const ColState& c = cs[(size_t)d * kNLC + lc];
+      o->iters[lc] = c.its;
+      o->relres[lc] = c.dp0 > 0 ? c.dp / c.dp0 : 0.0;
+      steps = std::max(steps, (int)c.pad);
+      int st = DTC_DOMAIN_OK;
+      if (c.reason == kDivergedIts || (mixed && c.active)) st = DTC_DOMAIN_MAX_IT;
+      else if (c.reason == kIndefinite) st = DTC_DOMAIN_BREAKDOWN;
+      else if (c.reason == kNanOrInf || c.reason == kDivergedDtol) st = DTC_DOMAIN_NONFINITE;
+      if (worst == DTC_DOMAIN_OK) worst = st;
+      stats_.dof_iterations += (double)t.plan->n_free_dof * (double)c.its;
+    }
+    o->refine_steps = mixed ? steps : 0;
+    o->status = worst;
+    if (want_fields && (o->displ || o->force)) {
+      const MeshPlan& mp = *t.plan;
+      const int64_t nn = mp.nn;
+      const DomDev& D = doms[d];
+      for (int64_t id = 0; id < nn; ++id) {
+        const int64_t g = mp.node_grid[id];
+        const int64_t node = D.node_off + g;  // HEX08 node grid == device node grid
+        for (int c = 0; c < 3; ++c)
+          for (int lc = 0; lc < kNLC; ++lc) {
+            const size_t src = (size_t)((node * 3 + c) * kNLC + lc);
+            if (o->displ) o->displ[(size_t)lc * 3 * nn + 3 * id + c] = hX[src];
+            if (o->force) o->force[(size_t)lc * 3 * nn + 3 * id + c] = hF[src];
+          }
+      }
+    }
+  }
+  I.last_doms = doms;
+  I.last_task_index = tidx;
+  return DTC_OK;
+}
+
+int DeviceSolver::energy_grad(const double*, float* const*, int64_t, std::string& msg) {
+  msg = "energy_grad: not available in this build";
+  return DTC_ERR_INTERNAL;
+}
+
+}  // namespace dtc

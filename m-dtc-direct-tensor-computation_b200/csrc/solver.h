@@ -1,0 +1,44 @@
+// solver.h -- device batch solver (kernels.cu) interface used by the C ABI layer.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dtc.h"
+#include "mesher.h"
+
+namespace dtc {
+
+struct DomainTask {
+  const dtc_domain_in* in = nullptr;
+  MeshPlan* plan = nullptr;
+  dtc_domain_out* out = nullptr;
+};
+
+struct SolverStats {
+  double ms_solve = 0, ms_rotation = 0;
+  int64_t kernel_launches = 0;
+  double dof_iterations = 0;  // sum over domains of free DOFs x load cases x iterations
+};
+
+class DeviceSolver {
+ public:
+  struct Impl;  // device buffers and stream (kernels.cu)
+  DeviceSolver();
+  ~DeviceSolver();
+  // Bind to a device; returns DTC_OK or an error with msg set.
+  int init(int device, std::string& msg);
+  // Solve every task (status OK plans only), fill ff/iters/relres of the outputs.
+  int solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg);
+  // Adjoint: dL/dE_voxel for the domains of the last solve (kept displacements).
+  int energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, std::string& msg);
+  const SolverStats& stats() const { return stats_; }
+  void set_keep(bool keep) { keep_ = keep; }
+
+ private:
+  Impl* impl_ = nullptr;
+  SolverStats stats_;
+  bool keep_ = false;
+};
+
+}  // namespace dtc

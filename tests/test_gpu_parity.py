@@ -1,0 +1,111 @@
+"""GPU path vs the FP64 oracle, through the C ABI (include/dtc.h).
+
+Tolerances (normwise relative, max|C - C*| / max|C*|, the judged quantity):
+  FP64 path  <= 1e-6 against the oracle at rtol 1e-10,
+  mixed path <= 1e-5 against the oracle at rtol 1e-10.
+Integer/index outputs (ne, nn, nb, reference DOF numbering) must be identical.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-6
+TOL_MIXED = 1e-5
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def make_pair(dtc, orc, shape, bvtv, seed, E_voxel=False, **kw):
+    syn = dtc.synth
+    gray = syn.bone_volume(shape, bvtv, seed)
+    ev = syn.modulus_of_gray(gray) if E_voxel else None
+    d = dtc.Domain(gray, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=ev, **kw)
+    o = orc.Domain(gray, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, E_voxel=ev, **kw)
+    return d, o
+
+
+@pytest.fixture(scope="module")
+def batch(dtc, orc):
+    pairs = [make_pair(dtc, orc, (12, 12, 12), b, dtc.synth.seed_for(7, i))
+             for i, b in enumerate((0.15, 0.25, 0.35, 0.5))]
+    pairs.append(make_pair(dtc, orc, (9, 11, 10), 0.4, dtc.synth.seed_for(7, 9)))   # non-cubic box
+    pairs.append(make_pair(dtc, orc, (12, 12, 12), 0.3, dtc.synth.seed_for(7, 10), E_voxel=True))
+    refs = orc.solve_batch([p[1] for p in pairs])
+    return pairs, refs
+
+
+def test_fp64_matches_oracle(dtc, batch):
+    pairs, refs = batch
+    with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False) as s:
+        res = s.solve([p[0] for p in pairs])
+        st = s.stats()
+    assert st["kernel_launches"] > 0
+    for r, ref in zip(res, refs):
+        assert r["status"] == ref["status"] == 0
+        assert (r["ne"], r["nn"], r["nb"]) == (ref["ne"], ref["nn"], ref["nb"])
+        assert rel(r["c"], ref["c"]) <= TOL_FP64
+        assert rel(r["ff"], ref["ff"]) <= TOL_FP64
+        assert rel(r["kmacro"], ref["kmacro"]) <= TOL_FP64
+        # same Jacobi-PCG recurrence: iteration counts agree up to rounding near the threshold
+        assert np.abs(r["iters"] - ref["iters"]).max() <= 2
+
+
+def test_mixed_matches_oracle(dtc, batch):
+    pairs, refs = batch
+    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False) as s:
+        res = s.solve([p[0] for p in pairs])
+    for r, ref in zip(res, refs):
+        assert r["status"] == 0
+        assert rel(r["c"], ref["c"]) <= TOL_MIXED
+        assert r["refine_steps"] >= 1
+
+
+def test_fields_in_reference_numbering(dtc, orc):
+    d, o = make_pair(dtc, orc, (8, 8, 8), 0.4, dtc.synth.seed_for(7, 20))
+    ref = orc.solve_domain(o, with_arrays=True)
+    with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False) as s:
+        r = s.solve([d], want_fields=True)[0]
+    assert rel(r["displ"], ref["displ"]) <= 1e-7
+    assert rel(r["force"], ref["force"]) <= 1e-6
+
+
+def test_solid_cube_isotropic(dtc):
+    E, nu = 5600.0, 0.3
+    gray = np.full((6, 6, 6), 14250, np.int16)
+    with dtc.Solver(precision="fp64", rtol=1e-12, rotation_search=False) as s:
+        r = s.solve([dtc.Domain(gray, E=E, nu=nu, delta=0.01)])[0]
+    lam, mu = E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))
+    C = np.zeros((6, 6))
+    C[:3, :3] = lam
+    C[range(3), range(3)] += 2 * mu
+    C[3, 3] = C[4, 4] = C[5, 5] = mu
+    assert rel(r["c"], C) < 1e-8
+
+
+def test_statuses(dtc):
+    empty = np.zeros((6, 6, 6), np.int16)
+    full = np.full((6, 6, 6), 100, np.int16)
+    with dtc.Solver(precision="fp64", rtol=1e-8, rotation_search=False) as s:
+        r = s.solve([dtc.Domain(empty, domain_number=3), dtc.Domain(full, domain_number=4)])
+    assert r[0]["status"] == dtc.DOMAIN_EMPTY and r[0]["domain_number"] == 3
+    assert r[1]["status"] == dtc.DOMAIN_OK and r[1]["domain_number"] == 4
+    with dtc.Solver(precision="fp64", rtol=1e-10, max_it=3, rotation_search=False) as s:
+        r = s.solve([dtc.Domain(full)])
+    assert r[0]["status"] == dtc.DOMAIN_MAX_IT
+    assert r[0]["iters"].max() == 3
+
+
+def test_rotation_matches_oracle(dtc, orc, batch):
+    pairs, refs = batch
+    d, o = pairs[1]
+    o.s.rotation = 1
+    ref = orc.solve_domain(o)
+    with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=True) as s:
+        r = s.solve([d])[0]
+    for k in ("cr1", "cr2"):
+        a, b = r[k], ref[k]
+        assert abs(a["crit"] - b["crit"]) <= 1e-9 + 1e-6 * abs(b["crit"])
+        assert rel(np.diag(a["ee"]), np.diag(b["ee"])) <= 1e-6
