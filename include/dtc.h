@@ -157,6 +157,11 @@ dtc_status dtc_solve_batch(dtc_handle* handle, const dtc_domain_in* in, int64_t 
  * generate_boundaries).  Needs no device. */
 dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out);
 
+/* Host-only: element stiffness matrix of one voxel element, column-major (3*elem_type)^2,
+ * node order of the mesher.  Mirrors Hexe08 / Hexe20 (f-src/mod_linfe.f90:161-776,
+ * 890-4509), which tabulate it for a cube of edge a = phdsize(1)*delta(1) and modulus E. */
+dtc_status dtc_element_stiffness(int32_t elem_type, double E, double a, double nu, double* ke);
+
 /* Adjoint of the last dtc_solve_batch on this handle (which must have run with
  * keep_displacements = 1 and E_voxel given): for each domain i, dL/dE_voxel given
  * dL/dC = dloss_dc[36*i .. 36*i+35] (column-major 6x6, C = out.c).  Writes

@@ -17,7 +17,7 @@ from . import capi, synth
 from .capi import (DOMAIN_BREAKDOWN, DOMAIN_EMPTY, DOMAIN_FEW_NODES, DOMAIN_MAX_IT, DOMAIN_NO_STRUCTURE,
                    DOMAIN_NONFINITE, DOMAIN_OK, HEX08, HEX20, PREC_FP64, PREC_MIXED, DTCError)
 
-__all__ = ["Domain", "Solver", "mesh_domain", "solve_batch", "DTCError", "HEX08", "HEX20",
+__all__ = ["Domain", "Solver", "mesh_domain", "element_stiffness", "solve_batch", "DTCError", "HEX08", "HEX20",
            "DOMAIN_OK", "DOMAIN_EMPTY", "DOMAIN_NO_STRUCTURE", "DOMAIN_FEW_NODES", "DOMAIN_MAX_IT",
            "DOMAIN_BREAKDOWN", "DOMAIN_NONFINITE"]
 
@@ -156,6 +156,16 @@ class Solver:
 def solve_batch(domains, want_fields=False, **options):
     with Solver(**options) as s:
         return s.solve(domains, want_fields=want_fields)
+
+
+def element_stiffness(elem_type, E, a, nu):
+    """Voxel element stiffness (Hexe08 / Hexe20 of the reference), (3n x 3n) float64."""
+    nd = 3 * elem_type
+    ke = np.zeros((nd, nd), order="F")
+    rc = capi.load().dtc_element_stiffness(elem_type, E, a, nu, ke.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != capi.DTC_OK:
+        raise DTCError(rc, "dtc_element_stiffness failed")
+    return ke
 
 
 def mesh_domain(domain):

@@ -75,6 +75,7 @@ SIGNATURES = {
     "dtc_mesh_domain": (C.c_int, [C.POINTER(DomainIn), C.POINTER(MeshOut)]),
     "dtc_energy_grad": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.POINTER(C.c_float)), C.c_int64]),
     "dtc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
+    "dtc_element_stiffness": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "dtc_last_error": (C.c_char_p, [C.c_void_p]),
 }
 

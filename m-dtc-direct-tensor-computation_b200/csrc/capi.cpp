@@ -272,6 +272,15 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
   return DTC_OK;
 }
 
+dtc_status dtc_element_stiffness(int32_t elem_type, double E, double a, double nu, double* ke) {
+  if (!ke || (elem_type != DTC_HEX08 && elem_type != DTC_HEX20) || !(a > 0) || !(nu > -1.0 && nu < 0.5))
+    return DTC_ERR_INVALID_ARGUMENT;
+  const int nd = 3 * elem_type;
+  voxel_stiffness(elem_type, nu, ke);
+  for (int i = 0; i < nd * nd; ++i) ke[i] *= E * a;
+  return DTC_OK;
+}
+
 dtc_status dtc_energy_grad(dtc_handle* h, const double* dloss_dc, float* const* grad_e, int64_t n) {
   if (!h || !dloss_dc || !grad_e || n < 0) return DTC_ERR_INVALID_ARGUMENT;
   return (dtc_status)h->solver.energy_grad(dloss_dc, grad_e, n, h->err);
