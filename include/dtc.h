@@ -65,14 +65,19 @@ typedef struct dtc_options {
                               the reference's PETSc option -ksp_rtol (f-src/mod_parameters.f90:31) */
   int64_t max_it;          /* CG iteration cap per load case (-ksp_max_it, :32); for the mixed
                               path the cap on the summed inner iterations */
-  double inner_rtol;       /* mixed path: reduction asked of each FP32 inner solve (0 -> 1e-5) */
+  double inner_rtol;       /* mixed path: reduction asked of each FP32 inner solve
+                              (0 -> max(0.3 rtol, 1e-7)) */
   int32_t max_refine;      /* mixed path: cap on FP64 refinement steps (0 -> 12) */
   int32_t rotation_search; /* 1: run the CR1/CR2 rotation search (mod_struct_calcmat.f90:533-1603) */
   int32_t device;          /* CUDA device ordinal */
   int32_t host_threads;    /* threads for host-side meshing (0 -> hardware concurrency) */
   int32_t keep_displacements; /* 1: keep the converged displacements on the device for
                                  dtc_energy_grad (the adjoint); 0: release them */
-  int32_t reserved[8];
+  int32_t profile_kernels; /* 1: time every solver kernel with CUDA events on its stream
+                              (dtc_get_kernel_stats); adds event records, off for production */
+  int32_t mixed_matvec;    /* stiffness contraction of the FP32 inner solve: 0 = SIMT FP32,
+                              1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy) */
+  int32_t reserved[6];
 } dtc_options;
 
 typedef struct dtc_domain_in {
@@ -175,6 +180,20 @@ dtc_status dtc_energy_grad(dtc_handle* handle, const double* dloss_dc, float* co
  * kernels launched, and sum over domains of free DOFs x load cases x CG iterations. */
 dtc_status dtc_get_stats(const dtc_handle* handle, double* ms_solve, int64_t* kernel_launches,
                          double* dof_iterations);
+
+/* Per kernel class of the last dtc_solve_batch (filled when profile_kernels = 1): launches,
+ * summed CUDA-event time, and the algorithmic bytes / flops of one average launch. */
+typedef struct dtc_kernel_stats {
+  char name[32];
+  int64_t launches;
+  double ms_total;
+  double bytes_per_launch;
+  double flops_per_launch;
+} dtc_kernel_stats;
+
+/* Copies up to cap entries; *count receives the number of kernel classes. */
+dtc_status dtc_get_kernel_stats(const dtc_handle* handle, dtc_kernel_stats* out, int32_t cap,
+                                int32_t* count);
 
 /* Message describing the last error on this handle (never NULL). */
 const char* dtc_last_error(const dtc_handle* handle);

@@ -91,8 +91,9 @@ def _result(o, fields):
 class Solver:
     """A handle on one GPU (dtc_create / dtc_destroy)."""
 
-    def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=1e-5, max_refine=12,
-                 rotation_search=True, device=0, host_threads=0, keep_displacements=False):
+    def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=0.0, max_refine=12,
+                 rotation_search=True, device=0, host_threads=0, keep_displacements=False,
+                 profile_kernels=False, mixed_matvec="simt"):
         self.lib = capi.load()
         o = capi.Options()
         self.lib.dtc_default_options(C.byref(o))
@@ -100,6 +101,8 @@ class Solver:
         o.rtol, o.max_it, o.inner_rtol, o.max_refine = float(rtol), int(max_it), float(inner_rtol), int(max_refine)
         o.rotation_search, o.device, o.host_threads = int(bool(rotation_search)), int(device), int(host_threads)
         o.keep_displacements = int(bool(keep_displacements))
+        o.profile_kernels = int(bool(profile_kernels))
+        o.mixed_matvec = {"simt": 0, "tensor": 1}[mixed_matvec]
         self.options = o
         h = C.c_void_p()
         rc = self.lib.dtc_create(C.byref(h), C.byref(o))
@@ -144,6 +147,16 @@ class Solver:
         ms, launches, dofit = C.c_double(), C.c_int64(), C.c_double()
         self._check(self.lib.dtc_get_stats(self.handle, C.byref(ms), C.byref(launches), C.byref(dofit)))
         return {"ms_solve": ms.value, "kernel_launches": launches.value, "dof_iterations": dofit.value}
+
+    def kernel_stats(self):
+        """Per kernel class: launches, CUDA-event ms, algorithmic bytes/flops per launch."""
+        buf = (capi.KernelStats * 32)()
+        cnt = C.c_int32()
+        self._check(self.lib.dtc_get_kernel_stats(self.handle, buf, 32, C.byref(cnt)))
+        return {buf[i].name.decode(): {"launches": buf[i].launches, "ms_total": buf[i].ms_total,
+                                       "bytes_per_launch": buf[i].bytes_per_launch,
+                                       "flops_per_launch": buf[i].flops_per_launch}
+                for i in range(cnt.value)}
 
     def energy_grad(self, dloss_dc, grads):
         """dL/dE_voxel of the last solve; grads: list of float32 arrays shaped like phi."""

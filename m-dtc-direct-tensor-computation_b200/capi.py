@@ -25,7 +25,8 @@ class Options(C.Structure):
         ("abi_version", C.c_int32), ("precision", C.c_int32), ("rtol", C.c_double),
         ("max_it", C.c_int64), ("inner_rtol", C.c_double), ("max_refine", C.c_int32),
         ("rotation_search", C.c_int32), ("device", C.c_int32), ("host_threads", C.c_int32),
-        ("keep_displacements", C.c_int32), ("reserved", C.c_int32 * 8),
+        ("keep_displacements", C.c_int32), ("profile_kernels", C.c_int32),
+        ("mixed_matvec", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -55,6 +56,11 @@ class DomainOut(C.Structure):
     ]
 
 
+class KernelStats(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("ms_total", C.c_double),
+                ("bytes_per_launch", C.c_double), ("flops_per_launch", C.c_double)]
+
+
 class MeshOut(C.Structure):
     _fields_ = [
         ("ne", C.c_int64), ("nn", C.c_int64), ("nb", C.c_int64),
@@ -76,6 +82,7 @@ SIGNATURES = {
     "dtc_energy_grad": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.POINTER(C.c_float)), C.c_int64]),
     "dtc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "dtc_element_stiffness": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "dtc_get_kernel_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStats), C.c_int32, C.POINTER(C.c_int32)]),
     "dtc_last_error": (C.c_char_p, [C.c_void_p]),
 }
 

@@ -116,7 +116,7 @@ void dtc_default_options(dtc_options* opt) {
   opt->precision = DTC_PREC_FP64;
   opt->rtol = 1e-3;       // -ksp_rtol 1.e-03 (f-src/mod_parameters.f90:31)
   opt->max_it = 500000;   // -ksp_max_it 500000 (:32)
-  opt->inner_rtol = 1e-5;
+  opt->inner_rtol = 0.0;   // automatic: max(0.3 rtol, 1e-7)
   opt->max_refine = 12;
   opt->rotation_search = 1;
   opt->device = 0;
@@ -243,9 +243,17 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     }
     int rc = h->solver.solve(chunk, h->opt, in[0].nu, h->err);
     if (rc != DTC_OK) return (dtc_status)rc;
-    h->last.ms_solve += h->solver.stats().ms_solve;
-    h->last.kernel_launches += h->solver.stats().kernel_launches;
-    h->last.dof_iterations += h->solver.stats().dof_iterations;
+    const SolverStats& ss = h->solver.stats();
+    h->last.ms_solve += ss.ms_solve;
+    h->last.kernel_launches += ss.kernel_launches;
+    h->last.dof_iterations += ss.dof_iterations;
+    for (int c = 0; c < kcNumClasses; ++c) {
+      h->last.kc[c].name = ss.kc[c].name;
+      h->last.kc[c].launches += ss.kc[c].launches;
+      h->last.kc[c].ms += ss.kc[c].ms;
+      h->last.kc[c].bytes += ss.kc[c].bytes;
+      h->last.kc[c].flops += ss.kc[c].flops;
+    }
   }
   std::vector<const double*> ees;
   std::vector<dtc_domain_out*> rot_out;
@@ -269,6 +277,26 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
       finish_rotation(ees[d], 2, &ang[6 * d + 3], jj[2 * d + 1], crit[2 * d + 1], rot_out[d]);
     }
   }
+  return DTC_OK;
+}
+
+dtc_status dtc_get_kernel_stats(const dtc_handle* h, dtc_kernel_stats* out, int32_t cap, int32_t* count) {
+  if (!h || (cap > 0 && !out)) return DTC_ERR_INVALID_ARGUMENT;
+  int32_t n = 0;
+  for (int c = 0; c < kcNumClasses; ++c) {
+    const KernelClass& k = h->last.kc[c];
+    if (k.launches == 0) continue;
+    if (n < cap) {
+      std::memset(&out[n], 0, sizeof(out[n]));
+      std::strncpy(out[n].name, k.name, sizeof(out[n].name) - 1);
+      out[n].launches = k.launches;
+      out[n].ms_total = k.ms;
+      out[n].bytes_per_launch = k.bytes / (double)k.launches;
+      out[n].flops_per_launch = k.flops / (double)k.launches;
+    }
+    ++n;
+  }
+  if (count) *count = n;
   return DTC_OK;
 }
 

@@ -117,10 +117,10 @@ __global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ ti
                                                      T* __restrict__ y, double scale, double* __restrict__ acc,
                                                      const int* __restrict__ dom_active) {
   __shared__ double red[32];
-  const Tile t = tiles[blockIdx.x];
+  const Tile t = tiles[blockIdx.x / 3];
   if (dom_active && !dom_active[t.dom]) return;
   const DomDev D = doms[t.dom];
-  const int lc = blockIdx.y * kLcGroup + (threadIdx.x & 7);
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
   const int row = threadIdx.x >> 3;
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   const int lo = ALL ? 0 : 1;
@@ -252,10 +252,10 @@ __global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __rest
 // -------------------------------------------------------------------------------------
 // CG vector kernels on interior tiles; lane = load case, row = (y,z), sweep x.
 #define DTC_TILE_PROLOGUE                                                      \
-  const Tile t = tiles[blockIdx.x];                                            \
+  const Tile t = tiles[blockIdx.x / 3];                                        \
   if (dom_active && !dom_active[t.dom]) return;                                \
   const DomDev D = doms[t.dom];                                                \
-  const int lc = blockIdx.y * kLcGroup + (threadIdx.x & 7);                    \
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);              \
   const int row = threadIdx.x >> 3;                                            \
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);                     \
   const bool rowok = yy >= 1 && yy <= D.L[1] - 1 && zz >= 1 && zz <= D.L[2] - 1; \
@@ -561,9 +561,9 @@ __global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ t
                                                      const uint8_t* __restrict__ flags, const double* __restrict__ F,
                                                      double* __restrict__ ff) {
   __shared__ double part[16][8][25];
-  const Tile t = tiles[blockIdx.x];
+  const Tile t = tiles[blockIdx.x / 3];
   const DomDev D = doms[t.dom];
-  const int lcl = threadIdx.x & 7, lc = blockIdx.y * kLcGroup + lcl;
+  const int lcl = threadIdx.x & 7, lc = (blockIdx.x % 3) * kLcGroup + lcl;
   const int row = threadIdx.x >> 3;
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   double acc[24];
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ t
     const int l8 = j / 24, k = j % 24;
     double s = 0.0;
     for (int r2 = 0; r2 < 16; ++r2) s += part[r2][l8][k];
-    const int lcg = blockIdx.y * kLcGroup + l8;
+    const int lcg = (blockIdx.x % 3) * kLcGroup + l8;
     atomicAdd(ff + (int64_t)t.dom * 576 + k + 24 * lcg, s);
   }
 }
@@ -610,12 +610,51 @@ struct DeviceSolver::Impl {
   // last solve kept for the adjoint
   std::vector<DomDev> last_doms;
   std::vector<int64_t> last_task_index;
+  bool tensor_matvec = false;   // FP32 inner solve on tcgen05
+  // kernel profiling with CUDA events (opt-in)
+  bool profile = false;
+  std::vector<cudaEvent_t> ev;
+  std::vector<std::pair<int, int>> pending;   // (class, event pair index)
+  std::vector<double> dom_mv_bytes, dom_mv_flops, dom_vec_bytes;  // per domain, per launch
+  std::vector<int> h_active;                  // domains active at the last chunk boundary
+  SolverStats* stats = nullptr;
+  int begin(int /*cls*/) {
+    if (!profile) return -1;
+    const int k = (int)pending.size();
+    while ((int)ev.size() < 2 * (k + 1)) { cudaEvent_t e; cudaEventCreate(&e); ev.push_back(e); }
+    cudaEventRecord(ev[2 * k], stream);
+    return k;
+  }
+  void end(int cls, int k, double bytes, double flops) {
+    if (k < 0) return;
+    cudaEventRecord(ev[2 * k + 1], stream);
+    pending.push_back({cls, k});
+    stats->kc[cls].bytes += bytes;
+    stats->kc[cls].flops += flops;
+  }
+  void flush() {
+    if (!profile || pending.empty()) return;
+    cudaStreamSynchronize(stream);
+    for (auto& pr : pending) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[2 * pr.second], ev[2 * pr.second + 1]);
+      stats->kc[pr.first].ms += ms;
+      stats->kc[pr.first].launches += 1;
+    }
+    pending.clear();
+  }
+  // algorithmic traffic of one launch over the domains active at the last chunk boundary
+  double active_sum(const std::vector<double>& per_dom) const {
+    double t = 0;
+    for (size_t d = 0; d < per_dom.size(); ++d) if (h_active.empty() || h_active[d]) t += per_dom[d];
+    return t;
+  }
 };
 
 namespace {
 
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
-           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bNumBufs };
+           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bNumBufs };
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
   if (I.caps[which] >= bytes && I.bufs[which]) return DTC_OK;
@@ -640,6 +679,7 @@ DeviceSolver::DeviceSolver() : impl_(new Impl) {}
 DeviceSolver::~DeviceSolver() {
   if (impl_) {
     if (impl_->device >= 0) cudaSetDevice(impl_->device);
+    for (cudaEvent_t e : impl_->ev) cudaEventDestroy(e);
     for (int i = 0; i < 32; ++i) if (impl_->bufs[i]) cudaFree(impl_->bufs[i]);
     if (impl_->stream) cudaStreamDestroy(impl_->stream);
     delete impl_;
@@ -655,6 +695,11 @@ int DeviceSolver::init(int device, std::string& msg) {
   impl_->device = device;
   return DTC_OK;
 }
+
+void launch_matvec_tc(const Tile* tiles, int64_t ntiles, const DomDev* doms, const float* svox,
+                      const uint8_t* flags, const float* u, float* y, double* acc_pw, const int* dom_active, int* err,
+                      cudaStream_t s);
+int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg);
 
 namespace {
 
@@ -672,7 +717,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
   double* zr = B<double>(I, bZr);
   int* act = B<int>(I, bDomAct);
   int* cnt = B<int>(I, bCount);
-  const dim3 grid((unsigned)nti, 3);
+  const dim3 grid((unsigned)(3 * nti));
   DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
@@ -683,21 +728,43 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
   const int chunk = 32;
   int h_count = 1;
   for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
+    const bool f32 = sizeof(T) == 4;
+    const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(T) : 0;
+    const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(T) : 0;
+    const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
     for (int k = 0; k < chunk; ++k) {
       if (nti > 0) {
+        int q = I.begin(0);
         k_direction<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
-        k_matvec<T, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+        I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
+        q = I.begin(0);
+        if (sizeof(T) == 4 && I.tensor_matvec)
+          launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
+                           B<int>(I, bErr), s);
+        else
+          k_matvec<T, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+        I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
+        q = I.begin(0);
         k_update<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
+        I.end(f32 ? kcUpdate32 : kcUpdate64, q, 6 * vb, 0);
       }
+      int q = I.begin(0);
       k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+      I.end(kcColstate, q, 0, 0);
       launches += 4;
     }
     k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
     launches += 1;
     if (int e = launch_check(msg)) return e;
     DTC_CUDA(cudaMemcpyAsync(&h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (I.profile) {
+      I.h_active.resize(ndom);
+      DTC_CUDA(cudaMemcpyAsync(I.h_active.data(), act, sizeof(int) * ndom, cudaMemcpyDeviceToHost, s));
+    }
     DTC_CUDA(cudaStreamSynchronize(s));
+    I.flush();
   }
+  I.h_active.clear();
   return DTC_OK;
 }
 
@@ -708,6 +775,16 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   DTC_CUDA(cudaSetDevice(I.device));
   cudaStream_t s = I.stream;
   stats_ = SolverStats();
+  static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
+                                             "direction_f32", "direction_f64", "colstate", "reaction_f64",
+                                             "project_f64"};
+  for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
+  I.stats = &stats_;
+  I.profile = opt.profile_kernels != 0;
+  I.tensor_matvec = opt.mixed_matvec == 1;
+  I.pending.clear();
+  I.h_active.clear();
+  I.dom_mv_bytes.clear(); I.dom_mv_flops.clear(); I.dom_vec_bytes.clear();
   // constant tables
   {
     double kh[576];
@@ -719,6 +796,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat64, kh, sizeof(kh), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
+    if (int e = upload_tc_operand(kh, s, msg)) return e;
   }
   // pack the batch (all solvable tasks at once; chunking by memory happens in the caller)
   std::vector<DomDev> doms;
@@ -757,6 +835,26 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
       for (int c = 0; c < 2; ++c)
         for (int b = 0; b < 2; ++b)
           for (int a2 = 0; a2 < 2; ++a2) act[(vx + a2) + (size_t)nx * ((vy + b) + (size_t)ny * (vz + c))] = 1;
+    }
+    // algorithmic work of one launch on this domain (elements of T per vector; flops):
+    // vector kernels touch 72 values per active interior node per vector; the matvec reads
+    // p and writes w (2 vectors) plus one float per voxel; its flops are, per active
+    // interior node and load case, 150 per kept neighbouring voxel (3 rows x 24 FMA + scale).
+    {
+      double nint = 0, kv = 0;
+      for (int z = 1; z < nz - 1; ++z)
+        for (int y = 1; y < ny - 1; ++y)
+          for (int x = 1; x < nx - 1; ++x) {
+            if (!act[x + (size_t)nx * (y + (size_t)ny * z)]) continue;
+            nint += 1;
+            for (int c = 0; c < 2; ++c)
+              for (int b = 0; b < 2; ++b)
+                for (int a2 = 0; a2 < 2; ++a2)
+                  kv += sv[(x - 1 + a2) + in.L[0] * ((y - 1 + b) + in.L[1] * (int64_t)(z - 1 + c))] != 0.0f;
+          }
+      I.dom_vec_bytes.push_back(72.0 * nint);
+      I.dom_mv_bytes.push_back(2 * 72.0 * nint + (double)nvox * 4.0 / 4.0);
+      I.dom_mv_flops.push_back(kv * 150.0 * kNLC);
     }
     auto tile_active = [&](int x0, int y0, int z0, int lo, int hx, int hy, int hz) {
       for (int z = z0; z < std::min(z0 + kTileZ, hz + 1); ++z)
@@ -813,6 +911,8 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   if ((e = ensure(I, bDomAct, sizeof(int) * ndom, msg))) return e;
   if ((e = ensure(I, bCount, sizeof(int), msg))) return e;
   if ((e = ensure(I, bFf, sizeof(double) * 576 * ndom, msg))) return e;
+  if ((e = ensure(I, bErr, sizeof(int), msg))) return e;
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bErr], 0, sizeof(int), s));
 
   auto t0 = std::chrono::steady_clock::now();
   DTC_CUDA(cudaMemcpyAsync(I.bufs[bDoms], doms.data(), sizeof(DomDev) * ndom, cudaMemcpyHostToDevice, s));
@@ -839,7 +939,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     L += 2;
   }
   if ((e = launch_check(msg))) return e;
-  const dim3 gi((unsigned)std::max<int64_t>(nti, 1), 3), ga((unsigned)std::max<int64_t>(nta, 1), 3);
+  const dim3 gi((unsigned)(3 * std::max<int64_t>(nti, 1))), ga((unsigned)(3 * std::max<int64_t>(nta, 1)));
   ColState* ost = B<ColState>(I, bOst);
   if (!mixed) {
     // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
@@ -855,7 +955,8 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     DTC_CUDA(cudaMemsetAsync(I.bufs[bR32], 0, vbytes32, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
-    const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : 1e-5;
+    // inner FP32 solves aim straight at the outer target when FP32 can reach it
+    const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);
     const int max_refine = opt.max_refine > 0 ? opt.max_refine : 12;
     int64_t inner_budget = opt.max_it;
     for (int step = 0; step <= max_refine; ++step) {
@@ -907,7 +1008,11 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     DTC_CUDA(cudaMemcpyAsync(hX.data(), X, vbytes64, cudaMemcpyDeviceToHost, s));
     DTC_CUDA(cudaMemcpyAsync(hF.data(), R64, vbytes64, cudaMemcpyDeviceToHost, s));
   }
+  int h_err = 0;
+  DTC_CUDA(cudaMemcpyAsync(&h_err, I.bufs[bErr], sizeof(int), cudaMemcpyDeviceToHost, s));
   DTC_CUDA(cudaStreamSynchronize(s));
+  I.flush();
+  if (h_err) { msg = "tensor-core matvec: an mbarrier wait timed out"; return DTC_ERR_INTERNAL; }
   stats_.ms_solve = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   for (int d = 0; d < ndom; ++d) {
     DomainTask& t = tasks[tidx[d]];

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 
+#include "../../include/dtc.h"
 #include "dtc_internal.h"
 
 namespace dtc {

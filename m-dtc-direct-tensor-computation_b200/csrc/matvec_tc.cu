@@ -1,0 +1,322 @@
+// matvec_tc.cu -- the voxel stiffness contraction on the 5th-generation tensor cores (sm_100a).
+//
+// w = K p on the interior nodes of one tile (8 x 4 x 4 owned nodes) for one group of 8 load
+// cases.  Every kept voxel v adjacent to an owned node contributes s_v * Khat * p_v, where
+// p_v holds the 24 DOFs of its 8 corners.  Per round the CTA stacks 16 voxels x 8 load cases
+// as the 128 rows of A (K = 24 voxel DOFs), multiplies by B = Khat (N = 24 output DOFs,
+// padded to 32) with tcgen05.mma kind::tf32 into a 128 x 32 FP32 accumulator in tensor
+// memory, reads it back with tcgen05.ld and adds s_v * D into shared-memory node
+// accumulators (only owned nodes are kept, so voxels on the tile rim are evaluated by every
+// tile they touch and no global atomics are needed).
+//
+// Precision: FP32 operands are split into tf32 hi + lo parts and the product is formed as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi (nine K=8 MMAs per round), which recovers FP32-level
+// accuracy; accumulation is FP32 in TMEM.
+//
+// Waits: the one mbarrier wait per round is bounded; on time-out the kernel records an
+// error code, waits (bounded) for its own MMAs, frees its tensor memory and returns.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "../../include/dtc.h"
+#include "kernels.cuh"
+
+namespace dtc {
+
+namespace tc {
+
+constexpr int kRows = 128;                 // M: 16 voxels x 8 load cases
+constexpr int kVoxPerRound = 16;
+constexpr int kK = 24, kN = 32, kKc = 8;   // voxel DOFs, padded output DOFs, K per MMA
+constexpr int kMaxVox = 9 * 5 * 5;         // voxels adjacent to an 8 x 4 x 4 node tile
+constexpr int kAChunkBytes = kRows * kKc * 4;   // 4 KB: one K-chunk of A in canonical layout
+constexpr int kBChunkBytes = kN * kKc * 4;      // 1 KB
+constexpr uint32_t kTmemCols = 32;
+constexpr long long kSpinLimit = 1ll << 26;
+
+// Canonical K-major, no-swizzle layout of a (rows x 8) tf32 chunk: 8-row x 16-byte core
+// matrices; the two K-halves of a row group are LBO = 128 B apart, row groups SBO = 256 B.
+__host__ __device__ constexpr int canon_offset(int r, int k) {
+  return (r & 7) * 16 + (r >> 3) * 256 + ((k >> 2) & 1) * 128 + (k & 3) * 4;
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+  d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;      // leading byte offset (K direction)
+  d |= (uint64_t)((256 >> 4) & 0x3FFF) << 32;      // stride byte offset (M/N direction)
+  d |= (uint64_t)1 << 46;                           // descriptor version (sm100)
+  // base offset 0, lbo mode 0, layout type 0 = SWIZZLE_NONE
+  return d;
+}
+
+// instruction descriptor: D f32, A/B tf32, both K-major, N = 32, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kRows >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+}  // namespace tc
+
+// Khat split into tf32 hi / lo, laid out as 6 canonical B chunks (hi k0..2, lo k0..2).
+__constant__ float c_bsplit[6 * tc::kN * tc::kKc];
+
+__global__ void __launch_bounds__(128, 4)
+    k_matvec_tc(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms, const float* __restrict__ svox,
+                const uint8_t* __restrict__ flags, const float* __restrict__ u, float* __restrict__ y,
+                double* __restrict__ acc_pw, const int* __restrict__ dom_active, int* __restrict__ err) {
+  using namespace tc;
+  __shared__ __align__(1024) unsigned char sA[2 * 3 * kAChunkBytes];   // 24 KB: hi chunks, lo chunks
+  __shared__ __align__(1024) unsigned char sB[6 * kBChunkBytes];       // 6 KB
+  __shared__ float acc[128 * 3 * 8];                                    // owned node x comp x lc
+  __shared__ int vlist[kMaxVox];
+  __shared__ float vscale[kMaxVox];
+  __shared__ int wcount[4];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int fail;
+  __shared__ double red[32];
+
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = blockIdx.x % 3;  // load-case group: the three groups of a tile run back to back
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  for (int i = tid; i < 6 * kN * kKc; i += 128) reinterpret_cast<float*>(sB)[i] = c_bsplit[i];
+  for (int i = tid; i < 128 * 3 * 8; i += 128) acc[i] = 0.0f;
+
+  // kept voxels adjacent to the owned nodes, deterministic order
+  const int L0 = D.L[0], L1 = D.L[1], L2 = D.L[2];
+  int nv = 0;
+  for (int base = 0; base < kMaxVox; base += 128) {
+    const int q = base + tid;
+    int vidx = -1;
+    float sv = 0.0f;
+    if (q < kMaxVox) {
+      const int ix = q % 9, iy = (q / 9) % 5, iz = q / 45;
+      const int vx = t.x0 - 1 + ix, vy = t.y0 - 1 + iy, vz = t.z0 - 1 + iz;
+      if (vx >= 0 && vy >= 0 && vz >= 0 && vx < L0 && vy < L1 && vz < L2) {
+        const int64_t o = vx + (int64_t)L0 * (vy + (int64_t)L1 * vz);
+        sv = __ldg(svox + D.vox_off + o);
+        if (sv != 0.0f) vidx = vx + L0 * (vy + L1 * vz);
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, vidx >= 0);
+    if (lane == 0) wcount[warp] = __popc(m);
+    __syncthreads();
+    int off = nv;
+    for (int w2 = 0; w2 < warp; ++w2) off += wcount[w2];
+    if (vidx >= 0) {
+      const int pos = off + __popc(m & ((1u << lane) - 1));
+      vlist[pos] = vidx;
+      vscale[pos] = sv;
+    }
+    nv += wcount[0] + wcount[1] + wcount[2] + wcount[3];
+    __syncthreads();
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const uint32_t sA_addr = smem_u32(sA), sB_addr = smem_u32(sB);
+  const int lcl = tid & 7, lc = g * 8 + lcl;
+  const int rounds = (nv + kVoxPerRound - 1) / kVoxPerRound;
+  const int lo_x = 1, hi_x = L0 - 1, hi_y = L1 - 1, hi_z = L2 - 1;
+
+  int rd = 0;
+  for (; rd < rounds; ++rd) {
+    const int vs = rd * kVoxPerRound + (tid >> 3);
+    int vx = 0, vy = 0, vz = 0;
+    float a[kK];
+    if (vs < nv) {
+      const int vi = vlist[vs];
+      vx = vi % L0; vy = (vi / L0) % L1; vz = vi / (L0 * L1);
+#pragma unroll
+      for (int lm = 0; lm < 8; ++lm) {
+        const int ox = (lm == 1 || lm == 2 || lm == 5 || lm == 6), oy = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
+                  oz = lm >= 4;
+        const int64_t nb = vec_index(node_index(D, vx + ox, vy + oy, vz + oz), 0, lc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[3 * lm + c] = __ldg(u + nb + c * kNLC);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kK; ++k) a[k] = 0.0f;
+    }
+    // A hi / lo chunks in canonical layout
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+      const float hi = to_tf32(a[k]);
+      const float lo = to_tf32(a[k] - hi);
+      const int kc = k >> 3, kk = k & 7;
+      *reinterpret_cast<float*>(sA + kc * kAChunkBytes + canon_offset(tid, kk)) = hi;
+      *reinterpret_cast<float*>(sA + (3 + kc) * kAChunkBytes + canon_offset(tid, kk)) = lo;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int kc = 0; kc < 3; ++kc) {
+        const uint64_t ahi = smem_desc(sA_addr + kc * kAChunkBytes), alo = smem_desc(sA_addr + (3 + kc) * kAChunkBytes);
+        const uint64_t bhi = smem_desc(sB_addr + kc * kBChunkBytes), blo = smem_desc(sB_addr + (3 + kc) * kBChunkBytes);
+        mma_tf32(tmem, ahi, bhi, kc > 0 ? 1u : 0u);
+        mma_tf32(tmem, ahi, blo, 1u);
+        mma_tf32(tmem, alo, bhi, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar))
+                   : "memory");
+    }
+    if (!mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1))) atomicOr(&fail, 1);
+    __syncthreads();
+    if (fail) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (vs < nv) {
+      const float s = vscale[vs];
+#pragma unroll
+      for (int lm = 0; lm < 8; ++lm) {
+        const int ox = (lm == 1 || lm == 2 || lm == 5 || lm == 6), oy = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
+                  oz = lm >= 4;
+        const int nx = vx + ox, ny = vy + oy, nz = vz + oz;
+        const int lx = nx - t.x0, ly = ny - t.y0, lz = nz - t.z0;
+        const bool own = lx >= 0 && lx < kTileX && ly >= 0 && ly < kTileY && lz >= 0 && lz < kTileZ && nx >= lo_x &&
+                         nx <= hi_x && ny >= 1 && ny <= hi_y && nz >= 1 && nz <= hi_z;
+        if (own) {
+          const int nl = lx + kTileX * (ly + kTileY * lz);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) atomicAdd(&acc[(nl * 3 + c) * 8 + lcl], s * __uint_as_float(r[3 * lm + c]));
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  if (fail) {
+    if (tid == 0) atomicExch(err, 1);
+    mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this round's MMAs
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+  if (fail) return;
+  // owned interior nodes: w = scale * acc, dot with p
+  double dot = 0.0;
+  const int nsub = tid >> 3;  // 16 node slots per pass
+  for (int nl = nsub; nl < 128; nl += 16) {
+    const int lx = nl % kTileX, ly = (nl / kTileX) % kTileY, lz = nl / (kTileX * kTileY);
+    const int x = t.x0 + lx, yv = t.y0 + ly, z = t.z0 + lz;
+    if (x > hi_x || yv > hi_y || z > hi_z) continue;
+    const int64_t node = node_index(D, x, yv, z);
+    if (!(flags[node] & kNodeActive)) continue;  // void node: w stays 0
+    float v[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = (float)(D.scale * (double)acc[(nl * 3 + c) * 8 + lcl]);
+    const int64_t b = vec_index(node, 0, lc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      y[b + c * kNLC] = v[c];
+      dot += (double)__ldg(u + b + c * kNLC) * (double)v[c];
+    }
+  }
+  const double s = block_sum_lc<double>(dot, red);
+  if (threadIdx.x < 8) atomicAdd(acc_pw + (int64_t)t.dom * kNLC + lc, s);
+}
+
+// Host: build the split Khat in the canonical B layout and upload it.
+int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg) {
+  using namespace tc;
+  float img[6 * kN * kKc];
+  for (int i = 0; i < 6 * kN * kKc; ++i) img[i] = 0.0f;
+  for (int n = 0; n < 24; ++n)
+    for (int k = 0; k < kK; ++k) {
+      const float full = (float)khat[n + 24 * k];
+      // round to tf32 (10-bit mantissa, nearest, ties away) on the host
+      uint32_t b;
+      std::memcpy(&b, &full, 4);
+      uint32_t hb = (b + 0x1000u) & 0xFFFFE000u;
+      float hi;
+      std::memcpy(&hi, &hb, 4);
+      float rem = full - hi;
+      uint32_t rb;
+      std::memcpy(&rb, &rem, 4);
+      uint32_t lb = (rb + 0x1000u) & 0xFFFFE000u;
+      float lo;
+      std::memcpy(&lo, &lb, 4);
+      const int kc = k >> 3, kk = k & 7;
+      img[(kc * kBChunkBytes + canon_offset(n, kk)) / 4] = hi;
+      img[((3 + kc) * kBChunkBytes + canon_offset(n, kk)) / 4] = lo;
+    }
+  DTC_CUDA(cudaMemcpyToSymbolAsync(c_bsplit, img, sizeof(img), 0, cudaMemcpyHostToDevice, s));
+  return DTC_OK;
+}
+
+void launch_matvec_tc(const Tile* tiles, int64_t ntiles, const DomDev* doms, const float* svox,
+                      const uint8_t* flags, const float* u, float* y, double* acc_pw, const int* dom_active, int* err,
+                      cudaStream_t s) {
+  if (ntiles <= 0) return;
+  k_matvec_tc<<<(unsigned)(3 * ntiles), 128, 0, s>>>(tiles, doms, svox, flags, u, y, acc_pw, dom_active, err);
+}
+
+}  // namespace dtc

@@ -15,10 +15,20 @@ struct DomainTask {
   dtc_domain_out* out = nullptr;
 };
 
+struct KernelClass {
+  const char* name = "";
+  int64_t launches = 0;
+  double ms = 0, bytes = 0, flops = 0;   // summed over launches
+};
+
+enum KClassId { kcMatvec32, kcMatvec64, kcUpdate32, kcUpdate64, kcDirection32, kcDirection64, kcColstate,
+                kcReaction, kcProject, kcNumClasses };
+
 struct SolverStats {
   double ms_solve = 0, ms_rotation = 0;
   int64_t kernel_launches = 0;
   double dof_iterations = 0;  // sum over domains of free DOFs x load cases x iterations
+  KernelClass kc[kcNumClasses];
 };
 
 class DeviceSolver {

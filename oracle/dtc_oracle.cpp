@@ -456,69 +456,88 @@ struct CGState { double beta = 0, betaold = 1, dpi = 0, dpiold = 0, dp0 = 0; int
 
 void pcg_batch(const CSR& A, const std::vector<double>& dinv, const double* b, double* x,
                int nrhs, double rtol, int64_t max_it, int64_t* its_out, int* reason_out) {
+  // Row-major passes over all columns; each column's sums run over the dofs in index
+  // order, exactly as a separate solve would.  Stopped columns get alpha = 0 (x, r frozen).
   const int64_t n = A.n;
-  std::vector<double> r(b, b + n * nrhs), z(n * nrhs), p(n * nrhs, 0.0), w(n * nrhs);
-  std::fill(x, x + n * nrhs, 0.0);
-  std::vector<CGState> st(nrhs);
+  const int R = nrhs;
+  std::vector<double> r(b, b + n * R), z(n * R), p(n * R, 0.0), w(n * R);
+  std::fill(x, x + n * R, 0.0);
+  std::vector<CGState> st(R);
   const double abstol = 1e-50, divtol = 1e5;
-  auto pc = [&](void) {
-    for (int64_t i = 0; i < n; ++i)
-      for (int c = 0; c < nrhs; ++c) z[i * nrhs + c] = dinv[i] * r[i * nrhs + c];
+  std::vector<double> s1(R), s2(R), coef(R);
+  std::vector<char> active(R, 1);
+  auto precond_and_dots = [&]() {   // z = D^-1 r ; s1 = z.z ; s2 = z.r
+    std::fill(s1.begin(), s1.end(), 0.0);
+    std::fill(s2.begin(), s2.end(), 0.0);
+    for (int64_t i = 0; i < n; ++i) {
+      const double d = dinv[i];
+      double* zi = &z[i * R];
+      const double* ri = &r[i * R];
+      for (int c = 0; c < R; ++c) {
+        zi[c] = d * ri[c];
+        s1[c] += zi[c] * zi[c];
+        s2[c] += zi[c] * ri[c];
+      }
+    }
   };
-  auto norm_z = [&](int c) { double s = 0; for (int64_t i = 0; i < n; ++i) s += z[i * nrhs + c] * z[i * nrhs + c]; return std::sqrt(s); };
-  auto dot = [&](const std::vector<double>& u, const std::vector<double>& v, int c) {
-    double s = 0; for (int64_t i = 0; i < n; ++i) s += u[i * nrhs + c] * v[i * nrhs + c]; return s; };
-  pc();
-  std::vector<char> active(nrhs, 1);
-  for (int c = 0; c < nrhs; ++c) {
-    double dp = norm_z(c);
+  precond_and_dots();
+  for (int c = 0; c < R; ++c) {
+    double dp = std::sqrt(s1[c]);
     st[c].dp0 = dp;
     double ttol = std::max(rtol * dp, abstol);
     if (std::isnan(dp) || std::isinf(dp)) { st[c].reason = -9; active[c] = 0; continue; }
     if (dp <= ttol) { st[c].reason = 2; active[c] = 0; continue; }
-    st[c].beta = dot(z, r, c);
+    st[c].beta = s2[c];
   }
   for (int64_t i = 0; i < max_it; ++i) {
     bool any = false;
-    for (int c = 0; c < nrhs; ++c) {
+    for (int c = 0; c < R; ++c) {
+      coef[c] = 0.0;
       if (!active[c]) continue;
       st[c].its = i + 1;
       if (st[c].beta == 0.0) { st[c].reason = 3; active[c] = 0; continue; }
       if (i > 0 && st[c].beta * st[c].betaold < 0.0) { st[c].reason = -8; active[c] = 0; continue; }
-      if (i == 0) { for (int64_t k = 0; k < n; ++k) p[k * nrhs + c] = z[k * nrhs + c]; }
-      else {
-        double bb = st[c].beta / st[c].betaold;
-        for (int64_t k = 0; k < n; ++k) p[k * nrhs + c] = z[k * nrhs + c] + bb * p[k * nrhs + c];
-      }
+      coef[c] = (i == 0) ? 0.0 : st[c].beta / st[c].betaold;
       any = true;
     }
     if (!any) break;
-    A.mult(p.data(), w.data(), nrhs);
-    bool any2 = false;
-    for (int c = 0; c < nrhs; ++c) {
+    for (int64_t k = 0; k < n * R; k += R)
+      for (int c = 0; c < R; ++c)
+        if (active[c]) p[k + c] = (i == 0) ? z[k + c] : z[k + c] + coef[c] * p[k + c];
+    A.mult(p.data(), w.data(), R);
+    std::fill(s1.begin(), s1.end(), 0.0);
+    for (int64_t k = 0; k < n * R; k += R)
+      for (int c = 0; c < R; ++c) s1[c] += p[k + c] * w[k + c];
+    for (int c = 0; c < R; ++c) {
+      coef[c] = 0.0;
       if (!active[c]) continue;
       st[c].dpiold = st[c].dpi;
-      st[c].dpi = dot(p, w, c);
+      st[c].dpi = s1[c];
       st[c].betaold = st[c].beta;
-      double s1 = (st[c].dpi > 0) - (st[c].dpi < 0), s0 = (st[c].dpiold > 0) - (st[c].dpiold < 0);
-      if (st[c].dpi == 0.0 || (i > 0 && s1 * s0 < 0.0)) { st[c].reason = -8; active[c] = 0; continue; }
-      double a = st[c].beta / st[c].dpi;
-      for (int64_t k = 0; k < n; ++k) {
-        x[k * nrhs + c] += a * p[k * nrhs + c];
-        r[k * nrhs + c] -= a * w[k * nrhs + c];
+      double sg1 = (st[c].dpi > 0) - (st[c].dpi < 0), sg0 = (st[c].dpiold > 0) - (st[c].dpiold < 0);
+      if (st[c].dpi == 0.0 || (i > 0 && sg1 * sg0 < 0.0)) { st[c].reason = -8; active[c] = 0; continue; }
+      coef[c] = st[c].beta / st[c].dpi;
+    }
+    for (int64_t k = 0; k < n * R; k += R)
+      for (int c = 0; c < R; ++c) {
+        x[k + c] += coef[c] * p[k + c];
+        r[k + c] -= coef[c] * w[k + c];
       }
-      for (int64_t k = 0; k < n; ++k) z[k * nrhs + c] = dinv[k] * r[k * nrhs + c];
-      double dp = norm_z(c);
+    precond_and_dots();
+    bool any2 = false;
+    for (int c = 0; c < R; ++c) {
+      if (!active[c]) continue;
+      double dp = std::sqrt(s1[c]);
       double ttol = std::max(rtol * st[c].dp0, abstol);
       if (std::isnan(dp) || std::isinf(dp)) { st[c].reason = -9; active[c] = 0; continue; }
       if (dp <= ttol) { st[c].reason = 2; active[c] = 0; continue; }
       if (dp >= divtol * st[c].dp0) { st[c].reason = -4; active[c] = 0; continue; }
-      st[c].beta = dot(z, r, c);
+      st[c].beta = s2[c];
       any2 = true;
     }
     if (!any2) break;
   }
-  for (int c = 0; c < nrhs; ++c) {
+  for (int c = 0; c < R; ++c) {
     if (active[c]) st[c].reason = -3;  // KSP_DIVERGED_ITS
     its_out[c] = st[c].its;
     reason_out[c] = st[c].reason;

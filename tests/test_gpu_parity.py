@@ -53,9 +53,10 @@ def test_fp64_matches_oracle(dtc, batch):
         assert np.abs(r["iters"] - ref["iters"]).max() <= 2
 
 
-def test_mixed_matches_oracle(dtc, batch):
+@pytest.mark.parametrize("matvec", ["simt", "tensor"])
+def test_mixed_matches_oracle(dtc, batch, matvec):
     pairs, refs = batch
-    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False) as s:
+    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, mixed_matvec=matvec) as s:
         res = s.solve([p[0] for p in pairs])
     for r, ref in zip(res, refs):
         assert r["status"] == 0
