@@ -181,6 +181,26 @@ dtc_status dtc_energy_grad(dtc_handle* handle, const double* dloss_dc, float* co
 dtc_status dtc_get_stats(const dtc_handle* handle, double* ms_solve, int64_t* kernel_launches,
                          double* dof_iterations);
 
+/* Rotation search (CR1/CR2 sweep and refinement, f-src/mod_struct_calcmat.f90:533-1603) on
+ * tensors already in device memory, without allocating anything.  For callers that cannot
+ * allocate device memory at the point of the call -- e.g. a host code that runs this step
+ * while it captures a CUDA stream, or a host that hands the library only memory from its
+ * own pool -- so the solver's usual per-call scratch allocation is not an option.
+ * No counterpart in the reference.
+ *   ee   : n x 36 doubles on the current device (6x6 column-major, symmetric)
+ *   ang  : n x 2 x 3 int64 outputs: argmin angles (alpha, phi, eta) for CR1 then CR2, in
+ *          units of 10^-jj degree
+ *   jj   : n x 2 int32 outputs: refinement iterations;  crit: n x 2 doubles: final criterion
+ *   stream: a cudaStream_t (NULL = default stream); work is stream-ordered, the call does
+ *          not synchronise.
+ * n must not exceed 1024: the scratch is one fixed 2 MiB device array per device, kept until
+ * the process exits, shared by all calls; calls that overlap on the GPU race on it.
+ * The first call on a device resolves that array's address and uploads two small tables, so
+ * it synchronises and should come before any stream capture.  Sizes beyond the maximum
+ * return DTC_ERR_INVALID_ARGUMENT. */
+dtc_status dtc_rotation_search_noalloc(const double* ee, int64_t n, int64_t* ang, int32_t* jj, double* crit,
+                                       void* stream);
+
 /* Per kernel class of the last dtc_solve_batch (filled when profile_kernels = 1): launches,
  * summed CUDA-event time, and the algorithmic bytes / flops of one average launch. */
 typedef struct dtc_kernel_stats {

@@ -83,6 +83,8 @@ SIGNATURES = {
     "dtc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "dtc_element_stiffness": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "dtc_get_kernel_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStats), C.c_int32, C.POINTER(C.c_int32)]),
+    "dtc_rotation_search_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]),
     "dtc_last_error": (C.c_char_p, [C.c_void_p]),
 }
 

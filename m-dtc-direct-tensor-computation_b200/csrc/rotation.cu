@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -226,4 +227,49 @@ int rotation_search_device(const std::vector<const double*>& ees, std::vector<in
   return DTC_OK;
 }
 
+// -------------------------------------------------------------------------------------
+// Allocation-free variant of the rotation search.  Its only scratch, the per-block sweep
+// minima, lives in a file-scope device array sized for kNoAllocMaxDomains domains
+// (1024 x 64 blocks x 2 criteria x 16 B = 2 MiB, held by every device that loads the
+// library until the process exits).
+constexpr int64_t kNoAllocMaxDomains = 1024;
+static __device__ __align__(256) ArgMin g_noalloc_part[kNoAllocMaxDomains * kSweepBlocks * 2];
+
+namespace {
+std::mutex g_noalloc_mu;
+ArgMin* g_noalloc_ptr[256] = {nullptr};   // device address of g_noalloc_part, per device ordinal
+}  // namespace
+
 }  // namespace dtc
+
+extern "C" dtc_status dtc_rotation_search_noalloc(const double* ee, int64_t n, int64_t* ang, int32_t* jj,
+                                                  double* crit, void* stream) {
+  using namespace dtc;
+  if (n < 0 || n > kNoAllocMaxDomains) return DTC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return DTC_OK;
+  if (!ee || !ang || !jj || !crit) return DTC_ERR_INVALID_ARGUMENT;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return DTC_ERR_CUDA;
+  ArgMin* part = nullptr;
+  {
+    // first call on a device: resolve the scratch array's device address and load the
+    // degree tables of the sweep, with that device current
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_part) != cudaSuccess || !p) return DTC_ERR_CUDA;
+      double c[181], sn[181];
+      degree_tables(c, sn);
+      if (cudaMemcpyToSymbol(c_cosd, c, sizeof(c)) != cudaSuccess ||
+          cudaMemcpyToSymbol(c_sind, sn, sizeof(sn)) != cudaSuccess)
+        return DTC_ERR_CUDA;
+      g_noalloc_ptr[dev] = static_cast<ArgMin*>(p);
+    }
+    part = g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // every block of the sweep writes its own two minima, so no clearing is needed
+  k_rot_sweep<<<dim3(kSweepBlocks, (unsigned)n), kRotThreads, 0, s>>>(ee, part);
+  k_rot_refine<<<dim3((unsigned)n, 2), kRotThreads, 0, s>>>(ee, part, std::acos(-1.0) / 180.0, ang, jj, crit);
+  return cudaGetLastError() == cudaSuccess ? DTC_OK : DTC_ERR_CUDA;
+}
