@@ -24,6 +24,10 @@ sys.path.insert(0, str(ROOT))
 import __graft_entry__ as ge  # noqa: E402
 
 METRIC = "domains/sec at ≤1e-5 rel tensor err: mixed+batched vs plain FP64, 1 B200"
+TARGET = 1e-5
+# rtol at which the reference algorithm (reaction projection, FP64) meets TARGET on this
+# workload, as calibrated on the GPU; the host-only reference arm cannot calibrate itself
+REF_RTOL = 1e-7
 
 
 def parse():
@@ -34,9 +38,10 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--ndom", type=int, default=512)
     p.add_argument("--L", type=int, default=32)
-    p.add_argument("--rtol", type=float, default=1e-6)
+    p.add_argument("--rtol", type=float, default=0.0, help="0: calibrate per arm to the accuracy target")
+    p.add_argument("--estimator", default="energy", choices=["energy", "reaction"])
     p.add_argument("--max-it", type=int, default=20000)
-    p.add_argument("--check", type=int, default=8, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
+    p.add_argument("--check", type=int, default=16, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
     p.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     return p.parse_args()
@@ -44,7 +49,7 @@ def parse():
 
 def workload(args):
     return {"workload": f"{args.ndom}x{args.L}^3 HEX08 domains per GPU, 24 load cases, BV/TV U(0.10,0.40), "
-                        "per-voxel E from gray values", "rtol": args.rtol,
+                        "per-voxel E from gray values",
             "l2": "inputs larger than L2 (vectors are GBs)", "parallelism": f"replicas{args.gpus}"}
 
 
@@ -108,20 +113,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(args, dtc, grays):
+def cpu_baseline(args, dtc, grays, rtol):
     """The FP64 CPU oracle on a bounded sample of the same workload: one domain per host
     thread, the domains of the first step of the GPU batch."""
     orc = ge.load_oracle()
     syn = dtc.synth
     cores = os.cpu_count() or 1
     nsample = min(len(grays), cores, 32)
-    doms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=args.rtol, max_it=args.max_it,
+    doms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=rtol, max_it=args.max_it,
                        E_voxel=syn.modulus_of_gray(g)) for g in grays[:nsample]]
     t0 = time.perf_counter()
     orc.solve_batch(doms, nthreads=nsample)
     dt = time.perf_counter() - t0
     return {"value": nsample / dt, "unit": "domains/s", "cores": nsample, "kind": "port",
-            "sample": f"first {nsample} domains of the batch ({args.L}^3, rtol {args.rtol}), one per thread, "
+            "sample": f"first {nsample} domains of the batch ({args.L}^3, rtol {rtol}), one per thread, "
                       f"{dt:.1f} s"}
 
 
@@ -137,7 +142,8 @@ def run_reference(args, dtc):
     cores = os.cpu_count() or 1
     nsample = min(args.ndom, cores, 32)
     grays, _ = make_inputs(dtc, nsample, args.L)
-    doms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=args.rtol, max_it=args.max_it,
+    rtol = args.rtol if args.rtol > 0 else REF_RTOL
+    doms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=rtol, max_it=args.max_it,
                        E_voxel=syn.modulus_of_gray(g)) for g in grays]
     times = []
     warm = min(args.warmup, 1)   # a host run needs no device warm-up; bounded total time
@@ -157,7 +163,7 @@ def run_reference(args, dtc):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload(args),
             "cpu_baseline": {"value": v, "unit": "domains/s", "cores": nsample, "kind": "port",
-                             "sample": f"{nsample} domains of {args.L}^3 per step, one per thread, rtol {args.rtol}"},
+                             "sample": f"{nsample} domains of {args.L}^3 per step, one per thread, rtol {rtol}"},
             "e2e": {"value": v, "unit": "domains/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -183,7 +189,33 @@ def main():
                        domain_number=i) for i, g in enumerate(grays)]
     h2d = sum(d.phi.nbytes + d.E_voxel.nbytes for d in doms)
     d2h = args.ndom * 8 * (576 + 36 + 48)
-    mixed = dtc.Solver(precision="mixed", rtol=args.rtol, max_it=args.max_it, rotation_search=False, device=local)
+
+    # accuracy gate: both arms are timed at the loosest rtol whose tensors stay within
+    # TARGET/2 of an FP64 rtol-1e-10 solve on a sample spread over the batch
+    nchk = min(args.check, args.ndom)
+    sample = [doms[i] for i in np.linspace(0, args.ndom - 1, nchk).astype(int)]
+    with dtc.Solver(precision="fp64", rtol=1e-10, max_it=10 * args.max_it, rotation_search=False, device=local) as ref:
+        truth = [r["c"] for r in ref.solve(sample)]
+
+    def max_err(res):
+        return max(float(np.abs(r["c"] - t).max() / np.abs(t).max()) for r, t in zip(res, truth))
+
+    ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8, 3e-9, 1e-9]
+    arms = {"mixed": dict(precision="mixed", estimator=args.estimator),
+            "fp64": dict(precision="fp64", estimator="reaction")}
+    rtol_of, err_of = {}, {}
+    for arm, kw in arms.items():
+        for rt in ladder if args.rtol <= 0 else [args.rtol]:
+            with dtc.Solver(rtol=rt, max_it=args.max_it, rotation_search=False, device=local, **kw) as sv:
+                e = max_err(sv.solve(sample))
+            if e <= 0.5 * TARGET or args.rtol > 0:
+                rtol_of[arm], err_of[arm] = rt, e
+                break
+        else:
+            rtol_of[arm], err_of[arm] = ladder[-1], e
+
+    mixed = dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
+                       device=local, estimator=args.estimator)
 
     def barrier():
         torch.cuda.synchronize()
@@ -212,23 +244,21 @@ def main():
         step_ms, t_e2e = float(tt[0]), float(tt[1])
     value = world * args.ndom / (step_ms / 1e3)
     e2e = world * args.ndom / t_e2e
-    # accuracy gate against FP64 at rtol 1e-10 on a sample
-    nchk = min(args.check, args.ndom)
-    with dtc.Solver(precision="fp64", rtol=1e-10, max_it=10 * args.max_it, rotation_search=False, device=local) as ref:
-        chk = ref.solve(doms[:nchk])
-    errs = [float(np.abs(res[i]["c"] - chk[i]["c"]).max() / np.abs(chk[i]["c"]).max()) for i in range(nchk)]
+    idx = np.linspace(0, args.ndom - 1, nchk).astype(int)
+    timed_err = max_err([res[i] for i in idx])
     fp64 = None
     if not args.no_fp64:
-        with dtc.Solver(precision="fp64", rtol=args.rtol, max_it=args.max_it, rotation_search=False,
+        with dtc.Solver(precision="fp64", rtol=rtol_of["fp64"], max_it=args.max_it, rotation_search=False,
                         device=local) as plain:
             plain.solve(doms)
             fp64_ms = plain.stats()["ms_solve"]
-        fp64 = {"value": world * args.ndom / (fp64_ms / 1e3), "ms_per_step": fp64_ms,
+        fp64 = {"value": world * args.ndom / (fp64_ms / 1e3), "ms_per_step": fp64_ms, "rtol": rtol_of["fp64"],
+                "max_rel_err": err_of["fp64"], "estimator": "reaction (reference)",
                 "speedup_mixed_over_fp64": fp64_ms / step_ms}
     peak, src = measured_peaks()
     # dominant kernel: one extra, untimed-for-the-metric step with CUDA-event timing per launch
-    with dtc.Solver(precision="mixed", rtol=args.rtol, max_it=args.max_it, rotation_search=False,
-                    device=local, profile_kernels=True) as prof:
+    with dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
+                    device=local, profile_kernels=True, estimator=args.estimator) as prof:
         prof.solve(doms)
         ks = prof.kernel_stats()
     top = max(ks, key=lambda k: ks[k]["ms_total"])
@@ -236,13 +266,14 @@ def main():
     t_launch = kt["ms_total"] / kt["launches"] / 1e3
     achieved = kt["bytes_per_launch"] / t_launch / 1e9
     share = {k: round(v["ms_total"] / sum(x["ms_total"] for x in ks.values()), 4) for k, v in ks.items()}
-    cpu = cpu_baseline(args, dtc, grays) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    cpu = cpu_baseline(args, dtc, grays, rtol_of["fp64"]) if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "domains/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": workload(args),
-                "max_rel_err_vs_fp64_1e-10": max(errs), "accuracy_sample": nchk,
+                "rtol": rtol_of["mixed"], "estimator": args.estimator,
+                "max_rel_err_vs_fp64_1e-10": timed_err, "accuracy_target": TARGET, "accuracy_sample": nchk,
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -77,7 +77,13 @@ typedef struct dtc_options {
                               (dtc_get_kernel_stats); adds event records, off for production */
   int32_t mixed_matvec;    /* stiffness contraction of the FP32 inner solve: 0 = SIMT FP32,
                               1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy) */
-  int32_t reserved[6];
+  int32_t inner_precond;   /* preconditioner of the FP32 inner solve: 0 = Jacobi (as PETSc's
+                              PCJACOBI), 1 = node-block Jacobi (3x3 diagonal blocks) */
+  int32_t tensor_estimator; /* how ff is formed from the solutions: 0 = projection of the
+                              reaction forces (the reference, mod_struct_calcmat.f90:254-280),
+                              error linear in the solve error; 1 = energy products
+                              ff = vv^-T (U^T K U), equal at the exact solution, error quadratic */
+  int32_t reserved[4];
 } dtc_options;
 
 typedef struct dtc_domain_in {

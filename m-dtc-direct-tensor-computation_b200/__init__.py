@@ -93,7 +93,7 @@ class Solver:
 
     def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=0.0, max_refine=12,
                  rotation_search=True, device=0, host_threads=0, keep_displacements=False,
-                 profile_kernels=False, mixed_matvec="simt"):
+                 profile_kernels=False, mixed_matvec="simt", inner_precond="block", estimator="reaction"):
         self.lib = capi.load()
         o = capi.Options()
         self.lib.dtc_default_options(C.byref(o))
@@ -103,6 +103,8 @@ class Solver:
         o.keep_displacements = int(bool(keep_displacements))
         o.profile_kernels = int(bool(profile_kernels))
         o.mixed_matvec = {"simt": 0, "tensor": 1}[mixed_matvec]
+        o.inner_precond = {"jacobi": 0, "block": 1}[inner_precond]
+        o.tensor_estimator = {"reaction": 0, "energy": 1}[estimator]
         self.options = o
         h = C.c_void_p()
         rc = self.lib.dtc_create(C.byref(h), C.byref(o))

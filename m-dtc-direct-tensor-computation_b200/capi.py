@@ -26,7 +26,8 @@ class Options(C.Structure):
         ("max_it", C.c_int64), ("inner_rtol", C.c_double), ("max_refine", C.c_int32),
         ("rotation_search", C.c_int32), ("device", C.c_int32), ("host_threads", C.c_int32),
         ("keep_displacements", C.c_int32), ("profile_kernels", C.c_int32),
-        ("mixed_matvec", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("mixed_matvec", C.c_int32), ("inner_precond", C.c_int32),
+        ("tensor_estimator", C.c_int32), ("reserved", C.c_int32 * 4),
     ]
 
 

@@ -119,6 +119,7 @@ void dtc_default_options(dtc_options* opt) {
   opt->inner_rtol = 0.0;   // automatic: max(0.3 rtol, 1e-7)
   opt->max_refine = 12;
   opt->rotation_search = 1;
+  opt->inner_precond = 1;
   opt->device = 0;
 }
 

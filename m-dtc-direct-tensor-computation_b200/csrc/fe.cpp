@@ -242,6 +242,21 @@ void homogenise(const double ff[576], const int64_t L[3], const double delta[3],
   out->sym_ee = symmetry_deviation(6, out->ee);
 }
 
+void energy_to_ff(const double gram[576], double ff[576]) {
+  double uu[8 * 3 * 24], vv[576];
+  macro_modes(1e-6, uu);
+  for (int lc = 0; lc < 24; ++lc)
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 8; ++l) vv[(8 * k + l) + 24 * lc] = uu[l + 8 * k + 24 * lc];
+  gauss_jordan_inverse(24, vv);
+  for (int lc = 0; lc < 24; ++lc)
+    for (int r = 0; r < 24; ++r) {
+      double s = 0.0;
+      for (int a = 0; a < 24; ++a) s += vv[a + 24 * r] * gram[a + 24 * lc];
+      ff[r + 24 * lc] = s;
+    }
+}
+
 void finish_rotation(const double ee[36], int which, const int64_t ang[3], int jj, double crit,
                      dtc_domain_out* out) {
   // quirk kept: the final angle scale is pi / (180 (10^jj - 1)) (:1017, :1464)

@@ -28,6 +28,12 @@ double boundary_value(const double* uu, const double N[8], int c, int lc);
 void homogenise(const double ff[576], const int64_t L[3], const double delta[3], double rve_strain,
                 dtc_domain_out* out);
 
+// Domain forces from the energy products M(a,b) = u_a^T K u_b of the 24 load-case solutions:
+// ff(r, lc) = sum_a vvbc^-1(a, r) M(a, lc), vvbc the load-case matrix of the boundary modes
+// actually prescribed (eps = 1e-6, mod_write_deck.f90:61).  Equal to the reaction projection
+// (mod_struct_calcmat.f90:254-280) at the exact solution.
+void energy_to_ff(const double gram[576], double ff[576]);
+
 // Rotation search results -> output record (mod_struct_calcmat.f90:1014-1137, 1462-1603):
 // ang = argmin indices in units of 10^-jj degree, jj = refinement iterations.
 void finish_rotation(const double ee[36], int which, const int64_t ang[3], int jj, double crit,

@@ -178,13 +178,15 @@ __global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ ti
 // node: lane = x offset in the tile, rows as in the matvec.
 __global__ void __launch_bounds__(kThreads) k_node_setup(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                          const float* __restrict__ svox, uint8_t* __restrict__ flags,
-                                                         double* __restrict__ dinv64, float* __restrict__ dinv32) {
+                                                         double* __restrict__ dinv64, float* __restrict__ dinv32,
+                                                         float* __restrict__ binv32) {
   const Tile t = tiles[blockIdx.x];
   const DomDev D = doms[t.dom];
   const int x = t.x0 + (threadIdx.x & 7), row = threadIdx.x >> 3;
   const int y = t.y0 + (row & 3), z = t.z0 + (row >> 2);
   if (x > D.L[0] || y > D.L[1] || z > D.L[2]) return;
   double d[3] = {0, 0, 0};
+  double blk[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   bool active = false;
   for (int a = 0; a < 2; ++a)
     for (int b = 0; b < 2; ++b)
@@ -196,6 +198,8 @@ __global__ void __launch_bounds__(kThreads) k_node_setup(const Tile* __restrict_
         active = true;
         const int ln = corner_local(1 - a, 1 - b, 1 - c);
         for (int k = 0; k < 3; ++k) d[k] += (double)s * c_khat64[(3 * ln + k) * 25];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) blk[i][j] += (double)s * c_khat64[(3 * ln + i) + 24 * (3 * ln + j)];
       }
   for (int k = 0; k < 3; ++k) d[k] *= D.scale;
   const bool bnd = (x == 0 || x == D.L[0] || y == 0 || y == D.L[1] || z == 0 || z == D.L[2]);
@@ -205,6 +209,39 @@ __global__ void __launch_bounds__(kThreads) k_node_setup(const Tile* __restrict_
     const double di = (active && !bnd && d[k] != 0.0) ? 1.0 / d[k] : 0.0;
     dinv64[n * 3 + k] = di;
     dinv32[n * 3 + k] = (float)di;
+  }
+  // inverse of the node's 3x3 diagonal block (node-block Jacobi), symmetric: xx yy zz xy xz yz
+  float bi[6] = {0, 0, 0, 0, 0, 0};
+  if (active && !bnd) {
+    const double a = blk[0][0], b = blk[0][1], c = blk[0][2], e = blk[1][1], f = blk[1][2], g = blk[2][2];
+    const double c00 = e * g - f * f, c01 = c * f - b * g, c02 = b * f - c * e;
+    const double det = a * c00 + b * c01 + c * c02;
+    if (det > 0.0) {
+      const double inv = 1.0 / (det * D.scale);
+      bi[0] = (float)(c00 * inv);
+      bi[1] = (float)((a * g - c * c) * inv);
+      bi[2] = (float)((a * e - b * b) * inv);
+      bi[3] = (float)(c01 * inv);
+      bi[4] = (float)(c02 * inv);
+      bi[5] = (float)((b * c - a * f) * inv);
+    }
+  }
+  for (int k = 0; k < 6; ++k) binv32[n * 6 + k] = bi[k];
+}
+
+// Preconditioner z = M^-1 r for the 3 components of one node: scalar Jacobi (PETSc PCJACOBI)
+// or node-block Jacobi (inverse 3x3 diagonal block, symmetric storage).
+template <typename T, bool BLOCK>
+__device__ __forceinline__ void precond(const T* __restrict__ m, int64_t n, const T (&r)[3], T (&z)[3]) {
+  if (BLOCK) {
+    const T* b = m + n * 6;
+    z[0] = b[0] * r[0] + b[3] * r[1] + b[4] * r[2];
+    z[1] = b[3] * r[0] + b[1] * r[1] + b[5] * r[2];
+    z[2] = b[4] * r[0] + b[5] * r[1] + b[2] * r[2];
+  } else {
+    z[0] = m[n * 3 + 0] * r[0];
+    z[1] = m[n * 3 + 1] * r[1];
+    z[2] = m[n * 3 + 2] * r[2];
   }
 }
 
@@ -261,8 +298,8 @@ __global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __rest
   const bool rowok = yy >= 1 && yy <= D.L[1] - 1 && zz >= 1 && zz <= D.L[2] - 1; \
   const int64_t col = (int64_t)t.dom * kNLC + lc;
 
-// p = D^-1 r + bfac * p
-template <typename T>
+// p = M^-1 r + bfac * p
+template <typename T, bool BLOCK>
 __global__ void __launch_bounds__(kThreads) k_direction(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                         const uint8_t* __restrict__ flags, const T* __restrict__ dinv,
                                                         const T* __restrict__ r, T* __restrict__ p,
@@ -276,17 +313,19 @@ __global__ void __launch_bounds__(kThreads) k_direction(const Tile* __restrict__
     if (x > D.L[0] - 1) break;
     const int64_t n = node_index(D, x, yy, zz);
     if (!(flags[n] & kNodeActive)) continue;
+    const int64_t k0 = vec_index(n, 0, lc);
+    T rr[3], z[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t k = vec_index(n, c, lc);
-      p[k] = dinv[n * 3 + c] * r[k] + bf * p[k];
-    }
+    for (int c = 0; c < 3; ++c) rr[c] = r[k0 + c * kNLC];
+    precond<T, BLOCK>(dinv, n, rr, z);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p[k0 + c * kNLC] = z[c] + bf * p[k0 + c * kNLC];
   }
 }
 
-// x += alpha p ; r -= alpha w ; z = D^-1 r ; acc_zz += z.z ; acc_zr += z.r
+// x += alpha p ; r -= alpha w ; z = M^-1 r ; acc_zz += z.z ; acc_zr += z.r
 // alpha = beta / (p.w) unless the column stopped or p.w flags an indefinite operator.
-template <typename T>
+template <typename T, bool BLOCK>
 __global__ void __launch_bounds__(kThreads) k_update(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                      const uint8_t* __restrict__ flags, const T* __restrict__ dinv,
                                                      T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
@@ -307,15 +346,20 @@ __global__ void __launch_bounds__(kThreads) k_update(const Tile* __restrict__ ti
       if (xx > D.L[0] - 1) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
+      const int64_t k0 = vec_index(n, 0, lc);
+      T rn[3], z[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const int64_t k = vec_index(n, c, lc);
+        const int64_t k = k0 + c * kNLC;
         x[k] = x[k] + a * p[k];
-        const T rn = r[k] - a * w[k];
-        r[k] = rn;
-        const T z = dinv[n * 3 + c] * rn;
-        zz2 += (double)z * (double)z;
-        zr += (double)z * (double)rn;
+        rn[c] = r[k] - a * w[k];
+        r[k] = rn[c];
+      }
+      precond<T, BLOCK>(dinv, n, rn, z);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        zz2 += (double)z[c] * (double)z[c];
+        zr += (double)z[c] * (double)rn[c];
       }
     }
   }
@@ -328,8 +372,8 @@ __global__ void __launch_bounds__(kThreads) k_update(const Tile* __restrict__ ti
   }
 }
 
-// z = D^-1 r; acc_zz += z.z ; acc_zr += z.r (start of a solve)
-template <typename T>
+// z = M^-1 r; acc_zz += z.z ; acc_zr += z.r (start of a solve)
+template <typename T, bool BLOCK>
 __global__ void __launch_bounds__(kThreads) k_initial_dots(const Tile* __restrict__ tiles,
                                                            const DomDev* __restrict__ doms,
                                                            const uint8_t* __restrict__ flags,
@@ -345,12 +389,15 @@ __global__ void __launch_bounds__(kThreads) k_initial_dots(const Tile* __restric
       if (xx > D.L[0] - 1) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
+      const int64_t k0 = vec_index(n, 0, lc);
+      T rn[3], z[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) rn[c] = r[k0 + c * kNLC];
+      precond<T, BLOCK>(dinv, n, rn, z);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const T rn = r[vec_index(n, c, lc)];
-        const T z = dinv[n * 3 + c] * rn;
-        zz2 += (double)z * (double)z;
-        zr += (double)z * (double)rn;
+        zz2 += (double)z[c] * (double)z[c];
+        zr += (double)z[c] * (double)rn[c];
       }
     }
   }
@@ -598,6 +645,51 @@ __global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ t
   }
 }
 
+// Energy products M(a,b) = u_a . (K u_b) over all nodes, 24 x 24 per domain (FP64).  With
+// F = K u from the reaction pass, M is the Gram matrix of the load-case solutions in the
+// stiffness inner product; ff = vv^-T M equals the reaction projection at the exact solution
+// and its error is quadratic in the solution error.
+__global__ void __launch_bounds__(kThreads) k_energy_gram(const Tile* __restrict__ tiles,
+                                                          const DomDev* __restrict__ doms,
+                                                          const uint8_t* __restrict__ flags,
+                                                          const double* __restrict__ X, const double* __restrict__ F,
+                                                          double* __restrict__ gram) {
+  __shared__ double part[16][8][25];
+  const Tile t = tiles[blockIdx.x / 3];
+  const DomDev D = doms[t.dom];
+  const int lcl = threadIdx.x & 7, b = (blockIdx.x % 3) * kLcGroup + lcl;
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  double acc[24];
+#pragma unroll
+  for (int k = 0; k < 24; ++k) acc[k] = 0.0;
+  if (yy <= D.L[1] && zz <= D.L[2]) {
+    for (int i = 0; i < kTileX; ++i) {
+      const int xx = t.x0 + i;
+      if (xx > D.L[0]) break;
+      const int64_t n = node_index(D, xx, yy, zz);
+      if (!(flags[n] & kNodeActive)) continue;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double f = F[vec_index(n, c, b)];
+        const double* xu = X + vec_index(n, c, 0);
+#pragma unroll
+        for (int a = 0; a < 24; ++a) acc[a] += xu[a] * f;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 24; ++k) part[row][lcl][k] = acc[k];
+  __syncthreads();
+  for (int j = threadIdx.x; j < 8 * 24; j += kThreads) {
+    const int l8 = j / 24, a = j % 24;
+    double sum = 0.0;
+    for (int r2 = 0; r2 < 16; ++r2) sum += part[r2][l8][a];
+    const int bg = (blockIdx.x % 3) * kLcGroup + l8;
+    atomicAdd(gram + (int64_t)t.dom * 576 + a + 24 * bg, sum);
+  }
+}
+
 // -------------------------------------------------------------------------------------
 // Host driver
 struct DeviceSolver::Impl {
@@ -654,7 +746,7 @@ struct DeviceSolver::Impl {
 namespace {
 
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
-           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bNumBufs };
+           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bNumBufs };
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
   if (I.caps[which] >= bytes && I.bufs[which]) return DTC_OK;
@@ -704,7 +796,7 @@ int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg);
 namespace {
 
 // CG on one precision: x (interior part), r = b on entry, p = 0 on entry.
-template <typename T>
+template <typename T, bool BLOCK>
 int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w, const T* dinv, double rtol,
            const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
   cudaStream_t s = I.stream;
@@ -721,7 +813,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
   DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
-  if (nti > 0) k_initial_dots<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, zz, zr, nullptr);
+  if (nti > 0) k_initial_dots<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, zz, zr, nullptr);
   k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs);
   launches += 2;
   if (int e = launch_check(msg)) return e;
@@ -735,7 +827,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
     for (int k = 0; k < chunk; ++k) {
       if (nti > 0) {
         int q = I.begin(0);
-        k_direction<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
+        k_direction<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
         I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
         q = I.begin(0);
         if (sizeof(T) == 4 && I.tensor_matvec)
@@ -745,7 +837,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
           k_matvec<T, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
         I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
         q = I.begin(0);
-        k_update<T><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
+        k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
         I.end(f32 ? kcUpdate32 : kcUpdate64, q, 6 * vb, 0);
       }
       int q = I.begin(0);
@@ -890,6 +982,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   if ((e = ensure(I, bFlags, node_total, msg))) return e;
   if ((e = ensure(I, bDinv64, sizeof(double) * node_total * 3, msg))) return e;
   if ((e = ensure(I, bDinv32, sizeof(float) * node_total * 3, msg))) return e;
+  if ((e = ensure(I, bBinv32, sizeof(float) * node_total * 6, msg))) return e;
   if ((e = ensure(I, bX, vbytes64, msg))) return e;
   if ((e = ensure(I, bR64, vbytes64, msg))) return e;
   if (mixed) {
@@ -933,8 +1026,9 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   double* R64 = B<double>(I, bR64);
   int64_t& L = stats_.kernel_launches;
   if (nta) {
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bBinv32], 0, sizeof(float) * node_total * 6, s));
     k_node_setup<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
-                                                    B<float>(I, bDinv32));
+                                                    B<float>(I, bDinv32), B<float>(I, bBinv32));
     k_boundary_values<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, fl, X);
     L += 2;
   }
@@ -946,7 +1040,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
     if (nti) { k_matvec<double, false, false><<<gi, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), X, R64, -1.0, nullptr, nullptr); ++L; }
-    if ((e = run_cg<double>(I, ndom, nti, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
+    if ((e = run_cg<double, false>(I, ndom, nti, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
                             opt.rtol, nullptr, opt.max_it, L, msg)))
       return e;
     DTC_CUDA(cudaMemcpyAsync(ost, I.bufs[bSt], sizeof(ColState) * ncol, cudaMemcpyDeviceToDevice, s));
@@ -977,9 +1071,15 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
       if (h_count == 0 || step == max_refine || inner_budget <= 0) break;
       if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
       DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
-      if ((e = run_cg<float>(I, ndom, nti, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
-                             B<float>(I, bDinv32), inner, B<double>(I, bTarget), inner_budget, L, msg)))
-        return e;
+      if (opt.inner_precond == 1)
+        e = run_cg<float, true>(I, ndom, nti, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
+                                B<float>(I, bW32), B<float>(I, bBinv32), inner, B<double>(I, bTarget), inner_budget,
+                                L, msg);
+      else
+        e = run_cg<float, false>(I, ndom, nti, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
+                                 B<float>(I, bW32), B<float>(I, bDinv32), inner, B<double>(I, bTarget), inner_budget,
+                                 L, msg);
+      if (e) return e;
       if (nti) { k_apply_correction<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<float>(I, bX32), X, ost); ++L; }
       k_add_inner_its<<<(unsigned)((ncol + 255) / 256), 256, 0, s>>>(ost, B<ColState>(I, bSt), (int64_t)ncol);
       ++L;
@@ -990,7 +1090,10 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
   if (nta) {
     k_matvec<double, true, false><<<ga, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), X, R64, 1.0, nullptr, nullptr);
-    k_project<<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf));
+    if (opt.tensor_estimator == 1)
+      k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf));
+    else
+      k_project<<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf));
     L += 2;
   }
   if ((e = launch_check(msg))) return e;
@@ -1017,7 +1120,8 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   for (int d = 0; d < ndom; ++d) {
     DomainTask& t = tasks[tidx[d]];
     dtc_domain_out* o = t.out;
-    std::memcpy(o->ff, &ff[(size_t)576 * d], sizeof(double) * 576);
+    if (opt.tensor_estimator == 1) energy_to_ff(&ff[(size_t)576 * d], o->ff);
+    else std::memcpy(o->ff, &ff[(size_t)576 * d], sizeof(double) * 576);
     int worst = DTC_DOMAIN_OK;
     int steps = 0;
     for (int lc = 0; lc < kNLC; ++lc) {

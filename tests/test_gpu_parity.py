@@ -53,15 +53,28 @@ def test_fp64_matches_oracle(dtc, batch):
         assert np.abs(r["iters"] - ref["iters"]).max() <= 2
 
 
-@pytest.mark.parametrize("matvec", ["simt", "tensor"])
-def test_mixed_matches_oracle(dtc, batch, matvec):
+@pytest.mark.parametrize("matvec,precond", [("simt", "block"), ("tensor", "block"), ("simt", "jacobi")])
+def test_mixed_matches_oracle(dtc, batch, matvec, precond):
     pairs, refs = batch
-    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, mixed_matvec=matvec) as s:
+    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, mixed_matvec=matvec,
+                    inner_precond=precond) as s:
         res = s.solve([p[0] for p in pairs])
     for r, ref in zip(res, refs):
         assert r["status"] == 0
         assert rel(r["c"], ref["c"]) <= TOL_MIXED
         assert r["refine_steps"] >= 1
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_energy_estimator_matches_oracle(dtc, batch, precision):
+    """ff from the energy products equals the reaction projection at convergence."""
+    pairs, refs = batch
+    with dtc.Solver(precision=precision, rtol=1e-10, rotation_search=False, estimator="energy") as s:
+        res = s.solve([p[0] for p in pairs])
+    tol = TOL_FP64 if precision == "fp64" else TOL_MIXED
+    for r, ref in zip(res, refs):
+        assert rel(r["c"], ref["c"]) <= tol
+        assert rel(r["ff"], ref["ff"]) <= tol
 
 
 def test_fields_in_reference_numbering(dtc, orc):
