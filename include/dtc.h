@@ -124,7 +124,9 @@ typedef struct dtc_domain_out {
   int32_t cr1_iters, cr2_iters;  /* refinement iterations jj */
   double density;          /* ne / (L0*L1*L2) (mod_struct_calcmat.f90:1642-1651) */
   double* displ;           /* optional (NULL to skip): 24 x 3nn displacements incl. boundary
-                              values, load-case major, reference DOF numbering 3*(node-1)+comp */
+                              values, load-case major, reference DOF numbering 3*(node-1)+comp;
+                              room for 72*(L0+1)(L1+1)(L2+1) doubles (HEX08) or
+                              72*(2L0+1)(2L1+1)(2L2+1) (HEX20) always suffices */
   double* force;           /* optional: 24 x 3nn reaction forces AA_org*u, same layout */
 } dtc_domain_out;
 

@@ -137,7 +137,8 @@ class Solver:
         keep = []
         if want_fields:
             for i, d in enumerate(domains):
-                cap = 24 * 3 * (d.L[0] + 1) * (d.L[1] + 1) * (d.L[2] + 1)
+                m = 1 if d.elem_type == HEX08 else 2   # HEX20 nodes live on the doubled grid
+                cap = 24 * 3 * (m * d.L[0] + 1) * (m * d.L[1] + 1) * (m * d.L[2] + 1)
                 fd, ff_ = np.zeros(cap), np.zeros(cap)
                 keep.append((fd, ff_))
                 outs[i].displ = fd.ctypes.data_as(C.POINTER(C.c_double))

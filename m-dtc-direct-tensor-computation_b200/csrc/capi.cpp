@@ -207,7 +207,7 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     std::string msg;
     if (validate_domain(in[i], msg)) { h->err = "domain " + std::to_string(i) + ": " + msg; return DTC_ERR_INVALID_ARGUMENT; }
     if (in[i].nu != in[0].nu) { h->err = "all domains of one call must share nu"; return DTC_ERR_INVALID_ARGUMENT; }
-    if (in[i].elem_type != DTC_HEX08) { h->err = "this build solves HEX08 micro elements only"; return DTC_ERR_INVALID_ARGUMENT; }
+    if (in[i].elem_type != in[0].elem_type) { h->err = "all domains of one call must share elem_type"; return DTC_ERR_INVALID_ARGUMENT; }
   }
   std::vector<MeshPlan> plans;
   bool want_fields = false;
@@ -237,7 +237,8 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     double bytes = 0;
     while (k < tasks.size()) {
       const dtc_domain_in& d = *tasks[k].in;
-      const double nb = (double)(d.L[0] + 1) * (d.L[1] + 1) * (d.L[2] + 1) * device_bytes_per_node();
+      const int mg = d.elem_type == DTC_HEX20 ? 2 : 1;   // HEX20 nodes live on the doubled grid
+      const double nb = (double)(mg * d.L[0] + 1) * (mg * d.L[1] + 1) * (mg * d.L[2] + 1) * device_bytes_per_node();
       if (!chunk.empty() && bytes + nb > budget) break;
       bytes += nb;
       chunk.push_back(tasks[k++]);

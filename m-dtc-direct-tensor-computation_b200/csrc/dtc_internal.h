@@ -1,7 +1,8 @@
 // dtc_internal.h -- shared definitions of the host planner and the sm_100a kernels.
 //
 // Device layout (one domain = one cubic control volume of L0 x L1 x L2 voxels):
-//  * nodes live on the (L0+1)(L1+1)(L2+1) voxel-corner grid, index n = x + nx*(y + ny*z);
+//  * nodes live on the (m*L0+1)(m*L1+1)(m*L2+1) grid (m = 1: voxel corners, HEX08; m = 2: the
+//    doubled grid carrying the HEX20 corner and mid-edge nodes), index n = x + nx*(y + ny*z);
 //  * every nodal vector is [node][component][load case] with the 24 load cases innermost,
 //    so the 24 right-hand sides of one DOF are one contiguous 96/192-byte run;
 //  * per voxel one float modulus factor: E_voxel, or 1.0 when every element uses E; 0 for
@@ -26,7 +27,9 @@ enum : uint8_t { kNodeActive = 1, kNodeBoundary = 2 };
 
 struct DomDev {
   int32_t L[3];        // voxels per edge
-  int32_t n[3];        // nodes per edge (L+1)
+  int32_t n[3];        // nodes per edge: m*L+1
+  int32_t m;           // node-grid refinement: 1 (HEX08 corners), 2 (HEX20 corners + mid-edges)
+  int32_t pad_;
   int64_t vox_off;     // offset into the voxel scale array
   int64_t node_off;    // offset into node arrays (vectors are node_off*72)
   int64_t min_c_off[3];  // xa_n - 1: node (i,j,k) sits at ((i,j,k) + min_c_off) * delta

@@ -1,10 +1,11 @@
 // kernels.cu -- sm_100a kernels of the batched voxel solver and its host driver.
 //
 // Operator: the assembled stiffness of the reference (MatSetValues of one Ke per element,
-// f-src/mod_dtc_main_subroutines.f90:516-579) is never formed.  K*u is applied matrix-free
-// as a node-centric sweep: the output at node n sums, over the <= 8 kept voxels around n,
-// s_v * Khat[rows of n's corner, :] * u_v, where s_v = E_v * a and Khat the unit voxel
-// stiffness.  Constrained DOFs (all nodes on the domain box, mod_struct_preprocess.f90:
+// f-src/mod_dtc_main_subroutines.f90:516-579) is never formed.  HEX08: K*u is applied
+// matrix-free as a node-centric sweep: the output at node n sums, over the <= 8 kept voxels
+// around n, s_v * Khat[rows of n's corner, :] * u_v, where s_v = E_v * a and Khat the unit
+// voxel stiffness.  HEX20: element-by-element on voxel bricks staged in shared memory
+// (ebe.cuh), nodes on the doubled grid.  Constrained DOFs (all nodes on the domain box, mod_struct_preprocess.f90:
 // 564-592) are excluded from the unknowns exactly like MatZeroRowsColumns with diag 0
 // (:945-951), so the iteration runs on the interior nodes only.
 //
@@ -29,6 +30,8 @@ namespace dtc {
 __constant__ double c_khat64[576];   // unit voxel stiffness, column-major (symmetric)
 __constant__ float c_khat32[576];
 __constant__ double c_uu[8 * 3 * kNLC];  // macro modes uu(8,3,24) for eps = 1e-6
+__constant__ double c_k20_64[3600];       // unit HEX20 element matrix (ring node order)
+__constant__ float c_k20_32[3600];
 
 template <typename T> struct KhatC;
 template <> struct KhatC<float> {
@@ -39,7 +42,7 @@ template <> struct KhatC<double> {
 };
 
 // -------------------------------------------------------------------------------------
-// Matrix-free K*u on one tile.  Window w[px][py][pz][c] holds u at x-1+px, y-1+py, z-1+pz;
+// HEX08: matrix-free K*u on one node tile (the default SIMT operator of the corner grid).  Window w[px][py][pz][c] holds u at x-1+px, y-1+py, z-1+pz;
 // sv[a][b][c] the scale of voxel (x-1+a, y-1+b, z-1+c).
 template <typename T>
 __device__ __forceinline__ void apply_node(const T (&w)[3][3][3][3], const float (&sv)[2][2][2], T (&acc)[3]) {
@@ -124,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ ti
   const int row = threadIdx.x >> 3;
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   const int lo = ALL ? 0 : 1;
-  const int xhi = ALL ? D.L[0] : D.L[0] - 1, yhi = ALL ? D.L[1] : D.L[1] - 1, zhi = ALL ? D.L[2] : D.L[2] - 1;
+  const int xhi = ALL ? D.n[0] - 1 : D.n[0] - 2, yhi = ALL ? D.n[1] - 1 : D.n[1] - 2, zhi = ALL ? D.n[2] - 1 : D.n[2] - 2;
   double dot = 0.0;
   if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi) {
     T w[3][3][3][3];
@@ -172,49 +175,77 @@ __global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ ti
   }
 }
 
+}  // namespace dtc
+
+#include "ebe.cuh"
+
+namespace dtc {
+
 // -------------------------------------------------------------------------------------
-// Node set-up: flags and the Jacobi diagonal sum_v s_v Khat(ii) (PCJACOBI of the
-// row-and-column-zeroed matrix; constrained rows are never iterated on).  One thread per
-// node: lane = x offset in the tile, rows as in the matvec.
+// Node set-up: flags, the Jacobi diagonal sum_v s_v Ke(ii) (PCJACOBI of the row-and-column-
+// zeroed matrix; constrained rows are never iterated on) and the node-block inverse.  One
+// thread per node of the (fine) grid.  Adjacent voxels of a node: per axis, a coordinate f
+// lies in voxel f/m - 1 (local offset m) and f/m (offset 0) when f is a multiple of m, else
+// only in (f-1)/2 (offset 1, HEX20 mid-edge).
+template <int NEN> __device__ __forceinline__ int local_node(int ox, int oy, int oz);
+template <> __device__ __forceinline__ int local_node<8>(int ox, int oy, int oz) { return corner_local(ox, oy, oz); }
+template <> __device__ __forceinline__ int local_node<20>(int ox, int oy, int oz) {
+  for (int a = 0; a < 20; ++a)
+    if (kRingOff[a][0] == ox && kRingOff[a][1] == oy && kRingOff[a][2] == oz) return a;
+  return -1;
+}
+template <int NEN> __device__ __forceinline__ double ke64(int i);
+template <> __device__ __forceinline__ double ke64<8>(int i) { return c_khat64[i]; }
+template <> __device__ __forceinline__ double ke64<20>(int i) { return c_k20_64[i]; }
+
+template <int NEN>
 __global__ void __launch_bounds__(kThreads) k_node_setup(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                          const float* __restrict__ svox, uint8_t* __restrict__ flags,
                                                          double* __restrict__ dinv64, float* __restrict__ dinv32,
                                                          float* __restrict__ binv32) {
+  constexpr int ND = 3 * NEN;
   const Tile t = tiles[blockIdx.x];
   const DomDev D = doms[t.dom];
   const int x = t.x0 + (threadIdx.x & 7), row = threadIdx.x >> 3;
   const int y = t.y0 + (row & 3), z = t.z0 + (row >> 2);
-  if (x > D.L[0] || y > D.L[1] || z > D.L[2]) return;
-  double d[3] = {0, 0, 0};
+  if (x >= D.n[0] || y >= D.n[1] || z >= D.n[2]) return;
+  const int m = D.m;
+  const int f[3] = {x, y, z};
+  int vc[3][2], oc[3][2], nc[3];
+  for (int d = 0; d < 3; ++d) {
+    if (f[d] % m == 0) { nc[d] = 2; vc[d][0] = f[d] / m - 1; oc[d][0] = m; vc[d][1] = f[d] / m; oc[d][1] = 0; }
+    else { nc[d] = 1; vc[d][0] = (f[d] - 1) / 2; oc[d][0] = 1; }
+  }
+  double d3[3] = {0, 0, 0};
   double blk[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   bool active = false;
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b)
-      for (int c = 0; c < 2; ++c) {
-        const int vx = x - 1 + a, vy = y - 1 + b, vz = z - 1 + c;
+  for (int i = 0; i < nc[0]; ++i)
+    for (int j = 0; j < nc[1]; ++j)
+      for (int k = 0; k < nc[2]; ++k) {
+        const int vx = vc[0][i], vy = vc[1][j], vz = vc[2][k];
         if (vx < 0 || vy < 0 || vz < 0 || vx >= D.L[0] || vy >= D.L[1] || vz >= D.L[2]) continue;
         const float s = svox[D.vox_off + vx + (int64_t)D.L[0] * (vy + (int64_t)D.L[1] * vz)];
         if (s == 0.0f) continue;
+        const int ln = local_node<NEN>(oc[0][i], oc[1][j], oc[2][k]);
+        if (ln < 0) continue;
         active = true;
-        const int ln = corner_local(1 - a, 1 - b, 1 - c);
-        for (int k = 0; k < 3; ++k) d[k] += (double)s * c_khat64[(3 * ln + k) * 25];
-        for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j) blk[i][j] += (double)s * c_khat64[(3 * ln + i) + 24 * (3 * ln + j)];
+        for (int a = 0; a < 3; ++a) d3[a] += (double)s * ke64<NEN>((3 * ln + a) * (ND + 1));
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) blk[a][b] += (double)s * ke64<NEN>((3 * ln + a) + ND * (3 * ln + b));
       }
-  for (int k = 0; k < 3; ++k) d[k] *= D.scale;
-  const bool bnd = (x == 0 || x == D.L[0] || y == 0 || y == D.L[1] || z == 0 || z == D.L[2]);
+  for (int a = 0; a < 3; ++a) d3[a] *= D.scale;
+  const bool bnd = (x == 0 || x == D.n[0] - 1 || y == 0 || y == D.n[1] - 1 || z == 0 || z == D.n[2] - 1);
   const int64_t n = node_index(D, x, y, z);
   flags[n] = (active ? kNodeActive : 0) | (bnd ? kNodeBoundary : 0);
-  for (int k = 0; k < 3; ++k) {
-    const double di = (active && !bnd && d[k] != 0.0) ? 1.0 / d[k] : 0.0;
-    dinv64[n * 3 + k] = di;
-    dinv32[n * 3 + k] = (float)di;
+  for (int a = 0; a < 3; ++a) {
+    const double di = (active && !bnd && d3[a] != 0.0) ? 1.0 / d3[a] : 0.0;
+    dinv64[n * 3 + a] = di;
+    dinv32[n * 3 + a] = (float)di;
   }
-  // inverse of the node's 3x3 diagonal block (node-block Jacobi), symmetric: xx yy zz xy xz yz
   float bi[6] = {0, 0, 0, 0, 0, 0};
   if (active && !bnd) {
-    const double a = blk[0][0], b = blk[0][1], c = blk[0][2], e = blk[1][1], f = blk[1][2], g = blk[2][2];
-    const double c00 = e * g - f * f, c01 = c * f - b * g, c02 = b * f - c * e;
+    const double a = blk[0][0], b = blk[0][1], c = blk[0][2], e = blk[1][1], ff = blk[1][2], g = blk[2][2];
+    const double c00 = e * g - ff * ff, c01 = c * ff - b * g, c02 = b * ff - c * e;
     const double det = a * c00 + b * c01 + c * c02;
     if (det > 0.0) {
       const double inv = 1.0 / (det * D.scale);
@@ -223,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_node_setup(const Tile* __restrict_
       bi[2] = (float)((a * e - b * b) * inv);
       bi[3] = (float)(c01 * inv);
       bi[4] = (float)(c02 * inv);
-      bi[5] = (float)((b * c - a * f) * inv);
+      bi[5] = (float)((b * c - a * ff) * inv);
     }
   }
   for (int k = 0; k < 6; ++k) binv32[n * 6 + k] = bi[k];
@@ -251,7 +282,8 @@ __device__ __forceinline__ void node_xi(const DomDev& D, int x, int y, int z, do
   const int g[3] = {x, y, z};
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const double pos = (double)((int64_t)g[k] + (int64_t)D.min_c_off[k]) * D.delta;
+    const double pos = D.m == 1 ? (double)((int64_t)g[k] + (int64_t)D.min_c_off[k]) * D.delta
+                                : ((double)g[k] / (double)D.m + (double)D.min_c_off[k]) * D.delta;
     xi[k] = 2.0 / (D.max_c[k] - D.min_c[k]) * pos - (D.max_c[k] + D.min_c[k]) / (D.max_c[k] - D.min_c[k]);
   }
 }
@@ -271,7 +303,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __rest
   const DomDev D = doms[t.dom];
   const int x = t.x0 + (threadIdx.x & 7), row = threadIdx.x >> 3;
   const int y = t.y0 + (row & 3), z = t.z0 + (row >> 2);
-  if (x > D.L[0] || y > D.L[1] || z > D.L[2]) return;
+  if (x >= D.n[0] || y >= D.n[1] || z >= D.n[2]) return;
   const int64_t n = node_index(D, x, y, z);
   const uint8_t f = flags[n];
   if (!(f & kNodeActive) || !(f & kNodeBoundary)) return;
@@ -295,7 +327,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __rest
   const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);              \
   const int row = threadIdx.x >> 3;                                            \
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);                     \
-  const bool rowok = yy >= 1 && yy <= D.L[1] - 1 && zz >= 1 && zz <= D.L[2] - 1; \
+  const bool rowok = yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2; \
   const int64_t col = (int64_t)t.dom * kNLC + lc;
 
 // p = M^-1 r + bfac * p
@@ -310,7 +342,7 @@ __global__ void __launch_bounds__(kThreads) k_direction(const Tile* __restrict__
   const T bf = (T)st[col].bfac;
   for (int i = 0; i < kTileX; ++i) {
     const int x = t.x0 + i;
-    if (x > D.L[0] - 1) break;
+    if (x > D.n[0] - 2) break;
     const int64_t n = node_index(D, x, yy, zz);
     if (!(flags[n] & kNodeActive)) continue;
     const int64_t k0 = vec_index(n, 0, lc);
@@ -343,7 +375,7 @@ __global__ void __launch_bounds__(kThreads) k_update(const Tile* __restrict__ ti
     const T a = (T)(s.beta / pw);
     for (int i = 0; i < kTileX; ++i) {
       const int xx = t.x0 + i;
-      if (xx > D.L[0] - 1) break;
+      if (xx > D.n[0] - 2) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
       const int64_t k0 = vec_index(n, 0, lc);
@@ -386,7 +418,7 @@ __global__ void __launch_bounds__(kThreads) k_initial_dots(const Tile* __restric
   if (rowok) {
     for (int i = 0; i < kTileX; ++i) {
       const int xx = t.x0 + i;
-      if (xx > D.L[0] - 1) break;
+      if (xx > D.n[0] - 2) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
       const int64_t k0 = vec_index(n, 0, lc);
@@ -529,7 +561,7 @@ __global__ void __launch_bounds__(kThreads) k_residual_norm(const Tile* __restri
   if (rowok) {
     for (int i = 0; i < kTileX; ++i) {
       const int xx = t.x0 + i;
-      if (xx > D.L[0] - 1) break;
+      if (xx > D.n[0] - 2) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
 #pragma unroll
@@ -555,7 +587,7 @@ __global__ void __launch_bounds__(kThreads) k_start_inner(const Tile* __restrict
   const bool on = ost[col].active != 0;
   for (int i = 0; i < kTileX; ++i) {
     const int xx = t.x0 + i;
-    if (xx > D.L[0] - 1) break;
+    if (xx > D.n[0] - 2) break;
     const int64_t n = node_index(D, xx, yy, zz);
     if (!(flags[n] & kNodeActive)) continue;
 #pragma unroll
@@ -579,7 +611,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_correction(const Tile* __res
   if (!rowok || !ost[col].active) return;
   for (int i = 0; i < kTileX; ++i) {
     const int xx = t.x0 + i;
-    if (xx > D.L[0] - 1) break;
+    if (xx > D.n[0] - 2) break;
     const int64_t n = node_index(D, xx, yy, zz);
     if (!(flags[n] & kNodeActive)) continue;
 #pragma unroll
@@ -616,10 +648,10 @@ __global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ t
   double acc[24];
 #pragma unroll
   for (int k = 0; k < 24; ++k) acc[k] = 0.0;
-  if (yy <= D.L[1] && zz <= D.L[2]) {
+  if (yy < D.n[1] && zz < D.n[2]) {
     for (int i = 0; i < kTileX; ++i) {
       const int xx = t.x0 + i;
-      if (xx > D.L[0]) break;
+      if (xx >= D.n[0]) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
       double xi[3], N[8];
@@ -663,10 +695,10 @@ __global__ void __launch_bounds__(kThreads) k_energy_gram(const Tile* __restrict
   double acc[24];
 #pragma unroll
   for (int k = 0; k < 24; ++k) acc[k] = 0.0;
-  if (yy <= D.L[1] && zz <= D.L[2]) {
+  if (yy < D.n[1] && zz < D.n[2]) {
     for (int i = 0; i < kTileX; ++i) {
       const int xx = t.x0 + i;
-      if (xx > D.L[0]) break;
+      if (xx >= D.n[0]) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
 #pragma unroll
@@ -746,7 +778,7 @@ struct DeviceSolver::Impl {
 namespace {
 
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
-           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bNumBufs };
+           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bNumBufs };
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
   if (I.caps[which] >= bytes && I.bufs[which]) return DTC_OK;
@@ -796,11 +828,58 @@ int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg);
 namespace {
 
 // CG on one precision: x (interior part), r = b on entry, p = 0 on entry.
-template <typename T, bool BLOCK>
-int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w, const T* dinv, double rtol,
-           const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
+template <typename T, int NEN, bool ALL, bool DOT>
+void launch_ebe(const Tile* bricks, int64_t nb, const DomDev* dd, const float* svox, const uint8_t* fl, const T* u, T* y,
+                double scale, double* acc, const int* act, cudaStream_t s) {
+  using S = EbeShape<T, NEN>;
+  if (nb <= 0) return;
+  k_ebe<T, NEN, ALL, DOT><<<(unsigned)(S::NGRP * nb), S::kThreadsEbe, S::smem, s>>>(bricks, dd, svox, fl, u, y, scale,
+                                                                                    acc, act);
+}
+
+template <typename T, int NEN, bool ALL, bool DOT>
+int allow_ebe_smem(std::string& msg) {
+  DTC_CUDA(cudaFuncSetAttribute(k_ebe<T, NEN, ALL, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)EbeShape<T, NEN>::smem));
+  return DTC_OK;
+}
+
+template <int NEN>
+int allow_all_ebe(std::string& msg) {
+  int e;
+  if ((e = allow_ebe_smem<float, NEN, false, true>(msg))) return e;
+  if ((e = allow_ebe_smem<double, NEN, false, true>(msg))) return e;
+  if ((e = allow_ebe_smem<double, NEN, false, false>(msg))) return e;
+  if ((e = allow_ebe_smem<double, NEN, true, false>(msg))) return e;
+  return DTC_OK;
+}
+
+// Work lists of one solve: node tiles (vector kernels and the HEX08 node-centric operator)
+// and voxel bricks (HEX20 element-by-element operator), over the interior / all nodes.
+struct Work {
+  const Tile *ti, *ta, *bi, *ba;
+  int64_t nti, nta, nbi, nba;
+};
+
+// y = scale * K u on the interior (ALL = false) or every node; DOT: acc[col] += u . y.
+template <typename T, int NEN, bool ALL, bool DOT>
+void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* fl, const T* u, T* y, double scale,
+             double* acc, const int* act, cudaStream_t s) {
+  if constexpr (NEN == 8) {
+    const int64_t nt = ALL ? W.nta : W.nti;
+    if (nt > 0)
+      k_matvec<T, ALL, DOT><<<(unsigned)(3 * nt), kThreads, 0, s>>>(ALL ? W.ta : W.ti, dd, svox, u, y, scale, acc, act);
+  } else {
+    launch_ebe<T, NEN, ALL, DOT>(ALL ? W.ba : W.bi, ALL ? W.nba : W.nbi, dd, svox, fl, u, y, scale, acc, act, s);
+  }
+}
+
+template <typename T, bool BLOCK, int NEN>
+int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* w, const T* dinv,
+           double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
   cudaStream_t s = I.stream;
-  const Tile* ti = B<Tile>(I, bTilesI);
+  const Tile* ti = W.ti;
+  const int64_t nti = W.nti;
   const DomDev* dd = B<DomDev>(I, bDoms);
   const uint8_t* fl = B<uint8_t>(I, bFlags);
   ColState* st = B<ColState>(I, bSt);
@@ -830,11 +909,11 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
         k_direction<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
         I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
         q = I.begin(0);
-        if (sizeof(T) == 4 && I.tensor_matvec)
+        if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
           launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
                            B<int>(I, bErr), s);
         else
-          k_matvec<T, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+          apply_k<T, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
         I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
         q = I.begin(0);
         k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
@@ -862,8 +941,9 @@ int run_cg(DeviceSolver::Impl& I, int ndom, int64_t nti, T* x, T* r, T* p, T* w,
 
 }  // namespace
 
-int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg) {
-  Impl& I = *impl_;
+template <int NEN>
+int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask>& tasks, const dtc_options& opt,
+              double nu, std::string& msg) {
   DTC_CUDA(cudaSetDevice(I.device));
   cudaStream_t s = I.stream;
   stats_ = SolverStats();
@@ -889,10 +969,22 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
     if (int e = upload_tc_operand(kh, s, msg)) return e;
+    if (NEN == 20) {
+      std::vector<double> k20(3600);
+      std::vector<float> k20f(3600);
+      voxel_stiffness(20, nu, k20.data());
+      for (int i = 0; i < 3600; ++i) k20f[i] = (float)k20[i];
+      DTC_CUDA(cudaMemcpyToSymbolAsync(c_k20_64, k20.data(), sizeof(double) * 3600, 0, cudaMemcpyHostToDevice, s));
+      DTC_CUDA(cudaMemcpyToSymbolAsync(c_k20_32, k20f.data(), sizeof(float) * 3600, 0, cudaMemcpyHostToDevice, s));
+    }
+    if constexpr (NEN == 20)
+      if (int e = allow_all_ebe<NEN>(msg)) return e;   // per device, cheap
   }
   // pack the batch (all solvable tasks at once; chunking by memory happens in the caller)
+  using EL = Elem<NEN>;
+  constexpr int m = EL::M;
   std::vector<DomDev> doms;
-  std::vector<Tile> tiles_i, tiles_a;
+  std::vector<Tile> tiles_i, tiles_a, bricks_i, bricks_a;
   std::vector<float> svox;
   std::vector<int64_t> tidx;
   int64_t node_total = 0;
@@ -902,7 +994,8 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     if (mp.status != DTC_DOMAIN_OK) continue;
     const dtc_domain_in& in = *t.in;
     DomDev D{};
-    for (int d = 0; d < 3; ++d) { D.L[d] = (int32_t)in.L[d]; D.n[d] = (int32_t)in.L[d] + 1; }
+    D.m = m;
+    for (int d = 0; d < 3; ++d) { D.L[d] = (int32_t)in.L[d]; D.n[d] = m * (int32_t)in.L[d] + 1; }
     D.vox_off = (int64_t)svox.size();
     D.node_off = node_total;
     D.delta = in.delta[0];
@@ -918,53 +1011,63 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     svox.resize(svox.size() + nvox);
     float* sv = svox.data() + D.vox_off;
     for (int64_t v = 0; v < nvox; ++v) sv[v] = mp.kept[v] ? (in.E_voxel ? in.E_voxel[v] : 1.0f) : 0.0f;
-    // node activity on the host for the tile lists
+    // node activity on the (fine) grid for the work lists; kept voxels per node for the flop count
     const int nx = D.n[0], ny = D.n[1], nz = D.n[2];
     std::vector<uint8_t> act((size_t)nx * ny * nz, 0);
+    double kept = 0;
     for (int64_t v = 0; v < nvox; ++v) {
       if (sv[v] == 0.0f) continue;
+      kept += 1;
       const int vx = (int)(v % in.L[0]), vy = (int)((v / in.L[0]) % in.L[1]), vz = (int)(v / (in.L[0] * in.L[1]));
-      for (int c = 0; c < 2; ++c)
-        for (int b = 0; b < 2; ++b)
-          for (int a2 = 0; a2 < 2; ++a2) act[(vx + a2) + (size_t)nx * ((vy + b) + (size_t)ny * (vz + c))] = 1;
+      for (int c = 0; c <= m; ++c)
+        for (int b2 = 0; b2 <= m; ++b2)
+          for (int a2 = 0; a2 <= m; ++a2) {
+            const int odd = (a2 == 1) + (b2 == 1) + (c == 1);
+            if (m == 2 && odd > 1) continue;   // HEX20 has no face or body nodes
+            act[(m * vx + a2) + (size_t)nx * ((m * vy + b2) + (size_t)ny * (m * vz + c))] = 1;
+          }
     }
-    // algorithmic work of one launch on this domain (elements of T per vector; flops):
-    // vector kernels touch 72 values per active interior node per vector; the matvec reads
-    // p and writes w (2 vectors) plus one float per voxel; its flops are, per active
-    // interior node and load case, 150 per kept neighbouring voxel (3 rows x 24 FMA + scale).
+    // algorithmic work of one launch on this domain, in elements of T per vector (bytes later)
+    // and flops: vector kernels touch 72 values per active interior node per vector; the
+    // stiffness application reads the input and writes the output (2 vectors) plus one
+    // float per voxel, and costs 2 * (3 NEN)^2 flops per kept voxel and load case.
     {
-      double nint = 0, kv = 0;
+      double nint = 0;
       for (int z = 1; z < nz - 1; ++z)
         for (int y = 1; y < ny - 1; ++y)
-          for (int x = 1; x < nx - 1; ++x) {
-            if (!act[x + (size_t)nx * (y + (size_t)ny * z)]) continue;
-            nint += 1;
-            for (int c = 0; c < 2; ++c)
-              for (int b = 0; b < 2; ++b)
-                for (int a2 = 0; a2 < 2; ++a2)
-                  kv += sv[(x - 1 + a2) + in.L[0] * ((y - 1 + b) + in.L[1] * (int64_t)(z - 1 + c))] != 0.0f;
-          }
+          for (int x = 1; x < nx - 1; ++x) nint += act[x + (size_t)nx * (y + (size_t)ny * z)];
       I.dom_vec_bytes.push_back(72.0 * nint);
-      I.dom_mv_bytes.push_back(2 * 72.0 * nint + (double)nvox * 4.0 / 4.0);
-      I.dom_mv_flops.push_back(kv * 150.0 * kNLC);
+      I.dom_mv_bytes.push_back(2 * 72.0 * nint + (double)nvox);
+      I.dom_mv_flops.push_back(kept * 2.0 * (3 * NEN) * (3 * NEN) * kNLC);
     }
-    auto tile_active = [&](int x0, int y0, int z0, int lo, int hx, int hy, int hz) {
-      for (int z = z0; z < std::min(z0 + kTileZ, hz + 1); ++z)
-        for (int y = y0; y < std::min(y0 + kTileY, hy + 1); ++y)
-          for (int x = x0; x < std::min(x0 + kTileX, hx + 1); ++x)
-            if (x >= lo && y >= lo && z >= lo && act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
+    auto any_active = [&](int x0, int y0, int z0, int sx, int sy, int sz, int lo, int hx, int hy, int hz) {
+      for (int z = std::max(z0, lo); z < std::min(z0 + sz, hz + 1); ++z)
+        for (int y = std::max(y0, lo); y < std::min(y0 + sy, hy + 1); ++y)
+          for (int x = std::max(x0, lo); x < std::min(x0 + sx, hx + 1); ++x)
+            if (act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
       return false;
     };
-    for (int z0 = 1; z0 <= (int)in.L[2] - 1; z0 += kTileZ)
-      for (int y0 = 1; y0 <= (int)in.L[1] - 1; y0 += kTileY)
-        for (int x0 = 1; x0 <= (int)in.L[0] - 1; x0 += kTileX)
-          if (tile_active(x0, y0, z0, 1, in.L[0] - 1, in.L[1] - 1, in.L[2] - 1))
+    // node tiles (vector kernels) over the interior / all nodes
+    for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
+      for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
+        for (int x0 = 1; x0 <= nx - 2; x0 += kTileX)
+          if (any_active(x0, y0, z0, kTileX, kTileY, kTileZ, 1, nx - 2, ny - 2, nz - 2))
             tiles_i.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
-    for (int z0 = 0; z0 <= (int)in.L[2]; z0 += kTileZ)
-      for (int y0 = 0; y0 <= (int)in.L[1]; y0 += kTileY)
-        for (int x0 = 0; x0 <= (int)in.L[0]; x0 += kTileX)
-          if (tile_active(x0, y0, z0, 0, in.L[0], in.L[1], in.L[2]))
+    for (int z0 = 0; z0 <= nz - 1; z0 += kTileZ)
+      for (int y0 = 0; y0 <= ny - 1; y0 += kTileY)
+        for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
+          if (any_active(x0, y0, z0, kTileX, kTileY, kTileZ, 0, nx - 1, ny - 1, nz - 1))
             tiles_a.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+    // voxel bricks (HEX20 operator): brick origin in voxels, owned nodes m*origin + [0, m*B)
+    for (int bz = 0; NEN == 20 && m * bz <= nz - 1; bz += EL::BZ)
+      for (int by = 0; m * by <= ny - 1; by += EL::BY)
+        for (int bx = 0; m * bx <= nx - 1; bx += EL::BX) {
+          const int ox = m * bx, oy = m * by, oz = m * bz;
+          if (any_active(ox, oy, oz, m * EL::BX, m * EL::BY, m * EL::BZ, 1, nx - 2, ny - 2, nz - 2))
+            bricks_i.push_back(Tile{dom, (int16_t)bx, (int16_t)by, (int16_t)bz, 0});
+          if (any_active(ox, oy, oz, m * EL::BX, m * EL::BY, m * EL::BZ, 0, nx - 1, ny - 1, nz - 1))
+            bricks_a.push_back(Tile{dom, (int16_t)bx, (int16_t)by, (int16_t)bz, 0});
+        }
     node_total += (int64_t)nx * ny * nz;
     doms.push_back(D);
     tidx.push_back((int64_t)k);
@@ -972,12 +1075,15 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   const int ndom = (int)doms.size();
   if (ndom == 0) return DTC_OK;
   const int64_t nti = (int64_t)tiles_i.size(), nta = (int64_t)tiles_a.size();
+  const int64_t nbi = (int64_t)bricks_i.size(), nba = (int64_t)bricks_a.size();
   const size_t vbytes64 = sizeof(double) * node_total * 3 * kNLC, vbytes32 = sizeof(float) * node_total * 3 * kNLC;
   const bool mixed = opt.precision == DTC_PREC_MIXED;
   int e;
   if ((e = ensure(I, bDoms, sizeof(DomDev) * ndom, msg))) return e;
   if ((e = ensure(I, bTilesI, sizeof(Tile) * std::max<int64_t>(nti, 1), msg))) return e;
   if ((e = ensure(I, bTilesA, sizeof(Tile) * std::max<int64_t>(nta, 1), msg))) return e;
+  if ((e = ensure(I, bBricksI, sizeof(Tile) * std::max<int64_t>(nbi, 1), msg))) return e;
+  if ((e = ensure(I, bBricksA, sizeof(Tile) * std::max<int64_t>(nba, 1), msg))) return e;
   if ((e = ensure(I, bSvox, sizeof(float) * svox.size(), msg))) return e;
   if ((e = ensure(I, bFlags, node_total, msg))) return e;
   if ((e = ensure(I, bDinv64, sizeof(double) * node_total * 3, msg))) return e;
@@ -1011,6 +1117,8 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   DTC_CUDA(cudaMemcpyAsync(I.bufs[bDoms], doms.data(), sizeof(DomDev) * ndom, cudaMemcpyHostToDevice, s));
   if (nti) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesI], tiles_i.data(), sizeof(Tile) * nti, cudaMemcpyHostToDevice, s));
   if (nta) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesA], tiles_a.data(), sizeof(Tile) * nta, cudaMemcpyHostToDevice, s));
+  if (nbi) DTC_CUDA(cudaMemcpyAsync(I.bufs[bBricksI], bricks_i.data(), sizeof(Tile) * nbi, cudaMemcpyHostToDevice, s));
+  if (nba) DTC_CUDA(cudaMemcpyAsync(I.bufs[bBricksA], bricks_a.data(), sizeof(Tile) * nba, cudaMemcpyHostToDevice, s));
   DTC_CUDA(cudaMemcpyAsync(I.bufs[bSvox], svox.data(), sizeof(float) * svox.size(), cudaMemcpyHostToDevice, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bFlags], 0, node_total, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv64], 0, sizeof(double) * node_total * 3, s));
@@ -1020,6 +1128,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * 576 * ndom, s));
   const Tile* ti = B<Tile>(I, bTilesI);
   const Tile* ta = B<Tile>(I, bTilesA);
+  const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba};
   const DomDev* dd = B<DomDev>(I, bDoms);
   uint8_t* fl = B<uint8_t>(I, bFlags);
   double* X = B<double>(I, bX);
@@ -1027,7 +1136,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   int64_t& L = stats_.kernel_launches;
   if (nta) {
     DTC_CUDA(cudaMemsetAsync(I.bufs[bBinv32], 0, sizeof(float) * node_total * 6, s));
-    k_node_setup<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
+    k_node_setup<NEN><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
                                                     B<float>(I, bDinv32), B<float>(I, bBinv32));
     k_boundary_values<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, fl, X);
     L += 2;
@@ -1039,8 +1148,9 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
     DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
-    if (nti) { k_matvec<double, false, false><<<gi, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), X, R64, -1.0, nullptr, nullptr); ++L; }
-    if ((e = run_cg<double, false>(I, ndom, nti, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
+    apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
+    ++L;
+    if ((e = run_cg<double, false, NEN>(I, ndom, W, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
                             opt.rtol, nullptr, opt.max_it, L, msg)))
       return e;
     DTC_CUDA(cudaMemcpyAsync(ost, I.bufs[bSt], sizeof(ColState) * ncol, cudaMemcpyDeviceToDevice, s));
@@ -1056,7 +1166,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
     for (int step = 0; step <= max_refine; ++step) {
       DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
       if (nti) {
-        k_matvec<double, false, false><<<gi, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), X, R64, -1.0, nullptr, nullptr);
+        apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
         k_residual_norm<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<double>(I, bDinv64), R64, B<double>(I, bZz));
         L += 2;
       }
@@ -1072,11 +1182,11 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
       if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
       DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
       if (opt.inner_precond == 1)
-        e = run_cg<float, true>(I, ndom, nti, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
+        e = run_cg<float, true, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
                                 B<float>(I, bW32), B<float>(I, bBinv32), inner, B<double>(I, bTarget), inner_budget,
                                 L, msg);
       else
-        e = run_cg<float, false>(I, ndom, nti, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
+        e = run_cg<float, false, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
                                  B<float>(I, bW32), B<float>(I, bDinv32), inner, B<double>(I, bTarget), inner_budget,
                                  L, msg);
       if (e) return e;
@@ -1089,7 +1199,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff)
   DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
   if (nta) {
-    k_matvec<double, true, false><<<ga, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), X, R64, 1.0, nullptr, nullptr);
+    apply_k<double, NEN, true, false>(W, dd, B<float>(I, bSvox), fl, X, R64, 1.0, nullptr, nullptr, s);
     if (opt.tensor_estimator == 1)
       k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf));
     else
@@ -1144,7 +1254,7 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
       const DomDev& D = doms[d];
       for (int64_t id = 0; id < nn; ++id) {
         const int64_t g = mp.node_grid[id];
-        const int64_t node = D.node_off + g;  // HEX08 node grid == device node grid
+        const int64_t node = D.node_off + g;  // the mesher's grid index is the device node index
         for (int c = 0; c < 3; ++c)
           for (int lc = 0; lc < kNLC; ++lc) {
             const size_t src = (size_t)((node * 3 + c) * kNLC + lc);
@@ -1157,6 +1267,18 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   I.last_doms = doms;
   I.last_task_index = tidx;
   return DTC_OK;
+}
+
+int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg) {
+  int nen = 0;
+  for (const DomainTask& t : tasks) {
+    if (t.plan->status != DTC_DOMAIN_OK) continue;
+    if (nen && t.in->elem_type != nen) { msg = "all domains of one solve must share the element type"; return DTC_ERR_INVALID_ARGUMENT; }
+    nen = t.in->elem_type;
+  }
+  if (nen == 0) return DTC_OK;
+  DTC_CUDA(cudaSetDevice(impl_->device));
+  return nen == 20 ? solve_nen<20>(*impl_, stats_, tasks, opt, nu, msg) : solve_nen<8>(*impl_, stats_, tasks, opt, nu, msg);
 }
 
 int DeviceSolver::energy_grad(const double*, float* const*, int64_t, std::string& msg) {

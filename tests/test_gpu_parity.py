@@ -123,3 +123,76 @@ def test_rotation_matches_oracle(dtc, orc, batch):
         a, b = r[k], ref[k]
         assert abs(a["crit"] - b["crit"]) <= 1e-9 + 1e-6 * abs(b["crit"])
         assert rel(np.diag(a["ee"]), np.diag(b["ee"])) <= 1e-6
+
+
+# ---------------------------------------------------------------- HEX20 (20-node serendipity bricks)
+
+def make_pair20(dtc, orc, shape, bvtv, seed, E_voxel=False):
+    syn = dtc.synth
+    gray = syn.bone_volume(shape, bvtv, seed)
+    ev = syn.modulus_of_gray(gray) if E_voxel else None
+    d = dtc.Domain(gray, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=ev)
+    o = orc.Domain(gray, nen=20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, E_voxel=ev)
+    return d, o
+
+
+@pytest.fixture(scope="module")
+def batch20(dtc, orc):
+    pairs = [make_pair20(dtc, orc, (8, 8, 8), b, dtc.synth.seed_for(20, i)) for i, b in enumerate((0.2, 0.4))]
+    pairs.append(make_pair20(dtc, orc, (7, 9, 6), 0.45, dtc.synth.seed_for(20, 5)))   # non-cubic box
+    pairs.append(make_pair20(dtc, orc, (8, 8, 8), 0.3, dtc.synth.seed_for(20, 6), E_voxel=True))
+    refs = orc.solve_batch([p[1] for p in pairs])
+    return pairs, refs
+
+
+def test_hex20_fp64_matches_oracle(dtc, batch20):
+    pairs, refs = batch20
+    with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False) as s:
+        res = s.solve([p[0] for p in pairs])
+    for r, ref in zip(res, refs):
+        assert r["status"] == ref["status"] == 0
+        assert (r["ne"], r["nn"], r["nb"]) == (ref["ne"], ref["nn"], ref["nb"])
+        assert rel(r["c"], ref["c"]) <= TOL_FP64
+        assert rel(r["ff"], ref["ff"]) <= TOL_FP64
+        assert np.abs(r["iters"] - ref["iters"]).max() <= 2
+
+
+@pytest.mark.parametrize("precond", ["block", "jacobi"])
+def test_hex20_mixed_matches_oracle(dtc, batch20, precond):
+    pairs, refs = batch20
+    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, inner_precond=precond) as s:
+        res = s.solve([p[0] for p in pairs])
+    for r, ref in zip(res, refs):
+        assert r["status"] == 0
+        assert rel(r["c"], ref["c"]) <= TOL_MIXED
+
+
+def test_hex20_fields_in_reference_numbering(dtc, orc):
+    d, o = make_pair20(dtc, orc, (6, 6, 6), 0.45, dtc.synth.seed_for(20, 9))
+    ref = orc.solve_domain(o, with_arrays=True)
+    with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False) as s:
+        r = s.solve([d], want_fields=True)[0]
+    assert r["displ"].shape == ref["displ"].shape
+    assert rel(r["displ"], ref["displ"]) <= 1e-7
+    assert rel(r["force"], ref["force"]) <= 1e-6
+
+
+def test_hex20_solid_cube_isotropic(dtc):
+    """Affine fields are exact for both element types: C of a solid cube is the material's."""
+    E, nu = 5600.0, 0.3
+    gray = np.full((4, 4, 4), 14250, np.int16)
+    with dtc.Solver(precision="fp64", rtol=1e-12, rotation_search=False) as s:
+        r = s.solve([dtc.Domain(gray, elem_type=dtc.HEX20, E=E, nu=nu, delta=0.01)])[0]
+    lam, mu = E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))
+    C = np.zeros((6, 6))
+    C[:3, :3] = lam
+    C[range(3), range(3)] += 2 * mu
+    C[3, 3] = C[4, 4] = C[5, 5] = mu
+    assert rel(r["c"], C) < 1e-8
+
+
+def test_mixed_element_types_rejected(dtc):
+    gray = np.full((4, 4, 4), 100, np.int16)
+    with dtc.Solver(precision="fp64", rtol=1e-8, rotation_search=False) as s:
+        with pytest.raises(Exception, match="elem_type"):
+            s.solve([dtc.Domain(gray), dtc.Domain(gray, elem_type=dtc.HEX20)])
