@@ -40,6 +40,8 @@ def parse():
     p.add_argument("--L", type=int, default=32)
     p.add_argument("--rtol", type=float, default=0.0, help="0: calibrate per arm to the accuracy target")
     p.add_argument("--estimator", default="energy", choices=["energy", "reaction"])
+    p.add_argument("--precond", default="mg", choices=["mg", "block", "jacobi"],
+                   help="preconditioner of the FP32 inner solve of the mixed arm")
     p.add_argument("--max-it", type=int, default=20000)
     p.add_argument("--check", type=int, default=16, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
@@ -201,7 +203,7 @@ def main():
         return max(float(np.abs(r["c"] - t).max() / np.abs(t).max()) for r, t in zip(res, truth))
 
     ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8, 3e-9, 1e-9]
-    arms = {"mixed": dict(precision="mixed", estimator=args.estimator),
+    arms = {"mixed": dict(precision="mixed", estimator=args.estimator, inner_precond=args.precond),
             "fp64": dict(precision="fp64", estimator="reaction")}
     rtol_of, err_of = {}, {}
     for arm, kw in arms.items():
@@ -215,7 +217,7 @@ def main():
             rtol_of[arm], err_of[arm] = ladder[-1], e
 
     mixed = dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
-                       device=local, estimator=args.estimator)
+                       device=local, estimator=args.estimator, inner_precond=args.precond)
 
     def barrier():
         torch.cuda.synchronize()
@@ -258,7 +260,8 @@ def main():
     peak, src = measured_peaks()
     # dominant kernel: one extra, untimed-for-the-metric step with CUDA-event timing per launch
     with dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
-                    device=local, profile_kernels=True, estimator=args.estimator) as prof:
+                    device=local, profile_kernels=True, estimator=args.estimator,
+                    inner_precond=args.precond) as prof:
         prof.solve(doms)
         ks = prof.kernel_stats()
     top = max(ks, key=lambda k: ks[k]["ms_total"])
@@ -272,7 +275,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": workload(args),
-                "rtol": rtol_of["mixed"], "estimator": args.estimator,
+                "rtol": rtol_of["mixed"], "estimator": args.estimator, "inner_precond": args.precond,
                 "max_rel_err_vs_fp64_1e-10": timed_err, "accuracy_target": TARGET, "accuracy_sample": nchk,
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),

@@ -103,7 +103,7 @@ class Solver:
         o.keep_displacements = int(bool(keep_displacements))
         o.profile_kernels = int(bool(profile_kernels))
         o.mixed_matvec = {"simt": 0, "tensor": 1}[mixed_matvec]
-        o.inner_precond = {"jacobi": 0, "block": 1}[inner_precond]
+        o.inner_precond = {"jacobi": 0, "block": 1, "mg": 2}[inner_precond]
         o.tensor_estimator = {"reaction": 0, "energy": 1}[estimator]
         self.options = o
         h = C.c_void_p()

@@ -134,6 +134,9 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
   }
   if (!(o.rtol > 0 && o.rtol < 1) || o.max_it < 1 || (o.precision != DTC_PREC_FP64 && o.precision != DTC_PREC_MIXED))
     return DTC_ERR_INVALID_ARGUMENT;
+  if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 1 ||
+      o.tensor_estimator < 0 || o.tensor_estimator > 1)
+    return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
   h->opt = o;

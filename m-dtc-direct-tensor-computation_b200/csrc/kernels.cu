@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ ti
 }  // namespace dtc
 
 #include "ebe.cuh"
+#include "mg.cuh"
 
 namespace dtc {
 
@@ -729,8 +730,8 @@ struct DeviceSolver::Impl {
   cudaStream_t stream = nullptr;
   // persistent buffers grown on demand
   std::vector<std::pair<void**, size_t>> owned;
-  void* bufs[32] = {nullptr};
-  size_t caps[32] = {0};
+  void* bufs[64] = {nullptr};
+  size_t caps[64] = {0};
   // last solve kept for the adjoint
   std::vector<DomDev> last_doms;
   std::vector<int64_t> last_task_index;
@@ -778,7 +779,10 @@ struct DeviceSolver::Impl {
 namespace {
 
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
-           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bNumBufs };
+           bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
+           bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
+           bNumBufs };
+static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
   if (I.caps[which] >= bytes && I.bufs[which]) return DTC_OK;
@@ -874,6 +878,273 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
   }
 }
 
+
+// -------------------------------------------------------------------------------------
+// Multigrid hierarchy of one solve (HEX08, FP32 inner solve).  Level 0 is the fine grid
+// already packed; levels >= 1 live in their own node / voxel arrays.  Per level: DomDev for
+// every domain (L = 0 where the domain has no such level), interior tiles of the domains that
+// smooth on the level (sm), interior tiles of every domain present (in: restriction target),
+// all tiles (node set-up), and the domains whose coarsest level it is (dense solve).
+struct MgPlan {
+  int nlev = 0;
+  float omega = 0.f;
+  std::vector<DomDev> doms;                         // nlev * ndom, level-major
+  std::vector<Tile> tiles;
+  std::vector<int64_t> sm_off, sm_n, in_off, in_n, all_off, all_n;
+  std::vector<int> lists;
+  std::vector<int64_t> list_off, list_n;
+  std::vector<float> svox;                          // voxels of levels >= 1
+  std::vector<float> minv;                          // ndom * 81 * 81
+  int64_t nodes = 0;                                // nodes of levels >= 1
+};
+
+// lambda_max of De^-1/2 Khat De^-1/2 (unit voxel, scalar diagonal De): bounds
+// lambda_max(D^-1 K) of every assembly of scaled voxels, D the assembled diagonal.
+double jacobi_bound(const double* kh) {
+  double v[24], w[24], lam = 0;
+  for (int i = 0; i < 24; ++i) v[i] = 1.0 + 0.01 * i;
+  for (int it = 0; it < 2000; ++it) {
+    double nrm = 0;
+    for (int i = 0; i < 24; ++i) {
+      double s = 0;
+      for (int j = 0; j < 24; ++j) s += kh[i + 24 * j] / std::sqrt(kh[i * 25] * kh[j * 25]) * v[j];
+      w[i] = s;
+      nrm += s * s;
+    }
+    nrm = std::sqrt(nrm);
+    double rq = 0;
+    for (int i = 0; i < 24; ++i) rq += v[i] * w[i];
+    double vn = 0;
+    for (int i = 0; i < 24; ++i) vn += v[i] * v[i];
+    lam = rq / vn;
+    for (int i = 0; i < 24; ++i) v[i] = w[i] / nrm;
+  }
+  return lam;
+}
+
+// Dense inverse of the coarsest operator over its <= 27 interior nodes (FP64 Cholesky; pivots
+// below 1e-12 of the largest diagonal entry are dropped, so floating pieces without a fixed
+// node get a zero correction), stored as float 81 x 81.
+void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* out) {
+  constexpr int N = kMgDenseN;
+  double A[N * N];
+  std::memset(A, 0, sizeof(A));
+  const int ix = D.n[0] - 2, iy = D.n[1] - 2, iz = D.n[2] - 2;
+  auto dof = [&](int x, int y, int z, int c) -> int {
+    if (x < 1 || y < 1 || z < 1 || x > ix || y > iy || z > iz) return -1;
+    return 3 * ((x - 1) + 3 * (y - 1) + 9 * (z - 1)) + c;
+  };
+  for (int vz = 0; vz < D.L[2]; ++vz)
+    for (int vy = 0; vy < D.L[1]; ++vy)
+      for (int vx = 0; vx < D.L[0]; ++vx) {
+        const double s = (double)sv[vx + D.L[0] * (vy + D.L[1] * vz)] * D.scale;
+        if (s == 0.0) continue;
+        for (int a = 0; a < 8; ++a)
+          for (int ca = 0; ca < 3; ++ca) {
+            const int ra = dof(vx + Elem<8>::off(a, 0), vy + Elem<8>::off(a, 1), vz + Elem<8>::off(a, 2), ca);
+            if (ra < 0) continue;
+            for (int b = 0; b < 8; ++b)
+              for (int cb = 0; cb < 3; ++cb) {
+                const int rb = dof(vx + Elem<8>::off(b, 0), vy + Elem<8>::off(b, 1), vz + Elem<8>::off(b, 2), cb);
+                if (rb < 0) continue;
+                A[ra * N + rb] += s * kh[(3 * a + ca) + 24 * (3 * b + cb)];
+              }
+          }
+      }
+  double dmax = 0;
+  for (int i = 0; i < N; ++i) dmax = std::max(dmax, A[i * N + i]);
+  bool keep[N];
+  double Lc[N * N];
+  std::memset(Lc, 0, sizeof(Lc));
+  for (int j = 0; j < N; ++j) {
+    double d = A[j * N + j];
+    for (int k = 0; k < j; ++k) d -= Lc[j * N + k] * Lc[j * N + k];
+    keep[j] = dmax > 0 && d > 1e-12 * dmax;
+    if (!keep[j]) continue;
+    const double ljj = std::sqrt(d);
+    Lc[j * N + j] = ljj;
+    for (int i = j + 1; i < N; ++i) {
+      double s = A[i * N + j];
+      for (int k = 0; k < j; ++k) s -= Lc[i * N + k] * Lc[j * N + k];
+      Lc[i * N + j] = s / ljj;
+    }
+  }
+  // inverse column by column: L L^T x = e_c on the kept DOFs
+  for (int c = 0; c < N; ++c) {
+    double y[N];
+    for (int i = 0; i < N; ++i) {
+      if (!keep[i]) { y[i] = 0; continue; }
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) s -= Lc[i * N + k] * y[k];
+      y[i] = s / Lc[i * N + i];
+    }
+    for (int i = N - 1; i >= 0; --i) {
+      if (!keep[i]) { y[i] = 0; continue; }
+      double s = y[i];
+      for (int k = i + 1; k < N; ++k) s -= Lc[k * N + i] * y[k];
+      y[i] = s / Lc[i * N + i];
+    }
+    for (int i = 0; i < N; ++i) out[i * N + c] = keep[c] ? (float)y[i] : 0.f;
+  }
+}
+
+// Build the hierarchy on the host from the fine voxel factors.  fine_i: interior tiles of the
+// fine level (level-0 smoothing tiles are those of domains with a coarser level).
+void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<float>& svox0,
+              const std::vector<Tile>& fine_i, double nu) {
+  const int ndom = (int)doms0.size();
+  double kh[576];
+  voxel_stiffness(8, nu, kh);
+  const double lam = jacobi_bound(kh);
+  P.omega = (float)(1.0 / (0.5 * (1.1 + 1.0 / 30.0) * lam));
+  std::vector<int> nlev(ndom, 1);
+  int nl = 1;
+  for (int d = 0; d < ndom; ++d) {
+    int L[3] = {doms0[d].L[0], doms0[d].L[1], doms0[d].L[2]};
+    while (std::max(L[0], std::max(L[1], L[2])) > kMgMaxCoarse) {
+      for (int k = 0; k < 3; ++k) L[k] = (L[k] + 1) / 2;
+      ++nlev[d];
+    }
+    nl = std::max(nl, nlev[d]);
+  }
+  P.nlev = nl;
+  P.doms.assign((size_t)nl * ndom, DomDev{});
+  P.sm_off.assign(nl, 0); P.sm_n.assign(nl, 0); P.in_off.assign(nl, 0); P.in_n.assign(nl, 0);
+  P.all_off.assign(nl, 0); P.all_n.assign(nl, 0); P.list_off.assign(nl, 0); P.list_n.assign(nl, 0);
+  P.tiles.clear(); P.lists.clear(); P.svox.clear(); P.nodes = 0;
+  P.minv.assign((size_t)ndom * kMgDenseN * kMgDenseN, 0.f);
+  for (int d = 0; d < ndom; ++d) P.doms[d] = doms0[d];
+  // level 0 smoothing tiles
+  P.sm_off[0] = 0;
+  for (const Tile& t : fine_i) if (nlev[t.dom] > 1) P.tiles.push_back(t);
+  P.sm_n[0] = (int64_t)P.tiles.size();
+  std::vector<std::vector<float>> cur(ndom);   // voxel factors of the current level per domain
+  for (int d = 0; d < ndom; ++d) cur[d].assign(svox0.begin() + doms0[d].vox_off,
+                                               svox0.begin() + doms0[d].vox_off +
+                                                   (int64_t)doms0[d].L[0] * doms0[d].L[1] * doms0[d].L[2]);
+  for (int l = 1; l < nl; ++l) {
+    std::vector<Tile> t_in, t_sm, t_all;
+    for (int d = 0; d < ndom; ++d) {
+      if (nlev[d] <= l) continue;
+      const DomDev& F = P.doms[(size_t)(l - 1) * ndom + d];
+      DomDev C = F;
+      for (int k = 0; k < 3; ++k) { C.L[k] = (F.L[k] + 1) / 2; C.n[k] = C.L[k] + 1; }
+      C.m = 1;
+      C.scale = 2.0 * F.scale;
+      C.vox_off = (int64_t)P.svox.size();
+      C.node_off = P.nodes;
+      std::vector<float> nv((size_t)C.L[0] * C.L[1] * C.L[2], 0.f);
+      for (int z = 0; z < F.L[2]; ++z)
+        for (int y = 0; y < F.L[1]; ++y)
+          for (int x = 0; x < F.L[0]; ++x)
+            nv[(x / 2) + (size_t)C.L[0] * ((y / 2) + (size_t)C.L[1] * (z / 2))] +=
+                0.125f * cur[d][x + (size_t)F.L[0] * (y + (size_t)F.L[1] * z)];
+      P.svox.insert(P.svox.end(), nv.begin(), nv.end());
+      P.nodes += (int64_t)C.n[0] * C.n[1] * C.n[2];
+      P.doms[(size_t)l * ndom + d] = C;
+      // activity and tiles
+      const int nx = C.n[0], ny = C.n[1], nz = C.n[2];
+      std::vector<uint8_t> act((size_t)nx * ny * nz, 0);
+      for (int z = 0; z < C.L[2]; ++z)
+        for (int y = 0; y < C.L[1]; ++y)
+          for (int x = 0; x < C.L[0]; ++x) {
+            if (nv[x + (size_t)C.L[0] * (y + (size_t)C.L[1] * z)] == 0.f) continue;
+            for (int c = 0; c < 2; ++c)
+              for (int b = 0; b < 2; ++b)
+                for (int a = 0; a < 2; ++a) act[(x + a) + (size_t)nx * ((y + b) + (size_t)ny * (z + c))] = 1;
+          }
+      auto any = [&](int x0, int y0, int z0, int lo, int hx, int hy, int hz) {
+        for (int z = std::max(z0, lo); z < std::min(z0 + kTileZ, hz + 1); ++z)
+          for (int y = std::max(y0, lo); y < std::min(y0 + kTileY, hy + 1); ++y)
+            for (int x = std::max(x0, lo); x < std::min(x0 + kTileX, hx + 1); ++x)
+              if (act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
+        return false;
+      };
+      for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
+        for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
+          for (int x0 = 1; x0 <= nx - 2; x0 += kTileX)
+            if (any(x0, y0, z0, 1, nx - 2, ny - 2, nz - 2)) {
+              const Tile t{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0};
+              t_in.push_back(t);
+              if (nlev[d] > l + 1) t_sm.push_back(t);
+            }
+      for (int z0 = 0; z0 <= nz - 1; z0 += kTileZ)
+        for (int y0 = 0; y0 <= ny - 1; y0 += kTileY)
+          for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
+            if (any(x0, y0, z0, 0, nx - 1, ny - 1, nz - 1)) t_all.push_back(Tile{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+      cur[d].swap(nv);
+    }
+    P.sm_off[l] = (int64_t)P.tiles.size(); P.sm_n[l] = (int64_t)t_sm.size();
+    P.tiles.insert(P.tiles.end(), t_sm.begin(), t_sm.end());
+    P.in_off[l] = (int64_t)P.tiles.size(); P.in_n[l] = (int64_t)t_in.size();
+    P.tiles.insert(P.tiles.end(), t_in.begin(), t_in.end());
+    P.all_off[l] = (int64_t)P.tiles.size(); P.all_n[l] = (int64_t)t_all.size();
+    P.tiles.insert(P.tiles.end(), t_all.begin(), t_all.end());
+  }
+  // coarsest levels: domain lists and dense inverses
+  for (int l = 0; l < nl; ++l) {
+    P.list_off[l] = (int64_t)P.lists.size();
+    for (int d = 0; d < ndom; ++d)
+      if (nlev[d] - 1 == l) {
+        P.lists.push_back(d);
+        const DomDev& C = P.doms[(size_t)l * ndom + d];
+        coarse_inverse(C, cur[d].data(), kh, &P.minv[(size_t)d * kMgDenseN * kMgDenseN]);
+      }
+    P.list_n[l] = (int64_t)P.lists.size() - P.list_off[l];
+  }
+}
+
+// One V-cycle z_0 = B r_0 for every active domain; on level 0 accumulates z.z and z.r.
+struct MgDev {
+  const MgPlan* P;
+  int ndom;
+  const Tile* tiles;
+  const DomDev* doms0;   // fine level
+  const DomDev* doms;    // nlev * ndom
+  const float *svox0, *svox, *dinv0, *dinv, *minv;
+  const uint8_t *flags0, *flags;
+  const int* lists;
+  float *b, *t, *z;      // levels >= 1
+  float *t0, *z0;        // fine level
+};
+
+void mg_vcycle(const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act, cudaStream_t s,
+               int64_t& launches) {
+  const MgPlan& P = *M.P;
+  const DomDev* dl = l == 0 ? M.doms0 : M.doms + (size_t)l * M.ndom;
+  const float* sv = l == 0 ? M.svox0 : M.svox;
+  const float* di = l == 0 ? M.dinv0 : M.dinv;
+  const uint8_t* fl = l == 0 ? M.flags0 : M.flags;
+  const float* b = l == 0 ? r0 : M.b;
+  float* t = l == 0 ? M.t0 : M.t;
+  float* z = l == 0 ? M.z0 : M.z;
+  if (P.list_n[l] > 0) {
+    if (l == 0)
+      k_mg_coarse<true><<<(unsigned)P.list_n[l], 256, 0, s>>>(M.lists + P.list_off[l], dl, M.minv, b, z, zz, zr, act);
+    else
+      k_mg_coarse<false><<<(unsigned)P.list_n[l], 256, 0, s>>>(M.lists + P.list_off[l], dl, M.minv, b, z, nullptr,
+                                                               nullptr, act);
+    ++launches;
+  }
+  const int64_t nsm = P.sm_n[l];
+  if (nsm == 0 || l + 1 >= P.nlev) return;
+  const Tile* tsm = M.tiles + P.sm_off[l];
+  const unsigned g = (unsigned)(3 * nsm);
+  k_mg_matvec<kMgPre, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, di, b, nullptr, z, P.omega, nullptr, nullptr, act);
+  const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
+  if (P.in_n[l + 1] > 0)
+    k_mg_restrict<<<(unsigned)(3 * P.in_n[l + 1]), kThreads, 0, s>>>(M.tiles + P.in_off[l + 1], dc, M.flags, dl, z,
+                                                                    M.b, act);
+  launches += 2;
+  mg_vcycle(M, l + 1, r0, zz, zr, act, s, launches);
+  k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, di, b, dc, M.z, P.omega, t, act);
+  if (l == 0)
+    k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, di, b, t, z, P.omega, zz, zr, act);
+  else
+    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, di, b, t, z, P.omega, nullptr, nullptr, act);
+  launches += 2;
+}
+
 template <typename T, bool BLOCK, int NEN>
 int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* w, const T* dinv,
            double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
@@ -939,6 +1210,75 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
   return DTC_OK;
 }
 
+
+// FP32 CG preconditioned by one multigrid V-cycle per iteration (same column state machine
+// and stopping rule as run_cg, with z = B r in place of the Jacobi z).
+int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, float* x, float* r, float* p, float* w,
+              double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
+  cudaStream_t s = I.stream;
+  const Tile* ti = W.ti;
+  const int64_t nti = W.nti;
+  const DomDev* dd = B<DomDev>(I, bDoms);
+  const uint8_t* fl = B<uint8_t>(I, bFlags);
+  ColState* st = B<ColState>(I, bSt);
+  double* pw = B<double>(I, bPw);
+  double* zz = B<double>(I, bZz);
+  double* zr = B<double>(I, bZr);
+  int* act = B<int>(I, bDomAct);
+  int* cnt = B<int>(I, bCount);
+  const dim3 grid((unsigned)(3 * nti));
+  DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
+  DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
+  DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
+  {
+    const int q = I.begin(0);
+    mg_vcycle(M, 0, r, zz, zr, nullptr, s, launches);
+    I.end(kcMg32, q, 0, 0);
+  }
+  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs);
+  launches += 1;
+  if (int e = launch_check(msg)) return e;
+  const int chunk = 16;
+  int h_count = 1;
+  for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
+    const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(float) : 0;
+    const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(float) : 0;
+    const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
+    for (int k = 0; k < chunk; ++k) {
+      if (nti > 0) {
+        int q = I.begin(0);
+        k_direction_z<<<grid, kThreads, 0, s>>>(ti, dd, fl, M.z0, p, st, act);
+        I.end(kcDirection32, q, 3 * vb, 0);
+        q = I.begin(0);
+        k_matvec<float, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+        I.end(kcMatvec32, q, mb, mf);
+        q = I.begin(0);
+        k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, act);
+        I.end(kcUpdate32, q, 6 * vb, 0);
+        q = I.begin(0);
+        mg_vcycle(M, 0, r, zz, zr, act, s, launches);
+        I.end(kcMg32, q, 0, 0);
+        launches += 3;
+      }
+      const int q = I.begin(0);
+      k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+      I.end(kcColstate, q, 0, 0);
+      launches += 1;
+    }
+    k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
+    launches += 1;
+    if (int e = launch_check(msg)) return e;
+    DTC_CUDA(cudaMemcpyAsync(&h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (I.profile) {
+      I.h_active.resize(ndom);
+      DTC_CUDA(cudaMemcpyAsync(I.h_active.data(), act, sizeof(int) * ndom, cudaMemcpyDeviceToHost, s));
+    }
+    DTC_CUDA(cudaStreamSynchronize(s));
+    I.flush();
+  }
+  I.h_active.clear();
+  return DTC_OK;
+}
 }  // namespace
 
 template <int NEN>
@@ -949,7 +1289,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   stats_ = SolverStats();
   static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
                                              "direction_f32", "direction_f64", "colstate", "reaction_f64",
-                                             "project_f64"};
+                                             "project_f64", "mg_f32"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
@@ -1159,6 +1499,72 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemsetAsync(I.bufs[bR32], 0, vbytes32, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
+    // multigrid hierarchy (HEX08): built on the host from the voxel factors, set up on the device
+    const bool use_mg = NEN == 8 && opt.inner_precond == 2 && nti > 0;
+    MgPlan mgp;
+    MgDev mgd{};
+    if (use_mg) {
+      build_mg(mgp, doms, svox, tiles_i, nu);
+      const int64_t cn = std::max<int64_t>(mgp.nodes, 1);
+      if ((e = ensure(I, bZ32, vbytes32, msg)) || (e = ensure(I, bT32, vbytes32, msg)) ||
+          (e = ensure(I, bMgDoms, sizeof(DomDev) * mgp.doms.size(), msg)) ||
+          (e = ensure(I, bMgTiles, sizeof(Tile) * std::max<size_t>(mgp.tiles.size(), 1), msg)) ||
+          (e = ensure(I, bMgSvox, sizeof(float) * std::max<size_t>(mgp.svox.size(), 1), msg)) ||
+          (e = ensure(I, bMgFlags, cn, msg)) || (e = ensure(I, bMgDinv64, sizeof(double) * 3 * cn, msg)) ||
+          (e = ensure(I, bMgDinv32, sizeof(float) * 3 * cn, msg)) ||
+          (e = ensure(I, bMgBinv32, sizeof(float) * 6 * cn, msg)) ||
+          (e = ensure(I, bMgB, sizeof(float) * 72 * cn, msg)) || (e = ensure(I, bMgT, sizeof(float) * 72 * cn, msg)) ||
+          (e = ensure(I, bMgZ, sizeof(float) * 72 * cn, msg)) ||
+          (e = ensure(I, bMgMinv, sizeof(float) * mgp.minv.size(), msg)) ||
+          (e = ensure(I, bMgList, sizeof(int) * std::max<size_t>(mgp.lists.size(), 1), msg)))
+        return e;
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgDoms], mgp.doms.data(), sizeof(DomDev) * mgp.doms.size(),
+                               cudaMemcpyHostToDevice, s));
+      if (!mgp.tiles.empty())
+        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgTiles], mgp.tiles.data(), sizeof(Tile) * mgp.tiles.size(),
+                                 cudaMemcpyHostToDevice, s));
+      if (!mgp.svox.empty())
+        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgSvox], mgp.svox.data(), sizeof(float) * mgp.svox.size(),
+                                 cudaMemcpyHostToDevice, s));
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgMinv], mgp.minv.data(), sizeof(float) * mgp.minv.size(),
+                               cudaMemcpyHostToDevice, s));
+      if (!mgp.lists.empty())
+        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgList], mgp.lists.data(), sizeof(int) * mgp.lists.size(),
+                                 cudaMemcpyHostToDevice, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgFlags], 0, cn, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgDinv32], 0, sizeof(float) * 3 * cn, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgB], 0, sizeof(float) * 72 * cn, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgT], 0, sizeof(float) * 72 * cn, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgZ], 0, sizeof(float) * 72 * cn, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));
+      for (int l = 1; l < mgp.nlev; ++l)
+        if (mgp.all_n[l] > 0) {
+          k_node_setup<8><<<(unsigned)mgp.all_n[l], kThreads, 0, s>>>(
+              B<Tile>(I, bMgTiles) + mgp.all_off[l], B<DomDev>(I, bMgDoms) + (size_t)l * ndom, B<float>(I, bMgSvox),
+              B<uint8_t>(I, bMgFlags), B<double>(I, bMgDinv64), B<float>(I, bMgDinv32), B<float>(I, bMgBinv32));
+          ++L;
+        }
+      if ((e = launch_check(msg))) return e;
+      mgd.P = &mgp;
+      mgd.ndom = ndom;
+      mgd.tiles = B<Tile>(I, bMgTiles);
+      mgd.doms0 = dd;
+      mgd.doms = B<DomDev>(I, bMgDoms);
+      mgd.svox0 = B<float>(I, bSvox);
+      mgd.svox = B<float>(I, bMgSvox);
+      mgd.dinv0 = B<float>(I, bDinv32);
+      mgd.dinv = B<float>(I, bMgDinv32);
+      mgd.minv = B<float>(I, bMgMinv);
+      mgd.flags0 = fl;
+      mgd.flags = B<uint8_t>(I, bMgFlags);
+      mgd.lists = B<int>(I, bMgList);
+      mgd.b = B<float>(I, bMgB);
+      mgd.t = B<float>(I, bMgT);
+      mgd.z = B<float>(I, bMgZ);
+      mgd.t0 = B<float>(I, bT32);
+      mgd.z0 = B<float>(I, bZ32);
+    }
     // inner FP32 solves aim straight at the outer target when FP32 can reach it
     const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);
     const int max_refine = opt.max_refine > 0 ? opt.max_refine : 12;
@@ -1181,7 +1587,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       if (h_count == 0 || step == max_refine || inner_budget <= 0) break;
       if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
       DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
-      if (opt.inner_precond == 1)
+      if (use_mg)
+        e = run_cg_mg(I, ndom, W, mgd, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
+                      inner, B<double>(I, bTarget), inner_budget, L, msg);
+      else if (opt.inner_precond >= 1)
         e = run_cg<float, true, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
                                 B<float>(I, bW32), B<float>(I, bBinv32), inner, B<double>(I, bTarget), inner_budget,
                                 L, msg);

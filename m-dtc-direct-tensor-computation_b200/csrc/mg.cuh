@@ -1,0 +1,345 @@
+// mg.cuh -- geometric multigrid V-cycle that preconditions the FP32 inner solve (HEX08).
+//
+// Not a step of the reference (its KSP uses PCJACOBI, f-src/mod_dtc_main_subroutines.f90:
+// 995-1078); it only changes how fast the inner FP32 solve of the iterative refinement
+// reaches its tolerance, never the FP64 outer residual or the tensor it converges to.
+//
+// Hierarchy: level l+1 halves the voxel grid of level l (ceil(L/2) voxels per edge); a coarse
+// voxel carries the mean of the moduli of its <= 8 children (void and missing children count
+// as 0) and twice the edge, so its element matrix is 2 * mean(E) * a * Khat.  For moduli that
+// are constant inside each coarse voxel this equals the Galerkin product P^T K P of the
+// trilinear prolongation P, because the coarse trilinear space is nested in the fine one.
+// Every level keeps all nodes on its domain box fixed (zero correction).  The coarsest level
+// (at most 4 voxels per edge, at most 27 interior nodes) is solved with a dense inverse.
+//
+// Smoother: one damped-Jacobi sweep x = omega D^-1 r (Chebyshev of degree 1 on the interval
+// [lambda*/30, 1.1 lambda*], lambda* = the largest eigenvalue of De^-1/2 Khat De^-1/2 of the
+// unit voxel, an upper bound of lambda_max(D^-1 K) for any assembly of such voxels), the same
+// before and after the coarse correction, so the V-cycle is a fixed SPD operator.
+//
+// One V-cycle per CG iteration, per level l that is not a domain's coarsest:
+//   r_l = b_l - K_l (omega D_l^-1 b_l)           k_mg_matvec<kMgPre>
+//   b_{l+1} = P^T r_l                             k_mg_restrict
+//   (level l+1: recurse, or z_{l+1} = K^-1 b)     ...  / k_mg_coarse
+//   t_l = omega D_l^-1 b_l + P z_{l+1}            k_mg_prolong
+//   z_l = t_l + omega D_l^-1 (b_l - K_l t_l)      k_mg_matvec<kMgPost> (+ z.z, z.b on level 0)
+#pragma once
+
+namespace dtc {
+
+constexpr int kMgMaxCoarse = 4;                  // voxels per edge on the coarsest level
+constexpr int kMgDenseN = 81;                    // 3 * 3^3 interior DOFs at most
+enum { kMgPre = 0, kMgPost = 1 };
+
+// 3-plane window of omega * D^-1 b (pre-smoothing: the smoothed iterate is never stored)
+__device__ __forceinline__ void load_plane_jac(float (&pl)[3][3][3], const float* __restrict__ b,
+                                               const float* __restrict__ dinv, float omega, const DomDev& D, int x,
+                                               int y, int z, int lc) {
+#pragma unroll
+  for (int py = 0; py < 3; ++py)
+#pragma unroll
+    for (int pz = 0; pz < 3; ++pz) {
+      const int64_t n = node_index(D, x, y + py - 1, z + pz - 1);
+      const int64_t base = vec_index(n, 0, lc);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pl[py][pz][c] = omega * __ldg(dinv + n * 3 + c) * __ldg(b + base + c * kNLC);
+    }
+}
+
+__device__ __forceinline__ void load_plane_f(float (&pl)[3][3][3], const float* __restrict__ u, const DomDev& D, int x,
+                                             int y, int z, int lc) {
+#pragma unroll
+  for (int py = 0; py < 3; ++py)
+#pragma unroll
+    for (int pz = 0; pz < 3; ++pz) {
+      const int64_t base = vec_index(node_index(D, x, y + py - 1, z + pz - 1), 0, lc);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pl[py][pz][c] = __ldg(u + base + c * kNLC);
+    }
+}
+
+__device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __restrict__ svox, const DomDev& D, int vx,
+                                              int y, int z) {
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      sp[b][c] = __ldg(svox + D.vox_off + vx + (int64_t)D.L[0] * ((y - 1 + b) + (int64_t)D.L[1] * (z - 1 + c)));
+}
+
+// Smoother + residual on one level's interior tiles (same sweep as k_matvec).
+//   kMgPre : y = b - K (omega D^-1 b)
+//   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
+template <int MODE, bool DOT>
+__global__ void __launch_bounds__(kThreads) k_mg_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                        const float* __restrict__ svox,
+                                                        const float* __restrict__ dinv, const float* __restrict__ b,
+                                                        const float* __restrict__ u, float* __restrict__ y, float omega,
+                                                        double* __restrict__ acc_zz, double* __restrict__ acc_zr,
+                                                        const int* __restrict__ dom_active) {
+  __shared__ double red[32];
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  double szz = 0.0, szr = 0.0;
+  if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
+    float w[3][3][3][3];
+    float sv[2][2][2];
+    if (MODE == kMgPre) {
+      load_plane_jac(w[0], b, dinv, omega, D, t.x0 - 1, yy, zz, lc);
+      load_plane_jac(w[1], b, dinv, omega, D, t.x0, yy, zz, lc);
+    } else {
+      load_plane_f(w[0], u, D, t.x0 - 1, yy, zz, lc);
+      load_plane_f(w[1], u, D, t.x0, yy, zz, lc);
+    }
+    load_voxels_f(sv[0], svox, D, t.x0 - 1, yy, zz);
+#pragma unroll 1
+    for (int i = 0; i < kTileX; ++i) {
+      const int x = t.x0 + i;
+      if (x > D.n[0] - 2) break;
+      if (MODE == kMgPre) load_plane_jac(w[2], b, dinv, omega, D, x + 1, yy, zz, lc);
+      else load_plane_f(w[2], u, D, x + 1, yy, zz, lc);
+      load_voxels_f(sv[1], svox, D, x, yy, zz);
+      const bool any = (sv[0][0][0] != 0.f) | (sv[0][0][1] != 0.f) | (sv[0][1][0] != 0.f) | (sv[0][1][1] != 0.f) |
+                       (sv[1][0][0] != 0.f) | (sv[1][0][1] != 0.f) | (sv[1][1][0] != 0.f) | (sv[1][1][1] != 0.f);
+      if (any) {
+        float a3[3] = {0.f, 0.f, 0.f};
+        apply_node<float>(w, sv, a3);
+        const int64_t n = node_index(D, x, yy, zz);
+        const int64_t k0 = vec_index(n, 0, lc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float bc = b[k0 + c * kNLC];
+          const float res = bc - (float)(D.scale * (double)a3[c]);
+          float v;
+          if (MODE == kMgPre) v = res;
+          else v = w[1][1][1][c] + omega * dinv[n * 3 + c] * res;
+          y[k0 + c * kNLC] = v;
+          if (DOT) {
+            szz += (double)v * (double)v;
+            szr += (double)v * (double)bc;
+          }
+        }
+      }
+#pragma unroll
+      for (int py = 0; py < 3; ++py)
+#pragma unroll
+        for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            w[0][py][pz][c] = w[1][py][pz][c];
+            w[1][py][pz][c] = w[2][py][pz][c];
+          }
+#pragma unroll
+      for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+        for (int c2 = 0; c2 < 2; ++c2) sv[0][b2][c2] = sv[1][b2][c2];
+    }
+  }
+  if (DOT) {
+    const int64_t col = (int64_t)t.dom * kNLC + lc;
+    const double s1 = block_sum_lc<double>(szz, red);
+    __syncthreads();
+    const double s2 = block_sum_lc<double>(szr, red);
+    if (threadIdx.x < 8) {
+      atomicAdd(acc_zz + col, s1);
+      atomicAdd(acc_zr + col, s2);
+    }
+  }
+}
+
+// b_c = P^T r_f on the active interior nodes of the coarse level (full weighting:
+// weight 1 at the coincident fine node, 1/2 per axis offset by one).
+__global__ void __launch_bounds__(kThreads) k_mg_restrict(const Tile* __restrict__ tiles,
+                                                          const DomDev* __restrict__ doms_c,
+                                                          const uint8_t* __restrict__ flags_c,
+                                                          const DomDev* __restrict__ doms_f,
+                                                          const float* __restrict__ r_f, float* __restrict__ b_c,
+                                                          const int* __restrict__ dom_active) {
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev C = doms_c[t.dom];
+  const DomDev F = doms_f[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  if (yy < 1 || yy > C.n[1] - 2 || zz < 1 || zz > C.n[2] - 2) return;
+  for (int i = 0; i < kTileX; ++i) {
+    const int x = t.x0 + i;
+    if (x > C.n[0] - 2) break;
+    const int64_t nc = node_index(C, x, yy, zz);
+    if (!(flags_c[nc] & kNodeActive)) continue;
+    float s[3] = {0.f, 0.f, 0.f};
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int fz = 2 * zz + dz;
+      if (fz > F.n[2] - 1) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int fy = 2 * yy + dy;
+        if (fy > F.n[1] - 1) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int fx = 2 * x + dx;
+          if (fx > F.n[0] - 1) continue;
+          const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+          const int64_t k = vec_index(node_index(F, fx, fy, fz), 0, lc);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s[c] = fmaf(wgt, __ldg(r_f + k + c * kNLC), s[c]);
+        }
+      }
+    }
+    const int64_t k0 = vec_index(nc, 0, lc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b_c[k0 + c * kNLC] = s[c];
+  }
+}
+
+// t_f = omega D^-1 b_f + P z_c on the active interior nodes of the fine level (trilinear).
+__global__ void __launch_bounds__(kThreads) k_mg_prolong(const Tile* __restrict__ tiles,
+                                                         const DomDev* __restrict__ doms_f,
+                                                         const uint8_t* __restrict__ flags_f,
+                                                         const float* __restrict__ dinv_f,
+                                                         const float* __restrict__ b_f, const DomDev* __restrict__ doms_c,
+                                                         const float* __restrict__ z_c, float omega,
+                                                         float* __restrict__ t_f, const int* __restrict__ dom_active) {
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev F = doms_f[t.dom];
+  const DomDev C = doms_c[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  if (yy < 1 || yy > F.n[1] - 2 || zz < 1 || zz > F.n[2] - 2) return;
+  const int cy0 = yy >> 1, cy1 = (yy + 1) >> 1, cz0 = zz >> 1, cz1 = (zz + 1) >> 1;
+  for (int i = 0; i < kTileX; ++i) {
+    const int x = t.x0 + i;
+    if (x > F.n[0] - 2) break;
+    const int64_t nf = node_index(F, x, yy, zz);
+    if (!(flags_f[nf] & kNodeActive)) continue;
+    const int cx0 = x >> 1, cx1 = (x + 1) >> 1;
+    float s[3] = {0.f, 0.f, 0.f};
+    // odd coordinates average the two coarse neighbours, even ones take the coincident node
+    // (cx0 == cx1 then, and each of the duplicate corners carries half of it)
+    for (int kz = 0; kz < 2; ++kz)
+      for (int ky = 0; ky < 2; ++ky)
+        for (int kx = 0; kx < 2; ++kx) {
+          const int64_t k = vec_index(node_index(C, kx ? cx1 : cx0, ky ? cy1 : cy0, kz ? cz1 : cz0), 0, lc);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s[c] = fmaf(0.125f, __ldg(z_c + k + c * kNLC), s[c]);
+        }
+    const int64_t k0 = vec_index(nf, 0, lc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t_f[k0 + c * kNLC] = fmaf(omega * dinv_f[nf * 3 + c], b_f[k0 + c * kNLC], s[c]);
+  }
+}
+
+// Coarsest level: z = Minv b over the <= 27 interior nodes of each listed domain (one CTA per
+// domain, Minv 81 x 81 row-major on the DOFs 3 * ((x-1) + 3 (y-1) + 9 (z-1)) + c).
+// DOT (the coarsest level is the finest one): zz += z.z, zr += z.b.
+template <bool DOT>
+__global__ void __launch_bounds__(256) k_mg_coarse(const int* __restrict__ list, const DomDev* __restrict__ doms,
+                                                   const float* __restrict__ minv, const float* __restrict__ b,
+                                                   float* __restrict__ z, double* __restrict__ acc_zz,
+                                                   double* __restrict__ acc_zr, const int* __restrict__ dom_active) {
+  __shared__ float sb[kMgDenseN * kNLC];
+  __shared__ double red[2][kNLC];
+  const int d = list[blockIdx.x];
+  if (dom_active && !dom_active[d]) return;
+  const DomDev D = doms[d];
+  const int ix = D.n[0] - 2, iy = D.n[1] - 2, iz = D.n[2] - 2;   // interior nodes per axis (<= 3)
+  for (int i = threadIdx.x; i < kMgDenseN * kNLC; i += blockDim.x) {
+    const int lc = i % kNLC, dof = i / kNLC, node = dof / 3, c = dof % 3;
+    const int x = node % 3, y = (node / 3) % 3, zc = node / 9;
+    float v = 0.f;
+    if (x < ix && y < iy && zc < iz) v = b[vec_index(node_index(D, x + 1, y + 1, zc + 1), c, lc)];
+    sb[i] = v;
+  }
+  if (threadIdx.x < 2 * kNLC) red[threadIdx.x / kNLC][threadIdx.x % kNLC] = 0.0;
+  __syncthreads();
+  const float* M = minv + (int64_t)d * kMgDenseN * kMgDenseN;
+  for (int i = threadIdx.x; i < kMgDenseN * kNLC; i += blockDim.x) {
+    const int lc = i % kNLC, dof = i / kNLC, node = dof / 3, c = dof % 3;
+    const int x = node % 3, y = (node / 3) % 3, zc = node / 9;
+    if (x >= ix || y >= iy || zc >= iz) continue;
+    float s = 0.f;
+    for (int k = 0; k < kMgDenseN; ++k) s = fmaf(__ldg(M + dof * kMgDenseN + k), sb[k * kNLC + lc], s);
+    z[vec_index(node_index(D, x + 1, y + 1, zc + 1), c, lc)] = s;
+    if (DOT) {
+      atomicAdd(&red[0][lc], (double)s * (double)s);
+      atomicAdd(&red[1][lc], (double)s * (double)sb[dof * kNLC + lc]);
+    }
+  }
+  if (DOT) {
+    __syncthreads();
+    if (threadIdx.x < kNLC) {
+      atomicAdd(acc_zz + (int64_t)d * kNLC + threadIdx.x, red[0][threadIdx.x]);
+      atomicAdd(acc_zr + (int64_t)d * kNLC + threadIdx.x, red[1][threadIdx.x]);
+    }
+  }
+}
+
+// CG vectors with the preconditioned residual z given: p = z + bfac p
+__global__ void __launch_bounds__(kThreads) k_direction_z(const Tile* __restrict__ tiles,
+                                                          const DomDev* __restrict__ doms,
+                                                          const uint8_t* __restrict__ flags,
+                                                          const float* __restrict__ z, float* __restrict__ p,
+                                                          const ColState* __restrict__ st,
+                                                          const int* __restrict__ dom_active) {
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  const int64_t col = (int64_t)t.dom * kNLC + lc;
+  if (yy < 1 || yy > D.n[1] - 2 || zz < 1 || zz > D.n[2] - 2 || !st[col].active) return;
+  const float bf = (float)st[col].bfac;
+  for (int i = 0; i < kTileX; ++i) {
+    const int x = t.x0 + i;
+    if (x > D.n[0] - 2) break;
+    const int64_t n = node_index(D, x, yy, zz);
+    if (!(flags[n] & kNodeActive)) continue;
+    const int64_t k0 = vec_index(n, 0, lc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p[k0 + c * kNLC] = z[k0 + c * kNLC] + bf * p[k0 + c * kNLC];
+  }
+}
+
+// x += alpha p ; r -= alpha w  (alpha = beta / p.w unless the column stopped or p.w flags an
+// indefinite operator, exactly as in k_update)
+__global__ void __launch_bounds__(kThreads) k_update_xr(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                        const uint8_t* __restrict__ flags, float* __restrict__ x,
+                                                        float* __restrict__ r, const float* __restrict__ p,
+                                                        const float* __restrict__ w, const ColState* __restrict__ st,
+                                                        const double* __restrict__ acc_pw,
+                                                        const int* __restrict__ dom_active) {
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  const int64_t col = (int64_t)t.dom * kNLC + lc;
+  if (yy < 1 || yy > D.n[1] - 2 || zz < 1 || zz > D.n[2] - 2) return;
+  const ColState s = st[col];
+  const double pw = acc_pw[col];
+  const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0) || pw == 0.0);
+  if (!s.active || pw == 0.0 || flip) return;
+  const float a = (float)(s.beta / pw);
+  for (int i = 0; i < kTileX; ++i) {
+    const int xx = t.x0 + i;
+    if (xx > D.n[0] - 2) break;
+    const int64_t n = node_index(D, xx, yy, zz);
+    if (!(flags[n] & kNodeActive)) continue;
+    const int64_t k0 = vec_index(n, 0, lc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t k = k0 + c * kNLC;
+      x[k] = x[k] + a * p[k];
+      r[k] = r[k] - a * w[k];
+    }
+  }
+}
+
+}  // namespace dtc
