@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--check", type=int, default=16, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
     p.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    p.add_argument("--profile-step", action="store_true",
+                   help="one warm-up and one timed-free mixed solve only (for ncu captures)")
     return p.parse_args()
 
 
@@ -191,6 +193,21 @@ def main():
                        domain_number=i) for i, g in enumerate(grays)]
     h2d = sum(d.phi.nbytes + d.E_voxel.nbytes for d in doms)
     d2h = args.ndom * 8 * (576 + 36 + 48)
+
+    if args.profile_step:
+        # one warm-up solve, then one solve of the mixed arm at --rtol (for ncu launch lists:
+        # skip the first launches_per_solve launches)
+        rt = args.rtol if args.rtol > 0 else 3e-5
+        with dtc.Solver(precision="mixed", rtol=rt, max_it=args.max_it, rotation_search=False, device=local,
+                        estimator=args.estimator, inner_precond=args.precond) as sv:
+            sv.solve(doms)
+            n0 = sv.stats()["kernel_launches"]
+            sv.solve(doms)
+            torch.cuda.synchronize()
+            print(json.dumps({"profile_step": True, "ndom": args.ndom, "L": args.L, "rtol": rt,
+                              "inner_precond": args.precond, "launches_per_solve": n0,
+                              "launches_second": sv.stats()["kernel_launches"]}))
+        return
 
     # accuracy gate: both arms are timed at the loosest rtol whose tensors stay within
     # TARGET/2 of an FP64 rtol-1e-10 solve on a sample spread over the batch

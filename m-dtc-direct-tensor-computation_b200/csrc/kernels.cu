@@ -898,25 +898,50 @@ struct MgPlan {
   int64_t nodes = 0;                                // nodes of levels >= 1
 };
 
-// lambda_max of De^-1/2 Khat De^-1/2 (unit voxel, scalar diagonal De): bounds
-// lambda_max(D^-1 K) of every assembly of scaled voxels, D the assembled diagonal.
-double jacobi_bound(const double* kh) {
+// Largest eigenvalue of Khat v = lambda De v, De the node-block (3x3) diagonal of the unit
+// voxel matrix: bounds lambda_max(D^-1 K) of every assembly of scaled voxels, D its node-block
+// diagonal (x^T K x = sum_v x_v^T K_v x_v <= lambda sum_v x_v^T De_v x_v = lambda x^T D x).
+double block_jacobi_bound(const double* kh) {
+  double inv[8][9];
+  for (int a = 0; a < 8; ++a) {
+    double m[9];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) m[3 * i + j] = kh[(3 * a + i) + 24 * (3 * a + j)];
+    const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[2] * m[7] - m[1] * m[8], c02 = m[1] * m[5] - m[2] * m[4];
+    const double det = m[0] * c00 + m[3] * c01 + m[6] * c02;
+    inv[a][0] = c00 / det; inv[a][1] = c01 / det; inv[a][2] = c02 / det;
+    inv[a][3] = (m[5] * m[6] - m[3] * m[8]) / det; inv[a][4] = (m[0] * m[8] - m[2] * m[6]) / det;
+    inv[a][5] = (m[2] * m[3] - m[0] * m[5]) / det;
+    inv[a][6] = (m[3] * m[7] - m[4] * m[6]) / det; inv[a][7] = (m[1] * m[6] - m[0] * m[7]) / det;
+    inv[a][8] = (m[0] * m[4] - m[1] * m[3]) / det;
+  }
   double v[24], w[24], lam = 0;
   for (int i = 0; i < 24; ++i) v[i] = 1.0 + 0.01 * i;
-  for (int it = 0; it < 2000; ++it) {
-    double nrm = 0;
+  for (int it = 0; it < 3000; ++it) {
+    double kv[24];
     for (int i = 0; i < 24; ++i) {
       double s = 0;
-      for (int j = 0; j < 24; ++j) s += kh[i + 24 * j] / std::sqrt(kh[i * 25] * kh[j * 25]) * v[j];
-      w[i] = s;
-      nrm += s * s;
+      for (int j = 0; j < 24; ++j) s += kh[i + 24 * j] * v[j];
+      kv[i] = s;
     }
+    double vkv = 0, vdv = 0;
+    for (int a = 0; a < 8; ++a)
+      for (int i = 0; i < 3; ++i) {
+        double dv = 0;
+        for (int j = 0; j < 3; ++j) dv += kh[(3 * a + i) + 24 * (3 * a + j)] * v[3 * a + j];
+        vdv += v[3 * a + i] * dv;
+        vkv += v[3 * a + i] * kv[3 * a + i];
+      }
+    lam = vkv / vdv;
+    double nrm = 0;
+    for (int a = 0; a < 8; ++a)
+      for (int i = 0; i < 3; ++i) {
+        double s = 0;
+        for (int j = 0; j < 3; ++j) s += inv[a][3 * i + j] * kv[3 * a + j];
+        w[3 * a + i] = s;
+        nrm += s * s;
+      }
     nrm = std::sqrt(nrm);
-    double rq = 0;
-    for (int i = 0; i < 24; ++i) rq += v[i] * w[i];
-    double vn = 0;
-    for (int i = 0; i < 24; ++i) vn += v[i] * v[i];
-    lam = rq / vn;
     for (int i = 0; i < 24; ++i) v[i] = w[i] / nrm;
   }
   return lam;
@@ -995,7 +1020,7 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
   const int ndom = (int)doms0.size();
   double kh[576];
   voxel_stiffness(8, nu, kh);
-  const double lam = jacobi_bound(kh);
+  const double lam = block_jacobi_bound(kh);
   P.omega = (float)(1.0 / (0.5 * (1.1 + 1.0 / 30.0) * lam));
   std::vector<int> nlev(ndom, 1);
   int nl = 1;
@@ -1101,23 +1126,31 @@ struct MgDev {
   const Tile* tiles;
   const DomDev* doms0;   // fine level
   const DomDev* doms;    // nlev * ndom
-  const float *svox0, *svox, *dinv0, *dinv, *minv;
+  const float *svox0, *svox, *binv0, *binv, *minv;
   const uint8_t *flags0, *flags;
   const int* lists;
   float *b, *t, *z;      // levels >= 1
   float *t0, *z0;        // fine level
 };
 
-void mg_vcycle(const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act, cudaStream_t s,
+void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act,
                int64_t& launches) {
+  cudaStream_t s = I.stream;
   const MgPlan& P = *M.P;
   const DomDev* dl = l == 0 ? M.doms0 : M.doms + (size_t)l * M.ndom;
   const float* sv = l == 0 ? M.svox0 : M.svox;
-  const float* di = l == 0 ? M.dinv0 : M.dinv;
+  const float* bi = l == 0 ? M.binv0 : M.binv;
   const uint8_t* fl = l == 0 ? M.flags0 : M.flags;
   const float* b = l == 0 ? r0 : M.b;
   float* t = l == 0 ? M.t0 : M.t;
   float* z = l == 0 ? M.z0 : M.z;
+  // fine-level launches are profiled one by one with their algorithmic work; the coarser
+  // levels as one class
+  const bool fine = l == 0;
+  const double vb = I.profile && fine ? I.active_sum(I.dom_vec_bytes) * sizeof(float) : 0;
+  const double mb = I.profile && fine ? I.active_sum(I.dom_mv_bytes) * sizeof(float) : 0;
+  const double mf = I.profile && fine ? I.active_sum(I.dom_mv_flops) : 0;
+  const int q0 = fine ? -1 : I.begin(0);
   if (P.list_n[l] > 0) {
     if (l == 0)
       k_mg_coarse<true><<<(unsigned)P.list_n[l], 256, 0, s>>>(M.lists + P.list_off[l], dl, M.minv, b, z, zz, zr, act);
@@ -1127,21 +1160,37 @@ void mg_vcycle(const MgDev& M, int l, const float* r0, double* zz, double* zr, c
     ++launches;
   }
   const int64_t nsm = P.sm_n[l];
-  if (nsm == 0 || l + 1 >= P.nlev) return;
+  if (nsm == 0 || l + 1 >= P.nlev) {
+    if (!fine) I.end(kcMgCoarse, q0, 0, 0);
+    return;
+  }
   const Tile* tsm = M.tiles + P.sm_off[l];
   const unsigned g = (unsigned)(3 * nsm);
-  k_mg_matvec<kMgPre, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, di, b, nullptr, z, P.omega, nullptr, nullptr, act);
+  int q = fine ? I.begin(0) : -1;
+  k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, P.omega, t, act);
+  k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+  if (fine) I.end(kcMgPre, q, mb + 2 * vb + vb / 3, mf);
+  ++launches;
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
+  q = fine ? I.begin(0) : -1;
   if (P.in_n[l + 1] > 0)
     k_mg_restrict<<<(unsigned)(3 * P.in_n[l + 1]), kThreads, 0, s>>>(M.tiles + P.in_off[l + 1], dc, M.flags, dl, z,
                                                                     M.b, act);
+  if (fine) I.end(kcMgTransfer, q, vb * (1.0 + 1.0 / 8.0), 0);
   launches += 2;
-  mg_vcycle(M, l + 1, r0, zz, zr, act, s, launches);
-  k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, di, b, dc, M.z, P.omega, t, act);
+  if (!fine) I.end(kcMgCoarse, q0, 0, 0);
+  mg_vcycle(I, M, l + 1, r0, zz, zr, act, launches);
+  const int q1 = fine ? -1 : I.begin(0);
+  q = fine ? I.begin(0) : -1;
+  k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, dc, M.z, t, act);
+  if (fine) I.end(kcMgTransfer, q, vb * (2.0 + 1.0 / 8.0), 0);
+  q = fine ? I.begin(0) : -1;
   if (l == 0)
-    k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, di, b, t, z, P.omega, zz, zr, act);
+    k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, zz, zr, act);
   else
-    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, di, b, t, z, P.omega, nullptr, nullptr, act);
+    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+  if (fine) I.end(kcMgPost, q, mb + 2 * vb + vb / 3, mf);
+  if (!fine) I.end(kcMgCoarse, q1, 0, 0);
   launches += 2;
 }
 
@@ -1230,11 +1279,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
-  {
-    const int q = I.begin(0);
-    mg_vcycle(M, 0, r, zz, zr, nullptr, s, launches);
-    I.end(kcMg32, q, 0, 0);
-  }
+  mg_vcycle(I, M, 0, r, zz, zr, nullptr, launches);
   k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs);
   launches += 1;
   if (int e = launch_check(msg)) return e;
@@ -1255,9 +1300,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
         q = I.begin(0);
         k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, act);
         I.end(kcUpdate32, q, 6 * vb, 0);
-        q = I.begin(0);
-        mg_vcycle(M, 0, r, zz, zr, act, s, launches);
-        I.end(kcMg32, q, 0, 0);
+        mg_vcycle(I, M, 0, r, zz, zr, act, launches);
         launches += 3;
       }
       const int q = I.begin(0);
@@ -1289,7 +1332,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   stats_ = SolverStats();
   static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
                                              "direction_f32", "direction_f64", "colstate", "reaction_f64",
-                                             "project_f64", "mg_f32"};
+                                             "project_f64", "mg_presmooth_f32", "mg_postsmooth_f32",
+                                             "mg_transfer_f32", "mg_coarse_levels_f32"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
@@ -1532,7 +1576,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
         DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgList], mgp.lists.data(), sizeof(int) * mgp.lists.size(),
                                  cudaMemcpyHostToDevice, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bMgFlags], 0, cn, s));
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgDinv32], 0, sizeof(float) * 3 * cn, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgBinv32], 0, sizeof(float) * 6 * cn, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bMgB], 0, sizeof(float) * 72 * cn, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bMgT], 0, sizeof(float) * 72 * cn, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bMgZ], 0, sizeof(float) * 72 * cn, s));
@@ -1553,8 +1597,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.doms = B<DomDev>(I, bMgDoms);
       mgd.svox0 = B<float>(I, bSvox);
       mgd.svox = B<float>(I, bMgSvox);
-      mgd.dinv0 = B<float>(I, bDinv32);
-      mgd.dinv = B<float>(I, bMgDinv32);
+      mgd.binv0 = B<float>(I, bBinv32);
+      mgd.binv = B<float>(I, bMgBinv32);
       mgd.minv = B<float>(I, bMgMinv);
       mgd.flags0 = fl;
       mgd.flags = B<uint8_t>(I, bMgFlags);

@@ -12,16 +12,18 @@
 // Every level keeps all nodes on its domain box fixed (zero correction).  The coarsest level
 // (at most 4 voxels per edge, at most 27 interior nodes) is solved with a dense inverse.
 //
-// Smoother: one damped-Jacobi sweep x = omega D^-1 r (Chebyshev of degree 1 on the interval
-// [lambda*/30, 1.1 lambda*], lambda* = the largest eigenvalue of De^-1/2 Khat De^-1/2 of the
-// unit voxel, an upper bound of lambda_max(D^-1 K) for any assembly of such voxels), the same
-// before and after the coarse correction, so the V-cycle is a fixed SPD operator.
+// Smoother: one damped node-block-Jacobi sweep x = omega D^-1 r, D the 3x3 diagonal blocks
+// (Chebyshev of degree 1 on [lambda*/30, 1.1 lambda*]; lambda* = the largest eigenvalue of
+// Khat v = lambda De v for the unit voxel, De its node-block diagonal, bounds
+// lambda_max(D^-1 K) for any assembly of scaled voxels), the same before and after the coarse
+// correction, so the V-cycle is a fixed SPD operator.
 //
 // One V-cycle per CG iteration, per level l that is not a domain's coarsest:
-//   r_l = b_l - K_l (omega D_l^-1 b_l)           k_mg_matvec<kMgPre>
+//   t_l = omega D_l^-1 b_l                        k_mg_jacobi
+//   r_l = b_l - K_l t_l                           k_mg_matvec<kMgRes>
 //   b_{l+1} = P^T r_l                             k_mg_restrict
 //   (level l+1: recurse, or z_{l+1} = K^-1 b)     ...  / k_mg_coarse
-//   t_l = omega D_l^-1 b_l + P z_{l+1}            k_mg_prolong
+//   t_l += P z_{l+1}                              k_mg_prolong
 //   z_l = t_l + omega D_l^-1 (b_l - K_l t_l)      k_mg_matvec<kMgPost> (+ z.z, z.b on level 0)
 #pragma once
 
@@ -29,21 +31,17 @@ namespace dtc {
 
 constexpr int kMgMaxCoarse = 4;                  // voxels per edge on the coarsest level
 constexpr int kMgDenseN = 81;                    // 3 * 3^3 interior DOFs at most
-enum { kMgPre = 0, kMgPost = 1 };
+enum { kMgRes = 0, kMgPost = 1 };
 
-// 3-plane window of omega * D^-1 b (pre-smoothing: the smoothed iterate is never stored)
-__device__ __forceinline__ void load_plane_jac(float (&pl)[3][3][3], const float* __restrict__ b,
-                                               const float* __restrict__ dinv, float omega, const DomDev& D, int x,
-                                               int y, int z, int lc) {
-#pragma unroll
-  for (int py = 0; py < 3; ++py)
-#pragma unroll
-    for (int pz = 0; pz < 3; ++pz) {
-      const int64_t n = node_index(D, x, y + py - 1, z + pz - 1);
-      const int64_t base = vec_index(n, 0, lc);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) pl[py][pz][c] = omega * __ldg(dinv + n * 3 + c) * __ldg(b + base + c * kNLC);
-    }
+// z = omega * D^-1 r with D^-1 the symmetric 3x3 block inverse (00, 11, 22, 01, 02, 12)
+__device__ __forceinline__ void block_jacobi(const float* __restrict__ binv, int64_t n, float omega, const float (&r)[3],
+                                             float (&z)[3]) {
+  const float* b = binv + n * 6;
+  const float b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2), b3 = __ldg(b + 3), b4 = __ldg(b + 4),
+              b5 = __ldg(b + 5);
+  z[0] = omega * (b0 * r[0] + b3 * r[1] + b4 * r[2]);
+  z[1] = omega * (b3 * r[0] + b1 * r[1] + b5 * r[2]);
+  z[2] = omega * (b4 * r[0] + b5 * r[1] + b2 * r[2]);
 }
 
 __device__ __forceinline__ void load_plane_f(float (&pl)[3][3][3], const float* __restrict__ u, const DomDev& D, int x,
@@ -67,13 +65,13 @@ __device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __
       sp[b][c] = __ldg(svox + D.vox_off + vx + (int64_t)D.L[0] * ((y - 1 + b) + (int64_t)D.L[1] * (z - 1 + c)));
 }
 
-// Smoother + residual on one level's interior tiles (same sweep as k_matvec).
-//   kMgPre : y = b - K (omega D^-1 b)
+// Residual / smoother on one level's interior tiles (same sweep as k_matvec).
+//   kMgRes : y = b - K u
 //   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
 template <int MODE, bool DOT>
 __global__ void __launch_bounds__(kThreads) k_mg_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                         const float* __restrict__ svox,
-                                                        const float* __restrict__ dinv, const float* __restrict__ b,
+                                                        const float* __restrict__ binv, const float* __restrict__ b,
                                                         const float* __restrict__ u, float* __restrict__ y, float omega,
                                                         double* __restrict__ acc_zz, double* __restrict__ acc_zr,
                                                         const int* __restrict__ dom_active) {
@@ -88,20 +86,14 @@ __global__ void __launch_bounds__(kThreads) k_mg_matvec(const Tile* __restrict__
   if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
     float w[3][3][3][3];
     float sv[2][2][2];
-    if (MODE == kMgPre) {
-      load_plane_jac(w[0], b, dinv, omega, D, t.x0 - 1, yy, zz, lc);
-      load_plane_jac(w[1], b, dinv, omega, D, t.x0, yy, zz, lc);
-    } else {
-      load_plane_f(w[0], u, D, t.x0 - 1, yy, zz, lc);
-      load_plane_f(w[1], u, D, t.x0, yy, zz, lc);
-    }
+    load_plane_f(w[0], u, D, t.x0 - 1, yy, zz, lc);
+    load_plane_f(w[1], u, D, t.x0, yy, zz, lc);
     load_voxels_f(sv[0], svox, D, t.x0 - 1, yy, zz);
 #pragma unroll 1
     for (int i = 0; i < kTileX; ++i) {
       const int x = t.x0 + i;
       if (x > D.n[0] - 2) break;
-      if (MODE == kMgPre) load_plane_jac(w[2], b, dinv, omega, D, x + 1, yy, zz, lc);
-      else load_plane_f(w[2], u, D, x + 1, yy, zz, lc);
+      load_plane_f(w[2], u, D, x + 1, yy, zz, lc);
       load_voxels_f(sv[1], svox, D, x, yy, zz);
       const bool any = (sv[0][0][0] != 0.f) | (sv[0][0][1] != 0.f) | (sv[0][1][0] != 0.f) | (sv[0][1][1] != 0.f) |
                        (sv[1][0][0] != 0.f) | (sv[1][0][1] != 0.f) | (sv[1][1][0] != 0.f) | (sv[1][1][1] != 0.f);
@@ -110,17 +102,27 @@ __global__ void __launch_bounds__(kThreads) k_mg_matvec(const Tile* __restrict__
         apply_node<float>(w, sv, a3);
         const int64_t n = node_index(D, x, yy, zz);
         const int64_t k0 = vec_index(n, 0, lc);
+        float res[3], bc[3], v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const float bc = b[k0 + c * kNLC];
-          const float res = bc - (float)(D.scale * (double)a3[c]);
-          float v;
-          if (MODE == kMgPre) v = res;
-          else v = w[1][1][1][c] + omega * dinv[n * 3 + c] * res;
-          y[k0 + c * kNLC] = v;
+          bc[c] = b[k0 + c * kNLC];
+          res[c] = bc[c] - (float)(D.scale * (double)a3[c]);
+        }
+        if (MODE == kMgRes) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) v[c] = res[c];
+        } else {
+          float dz[3];
+          block_jacobi(binv, n, omega, res, dz);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) v[c] = w[1][1][1][c] + dz[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          y[k0 + c * kNLC] = v[c];
           if (DOT) {
-            szz += (double)v * (double)v;
-            szr += (double)v * (double)bc;
+            szz += (double)v[c] * (double)v[c];
+            szr += (double)v[c] * (double)bc[c];
           }
         }
       }
@@ -195,14 +197,13 @@ __global__ void __launch_bounds__(kThreads) k_mg_restrict(const Tile* __restrict
   }
 }
 
-// t_f = omega D^-1 b_f + P z_c on the active interior nodes of the fine level (trilinear).
+// t_f += P z_c on the active interior nodes of the fine level (trilinear).
 __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Tile* __restrict__ tiles,
                                                          const DomDev* __restrict__ doms_f,
                                                          const uint8_t* __restrict__ flags_f,
-                                                         const float* __restrict__ dinv_f,
-                                                         const float* __restrict__ b_f, const DomDev* __restrict__ doms_c,
-                                                         const float* __restrict__ z_c, float omega,
-                                                         float* __restrict__ t_f, const int* __restrict__ dom_active) {
+                                                         const DomDev* __restrict__ doms_c,
+                                                         const float* __restrict__ z_c, float* __restrict__ t_f,
+                                                         const int* __restrict__ dom_active) {
   const Tile t = tiles[blockIdx.x / 3];
   if (dom_active && !dom_active[t.dom]) return;
   const DomDev F = doms_f[t.dom];
@@ -230,7 +231,35 @@ __global__ void __launch_bounds__(kThreads) k_mg_prolong(const Tile* __restrict_
         }
     const int64_t k0 = vec_index(nf, 0, lc);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) t_f[k0 + c * kNLC] = fmaf(omega * dinv_f[nf * 3 + c], b_f[k0 + c * kNLC], s[c]);
+    for (int c = 0; c < 3; ++c) t_f[k0 + c * kNLC] += s[c];
+  }
+}
+
+// t = omega D^-1 b on the active interior nodes (pre-smoothing from a zero guess).
+__global__ void __launch_bounds__(kThreads) k_mg_jacobi(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                        const uint8_t* __restrict__ flags,
+                                                        const float* __restrict__ binv, const float* __restrict__ b,
+                                                        float omega, float* __restrict__ t_out,
+                                                        const int* __restrict__ dom_active) {
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  if (yy < 1 || yy > D.n[1] - 2 || zz < 1 || zz > D.n[2] - 2) return;
+  for (int i = 0; i < kTileX; ++i) {
+    const int x = t.x0 + i;
+    if (x > D.n[0] - 2) break;
+    const int64_t n = node_index(D, x, yy, zz);
+    if (!(flags[n] & kNodeActive)) continue;
+    const int64_t k0 = vec_index(n, 0, lc);
+    float r[3], z[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[c] = b[k0 + c * kNLC];
+    block_jacobi(binv, n, omega, r, z);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t_out[k0 + c * kNLC] = z[c];
   }
 }
 

@@ -22,7 +22,7 @@ struct KernelClass {
 };
 
 enum KClassId { kcMatvec32, kcMatvec64, kcUpdate32, kcUpdate64, kcDirection32, kcDirection64, kcColstate,
-                kcReaction, kcProject, kcMg32, kcNumClasses };
+                kcReaction, kcProject, kcMgPre, kcMgPost, kcMgTransfer, kcMgCoarse, kcNumClasses };
 
 struct SolverStats {
   double ms_solve = 0, ms_rotation = 0;
