@@ -85,7 +85,10 @@ typedef struct dtc_options {
                               reaction forces (the reference, mod_struct_calcmat.f90:254-280),
                               error linear in the solve error; 1 = energy products
                               ff = vv^-T (U^T K U), equal at the exact solution, error quadratic */
-  int32_t reserved[4];
+  int32_t chunk_domains;   /* at most this many domains per device pass (0: as many as fit in
+                              80% of the free device memory); the adjoint checkpoints the
+                              displacements of every pass but the last to host memory */
+  int32_t reserved[3];
 } dtc_options;
 
 typedef struct dtc_domain_in {

@@ -135,14 +135,13 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
   if (!(o.rtol > 0 && o.rtol < 1) || o.max_it < 1 || (o.precision != DTC_PREC_FP64 && o.precision != DTC_PREC_MIXED))
     return DTC_ERR_INVALID_ARGUMENT;
   if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 1 ||
-      o.tensor_estimator < 0 || o.tensor_estimator > 1)
+      o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0)
     return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
   h->opt = o;
   int rc = h->solver.init(o.device, h->err);
   if (rc != DTC_OK) { delete h; return (dtc_status)rc; }
-  h->solver.set_keep(o.keep_displacements != 0);
   *handle = h;
   return DTC_OK;
 }
@@ -227,37 +226,45 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     o->status = plans[i].status;
     o->ne = plans[i].ne; o->nn = plans[i].nn; o->nb = plans[i].nb;
     o->n_free_dof = plans[i].n_free_dof;
-    if (plans[i].status == DTC_DOMAIN_OK) tasks.push_back(DomainTask{&in[i], &plans[i], o});
+    if (plans[i].status == DTC_DOMAIN_OK) tasks.push_back(DomainTask{&in[i], &plans[i], o, i});
   }
   // memory-bounded chunks
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { h->err = "cudaMemGetInfo failed"; return DTC_ERR_CUDA; }
   const double budget = 0.80 * (double)free_b;
-  h->last = SolverStats();
-  size_t k = 0;
-  while (k < tasks.size()) {
-    std::vector<DomainTask> chunk;
+  std::vector<size_t> cuts{0};
+  {
     double bytes = 0;
-    while (k < tasks.size()) {
+    for (size_t k = 0; k < tasks.size(); ++k) {
       const dtc_domain_in& d = *tasks[k].in;
       const int mg = d.elem_type == DTC_HEX20 ? 2 : 1;   // HEX20 nodes live on the doubled grid
       const double nb = (double)(mg * d.L[0] + 1) * (mg * d.L[1] + 1) * (mg * d.L[2] + 1) * device_bytes_per_node();
-      if (!chunk.empty() && bytes + nb > budget) break;
+      const bool full = h->opt.chunk_domains > 0 && (int64_t)(k - cuts.back()) >= h->opt.chunk_domains;
+      if (k > cuts.back() && (bytes + nb > budget || full)) { cuts.push_back(k); bytes = 0; }
       bytes += nb;
-      chunk.push_back(tasks[k++]);
     }
+    cuts.push_back(tasks.size());
+  }
+  h->last = SolverStats();
+  const bool keep = h->opt.keep_displacements != 0;
+  h->solver.clear_kept();
+  for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+    if (cuts[c] == cuts[c + 1]) continue;
+    std::vector<DomainTask> chunk(tasks.begin() + cuts[c], tasks.begin() + cuts[c + 1]);
+    // the adjoint keeps the last chunk on the device and checkpoints the others to the host
+    h->solver.set_keep(!keep ? kKeepNone : (c + 2 == cuts.size() ? kKeepDevice : kKeepHost));
     int rc = h->solver.solve(chunk, h->opt, in[0].nu, h->err);
     if (rc != DTC_OK) return (dtc_status)rc;
     const SolverStats& ss = h->solver.stats();
     h->last.ms_solve += ss.ms_solve;
     h->last.kernel_launches += ss.kernel_launches;
     h->last.dof_iterations += ss.dof_iterations;
-    for (int c = 0; c < kcNumClasses; ++c) {
-      h->last.kc[c].name = ss.kc[c].name;
-      h->last.kc[c].launches += ss.kc[c].launches;
-      h->last.kc[c].ms += ss.kc[c].ms;
-      h->last.kc[c].bytes += ss.kc[c].bytes;
-      h->last.kc[c].flops += ss.kc[c].flops;
+    for (int q = 0; q < kcNumClasses; ++q) {
+      h->last.kc[q].name = ss.kc[q].name;
+      h->last.kc[q].launches += ss.kc[q].launches;
+      h->last.kc[q].ms += ss.kc[q].ms;
+      h->last.kc[q].bytes += ss.kc[q].bytes;
+      h->last.kc[q].flops += ss.kc[q].flops;
     }
   }
   std::vector<const double*> ees;
@@ -315,7 +322,10 @@ dtc_status dtc_element_stiffness(int32_t elem_type, double E, double a, double n
 }
 
 dtc_status dtc_energy_grad(dtc_handle* h, const double* dloss_dc, float* const* grad_e, int64_t n) {
-  if (!h || !dloss_dc || !grad_e || n < 0) return DTC_ERR_INVALID_ARGUMENT;
+  if (!h || (n > 0 && (!dloss_dc || !grad_e)) || n < 0) return DTC_ERR_INVALID_ARGUMENT;
+  h->err.clear();
+  if (!h->opt.keep_displacements) { h->err = "energy_grad needs keep_displacements = 1"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (cudaSetDevice(h->opt.device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
   return (dtc_status)h->solver.energy_grad(dloss_dc, grad_e, n, h->err);
 }
 

@@ -732,9 +732,20 @@ struct DeviceSolver::Impl {
   std::vector<std::pair<void**, size_t>> owned;
   void* bufs[64] = {nullptr};
   size_t caps[64] = {0};
-  // last solve kept for the adjoint
-  std::vector<DomDev> last_doms;
-  std::vector<int64_t> last_task_index;
+  // what the solves of the last batch kept for the adjoint: per chunk the domains (node and
+  // voxel offsets of that chunk), their batch positions, and the FP64 displacements, on the
+  // device for the chunk solved last (its buffers are still live) or copied to the host
+  struct AdjChunk {
+    std::vector<DomDev> doms;
+    std::vector<int64_t> index;
+    int64_t nodes = 0, voxels = 0;
+    bool on_device = false;
+    std::vector<double> X;       // host checkpoint: nodes * 72
+    std::vector<float> svox;     // host checkpoint: voxels
+  };
+  std::vector<AdjChunk> adj;
+  int adj_nen = 0;
+  double adj_nu = 0.3;
   bool tensor_matvec = false;   // FP32 inner solve on tcgen05
   // kernel profiling with CUDA events (opt-in)
   bool profile = false;
@@ -781,7 +792,7 @@ namespace {
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
-           bNumBufs };
+           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -1326,7 +1337,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
 
 template <int NEN>
 int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask>& tasks, const dtc_options& opt,
-              double nu, std::string& msg) {
+              double nu, int keep, std::string& msg) {
   DTC_CUDA(cudaSetDevice(I.device));
   cudaStream_t s = I.stream;
   stats_ = SolverStats();
@@ -1717,8 +1728,22 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       }
     }
   }
-  I.last_doms = doms;
-  I.last_task_index = tidx;
+  if (keep != kKeepNone) {
+    DeviceSolver::Impl::AdjChunk c;
+    c.doms = doms;
+    for (int d = 0; d < ndom; ++d) c.index.push_back(tasks[tidx[d]].index);
+    c.nodes = node_total;
+    c.voxels = (int64_t)svox.size();
+    c.on_device = keep == kKeepDevice;
+    if (!c.on_device) {
+      c.X.resize((size_t)node_total * 72);
+      c.svox = svox;
+      DTC_CUDA(cudaMemcpyAsync(c.X.data(), X, vbytes64, cudaMemcpyDeviceToHost, s));
+      DTC_CUDA(cudaStreamSynchronize(s));
+    }
+    I.adj.push_back(std::move(c));
+    I.adj_nen = NEN;
+  }
   return DTC_OK;
 }
 
@@ -1731,12 +1756,206 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   }
   if (nen == 0) return DTC_OK;
   DTC_CUDA(cudaSetDevice(impl_->device));
-  return nen == 20 ? solve_nen<20>(*impl_, stats_, tasks, opt, nu, msg) : solve_nen<8>(*impl_, stats_, tasks, opt, nu, msg);
+  impl_->adj_nu = nu;
+  return nen == 20 ? solve_nen<20>(*impl_, stats_, tasks, opt, nu, keep_, msg)
+                   : solve_nen<8>(*impl_, stats_, tasks, opt, nu, keep_, msg);
 }
 
-int DeviceSolver::energy_grad(const double*, float* const*, int64_t, std::string& msg) {
-  msg = "energy_grad: not available in this build";
-  return DTC_ERR_INTERNAL;
+void DeviceSolver::clear_kept() {
+  if (impl_) impl_->adj.clear();
+}
+
+namespace {
+
+// Nodal mixes of the kept load-case displacements: V[node][c][b] = sum_a X[node][c][a] G[a][b],
+// b < 6 (the columns of dL/dff the 6x6 tensor depends on).  One thread per (node, c).
+__global__ void k_adj_mix(const int64_t* __restrict__ blocks, const DomDev* __restrict__ doms,
+                          const double* __restrict__ X, const double* __restrict__ G, double* __restrict__ V) {
+  const int64_t e = blocks[2 * blockIdx.x], start = blocks[2 * blockIdx.x + 1];
+  const DomDev D = doms[e];
+  const int64_t nn = (int64_t)D.n[0] * D.n[1] * D.n[2];
+  const int64_t i = start + threadIdx.x;
+  if (i >= 3 * nn) return;
+  const int64_t node = D.node_off + i / 3;
+  const int c = (int)(i % 3);
+  const double* x = X + vec_index(node, c, 0);
+  const double* g = G + (int64_t)e * kNLC * 6;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < kNLC; ++a) {
+    const double xa = x[a];
+#pragma unroll
+    for (int b = 0; b < 6; ++b) v[b] = fma(xa, g[a * 6 + b], v[b]);
+  }
+#pragma unroll
+  for (int b = 0; b < 6; ++b) V[(node * 3 + c) * 8 + b] = v[b];
+}
+
+// dL/dE_v = a * sum_{b<6} V_b,v^T Khat u_b,v for every kept voxel (0 elsewhere): the
+// derivative of the energy products u_a^T K u_b (self-adjoint operator, so no adjoint solve).
+__global__ void k_energy_grad(const int64_t* __restrict__ blocks, const DomDev* __restrict__ doms,
+                              const float* __restrict__ svox, const double* __restrict__ X,
+                              const double* __restrict__ V, float* __restrict__ grad) {
+  const int64_t e = blocks[2 * blockIdx.x], start = blocks[2 * blockIdx.x + 1];
+  const DomDev D = doms[e];
+  const int64_t nvox = (int64_t)D.L[0] * D.L[1] * D.L[2];
+  const int64_t v = start + threadIdx.x;
+  if (v >= nvox) return;
+  const int64_t gi = D.vox_off + v;
+  if (svox[gi] == 0.0f) { grad[gi] = 0.0f; return; }
+  const int vx = (int)(v % D.L[0]), vy = (int)((v / D.L[0]) % D.L[1]), vz = (int)(v / ((int64_t)D.L[0] * D.L[1]));
+  int64_t nodes[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    nodes[a] = node_index(D, vx + Elem<8>::off(a, 0), vy + Elem<8>::off(a, 1), vz + Elem<8>::off(a, 2));
+  double sum = 0.0;
+  for (int b = 0; b < 6; ++b) {
+    double u[24], w[24];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[3 * a + c] = X[vec_index(nodes[a], c, b)];
+        w[3 * a + c] = V[(nodes[a] * 3 + c) * 8 + b];
+      }
+#pragma unroll
+    for (int i = 0; i < 24; ++i) {
+      double r = 0.0;
+#pragma unroll
+      for (int j = 0; j < 24; ++j) r = fma(c_khat64[i + 24 * j], u[j], r);
+      sum = fma(w[i], r, sum);
+    }
+  }
+  grad[gi] = (float)(D.scale * sum);
+}
+
+// dL/dff (24 x 24, column-major) of L through C = fv * meps (mod_struct_calcmat.f90:345-359,
+// 434-439) given dL/dC (column-major 6 x 6): only the first 6 load-case columns are touched.
+void dloss_dff(const double* dc, const int64_t L[3], const double delta, double* lff) {
+  std::memset(lff, 0, sizeof(double) * 576);
+  const double X = (double)L[0] * delta, Y = (double)L[1] * delta, Z = (double)L[2] * delta;
+  const double meps[6] = {1e6, 1e6, 1e6, -1e6, -1e6, 1e6};
+  auto add = [&](int r, int c, double w) { lff[(r - 1) + 24 * c] += w; };
+  for (int c = 0; c < 6; ++c) {
+    const double g0 = dc[0 + 6 * c] * meps[c], g1 = dc[1 + 6 * c] * meps[c], g2 = dc[2 + 6 * c] * meps[c];
+    const double g3 = dc[3 + 6 * c] * meps[c], g4 = dc[4 + 6 * c] * meps[c], g5 = dc[5 + 6 * c] * meps[c];
+    for (int r : {2, 3, 6, 7}) add(r, c, g0 / (Y * Z));
+    for (int r : {11, 12, 15, 16}) add(r, c, g1 / (X * Z));
+    for (int r : {21, 22, 23, 24}) add(r, c, g2 / (X * Y));
+    for (int r : {3, 4, 7, 8}) add(r, c, 0.5 * g3 / (X * Z));
+    for (int r : {10, 11, 14, 15}) add(r, c, 0.5 * g3 / (Y * Z));
+    for (int r : {5, 6, 7, 8}) add(r, c, 0.5 * g4 / (X * Y));
+    for (int r : {18, 19, 22, 23}) add(r, c, 0.5 * g4 / (Y * Z));
+    for (int r : {13, 14, 15, 16}) add(r, c, 0.5 * g5 / (X * Y));
+    for (int r : {19, 20, 23, 24}) add(r, c, 0.5 * g5 / (X * Z));
+  }
+}
+
+}  // namespace
+
+int DeviceSolver::energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, std::string& msg) {
+  Impl& I = *impl_;
+  DTC_CUDA(cudaSetDevice(I.device));
+  cudaStream_t s = I.stream;
+  if (I.adj.empty()) { msg = "energy_grad: no kept displacements (solve with keep_displacements = 1 first)"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (I.adj_nen != 8) { msg = "energy_grad: HEX08 domains only"; return DTC_ERR_INVALID_ARGUMENT; }
+  // G = vv_bc^-1 dL/dff (24 x 6 per domain, row-major a * 6 + b): the energy-product form of ff
+  double uu[8 * 3 * 24], vinv[576];
+  macro_modes(1e-6, uu);
+  for (int lc = 0; lc < 24; ++lc)
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 8; ++l) vinv[(8 * k + l) + 24 * lc] = uu[l + 8 * k + 24 * lc];
+  {
+    // Gauss-Jordan on a copy (the same inverse the forward uses)
+    double a[576], inv[576];
+    std::memcpy(a, vinv, sizeof(a));
+    for (int i = 0; i < 576; ++i) inv[i] = (i % 25 == 0) ? 1.0 : 0.0;
+    for (int c = 0; c < 24; ++c) {
+      int p = c;
+      for (int r = c + 1; r < 24; ++r) if (std::fabs(a[r + 24 * c]) > std::fabs(a[p + 24 * c])) p = r;
+      for (int k = 0; k < 24; ++k) { std::swap(a[c + 24 * k], a[p + 24 * k]); std::swap(inv[c + 24 * k], inv[p + 24 * k]); }
+      const double d = a[c + 24 * c];
+      for (int k = 0; k < 24; ++k) { a[c + 24 * k] /= d; inv[c + 24 * k] /= d; }
+      for (int r = 0; r < 24; ++r) {
+        if (r == c) continue;
+        const double f = a[r + 24 * c];
+        if (f == 0.0) continue;
+        for (int k = 0; k < 24; ++k) { a[r + 24 * k] -= f * a[c + 24 * k]; inv[r + 24 * k] -= f * inv[c + 24 * k]; }
+      }
+    }
+    std::memcpy(vinv, inv, sizeof(inv));
+  }
+  int e;
+  for (const Impl::AdjChunk& ch : I.adj) {
+    const int nd = (int)ch.doms.size();
+    std::vector<double> G((size_t)nd * kNLC * 6, 0.0);
+    for (int d = 0; d < nd; ++d) {
+      const int64_t k = ch.index[d];
+      if (k < 0 || k >= n) continue;
+      const DomDev& D = ch.doms[d];
+      const int64_t L[3] = {D.L[0], D.L[1], D.L[2]};
+      double lff[576];
+      dloss_dff(dloss_dc + 36 * k, L, D.delta, lff);
+      for (int a = 0; a < 24; ++a)
+        for (int b = 0; b < 6; ++b) {
+          double sum = 0.0;
+          for (int r = 0; r < 24; ++r) sum += vinv[a + 24 * r] * lff[r + 24 * b];
+          G[(size_t)d * kNLC * 6 + a * 6 + b] = sum;
+        }
+    }
+    // block tables (domain, first item) for the node and voxel kernels
+    std::vector<int64_t> nb, vb;
+    for (int d = 0; d < nd; ++d) {
+      const DomDev& D = ch.doms[d];
+      const int64_t items = 3 * (int64_t)D.n[0] * D.n[1] * D.n[2], vox = (int64_t)D.L[0] * D.L[1] * D.L[2];
+      for (int64_t q = 0; q < items; q += 256) { nb.push_back(d); nb.push_back(q); }
+      for (int64_t q = 0; q < vox; q += 128) { vb.push_back(d); vb.push_back(q); }
+    }
+    if ((e = ensure(I, bAdjG, sizeof(double) * G.size(), msg)) ||
+        (e = ensure(I, bAdjV, sizeof(double) * 24 * std::max<int64_t>(ch.nodes, 1), msg)) ||
+        (e = ensure(I, bAdjBlk, sizeof(int64_t) * (nb.size() + vb.size()), msg)) ||
+        (e = ensure(I, bAdjGrad, sizeof(float) * std::max<int64_t>(ch.voxels, 1), msg)) ||
+        (e = ensure(I, bAdjDoms, sizeof(DomDev) * nd, msg)))
+      return e;
+    const double* X;
+    const float* sv;
+    if (ch.on_device) {
+      X = B<double>(I, bX);
+      sv = B<float>(I, bSvox);
+    } else {
+      if ((e = ensure(I, bAdjX, sizeof(double) * ch.X.size(), msg)) ||
+          (e = ensure(I, bAdjSvox, sizeof(float) * std::max<size_t>(ch.svox.size(), 1), msg)))
+        return e;
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bAdjX], ch.X.data(), sizeof(double) * ch.X.size(), cudaMemcpyHostToDevice, s));
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bAdjSvox], ch.svox.data(), sizeof(float) * ch.svox.size(),
+                               cudaMemcpyHostToDevice, s));
+      X = B<double>(I, bAdjX);
+      sv = B<float>(I, bAdjSvox);
+    }
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bAdjG], G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bAdjDoms], ch.doms.data(), sizeof(DomDev) * nd, cudaMemcpyHostToDevice, s));
+    std::vector<int64_t> blk(nb);
+    blk.insert(blk.end(), vb.begin(), vb.end());
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bAdjBlk], blk.data(), sizeof(int64_t) * blk.size(), cudaMemcpyHostToDevice, s));
+    const int64_t* blocks = B<int64_t>(I, bAdjBlk);
+    if (!nb.empty())
+      k_adj_mix<<<(unsigned)(nb.size() / 2), 256, 0, s>>>(blocks, B<DomDev>(I, bAdjDoms), X, B<double>(I, bAdjG),
+                                                          B<double>(I, bAdjV));
+    if (!vb.empty())
+      k_energy_grad<<<(unsigned)(vb.size() / 2), 128, 0, s>>>(blocks + nb.size(), B<DomDev>(I, bAdjDoms), sv, X,
+                                                              B<double>(I, bAdjV), B<float>(I, bAdjGrad));
+    if ((e = launch_check(msg))) return e;
+    std::vector<float> hg((size_t)ch.voxels);
+    if (ch.voxels)
+      DTC_CUDA(cudaMemcpyAsync(hg.data(), I.bufs[bAdjGrad], sizeof(float) * hg.size(), cudaMemcpyDeviceToHost, s));
+    DTC_CUDA(cudaStreamSynchronize(s));
+    for (int d = 0; d < nd; ++d) {
+      const int64_t k = ch.index[d];
+      if (k < 0 || k >= n || !grad_e[k]) continue;
+      const DomDev& D = ch.doms[d];
+      std::memcpy(grad_e[k], hg.data() + D.vox_off, sizeof(float) * (size_t)D.L[0] * D.L[1] * D.L[2]);
+    }
+  }
+  return DTC_OK;
 }
 
 }  // namespace dtc

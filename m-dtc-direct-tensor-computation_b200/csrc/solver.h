@@ -13,7 +13,12 @@ struct DomainTask {
   const dtc_domain_in* in = nullptr;
   MeshPlan* plan = nullptr;
   dtc_domain_out* out = nullptr;
+  int64_t index = 0;          // position in the caller's batch
 };
+
+// What a solve keeps for the adjoint: nothing, the displacements on the device (the chunk
+// solved last), or a host copy (earlier chunks of a batch split by device memory).
+enum KeepMode { kKeepNone = 0, kKeepDevice = 1, kKeepHost = 2 };
 
 struct KernelClass {
   const char* name = "";
@@ -43,12 +48,14 @@ class DeviceSolver {
   // Adjoint: dL/dE_voxel for the domains of the last solve (kept displacements).
   int energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, std::string& msg);
   const SolverStats& stats() const { return stats_; }
-  void set_keep(bool keep) { keep_ = keep; }
+  void set_keep(int mode) { keep_ = mode; }
+  // Forget what earlier solves kept for the adjoint (start of a batch).
+  void clear_kept();
 
  private:
   Impl* impl_ = nullptr;
   SolverStats stats_;
-  bool keep_ = false;
+  int keep_ = kKeepNone;
 };
 
 }  // namespace dtc
