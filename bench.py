@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     p.add_argument("--profile-step", action="store_true",
                    help="one warm-up and one timed-free mixed solve only (for ncu captures)")
+    p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4"],
+                   help="c1 (default): the headline line; c0/c2/c3/c4 print their own measurement lines")
     return p.parse_args()
 
 
@@ -172,11 +174,151 @@ def run_reference(args, dtc):
     print(json.dumps(line), flush=True)
 
 
+
+def _timed(fn, steps, warmup):
+    """Device time per call (the library's CUDA-event solve time) and host wall time."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    dev, wall = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        d = fn()
+        wall.append(time.perf_counter() - t0)
+        dev.append(d)
+    torch.cuda.synchronize()
+    return float(np.mean(dev)), float(np.mean(wall))
+
+
+def _err(res, truth):
+    return max(float(np.abs(r["c"] - t["c"]).max() / np.abs(t["c"]).max()) for r, t in zip(res, truth)
+               if r["status"] == 0 and t["status"] == 0)
+
+
+def run_config(args, dtc):
+    """Measurement lines of the other workloads (not the headline metric line)."""
+    import torch
+    syn = dtc.synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    steps, warm = max(1, args.steps), max(1, min(args.warmup, 3))
+    line = {"config_id": args.config, "n_gpus": 1, "data": "synthetic"}
+    if args.config == "c0":
+        # 62^3 volume (60^3 core and a 1-voxel frame), BV/TV 0.25, 27 domains of 20^3, FP64 rtol 1e-10
+        vol = syn.bone_volume((62, 62, 62), 0.25, syn.seed_for(0, 0))
+        parts = syn.volume_domains(vol, 20)
+        doms = [dtc.Domain(sub, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, xa_n=xa, domain_number=d)
+                for d, xa, sub in parts]
+        with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=True, device=local) as sv:
+            def step():
+                sv.solve(doms)
+                return sv.stats()["ms_solve"]
+            dev, wall = _timed(step, steps, warm)
+        orc = ge.load_oracle()
+        odoms = [orc.Domain(sub, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, xa_n=xa, rotation=True)
+                 for _, xa, sub in parts]
+        cores = min(len(odoms), os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        orc.solve_batch(odoms, nthreads=cores)
+        tcpu = time.perf_counter() - t0
+        line.update({"workload": "27 HEX08 domains of 20^3 from a 62^3 volume (BV/TV 0.25), FP64 rtol 1e-10, "
+                                 "rotation search", "gpu_ms_device": dev, "gpu_ms_wall": wall,
+                     "gpu_domains_per_s_wall": len(doms) / wall,
+                     "cpu_oracle_s": tcpu, "cpu_cores": cores, "cpu_domains_per_s": len(doms) / tcpu})
+    elif args.config == "c2":
+        # 256 HEX20 domains of 24^3, BV/TV 0.25, mixed vs plain FP64
+        n = min(args.ndom, 256)
+        grays = [syn.bone_volume((24, 24, 24), 0.25, syn.seed_for(2, i)) for i in range(n)]
+        doms = [dtc.Domain(g, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA,
+                           E_voxel=syn.modulus_of_gray(g)) for g in grays]
+        sample = doms[:: max(1, n // 8)]
+        with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device=local) as ref:
+            truth = ref.solve(sample)
+        out = {}
+        for arm, kw, rt in (("mixed", dict(precision="mixed", estimator="energy", inner_precond="block"), 3e-6),
+                            ("fp64", dict(precision="fp64"), 3e-7)):
+            with dtc.Solver(rtol=rt, rotation_search=False, device=local, **kw) as sv:
+                err = _err(sv.solve(sample), truth)
+
+                def step():
+                    sv.solve(doms)
+                    return sv.stats()["ms_solve"]
+                dev, wall = _timed(step, steps, warm)
+            out[arm] = {"domains_per_s": n / (dev / 1e3), "ms_per_step": dev, "rtol": rt, "max_rel_err": err,
+                        "e2e_domains_per_s": n / wall}
+        line.update({"workload": f"{n} HEX20 domains of 24^3, BV/TV 0.25, per-voxel E", "mixed": out["mixed"],
+                     "fp64_plain": out["fp64"],
+                     "speedup_mixed_over_fp64": out["mixed"]["domains_per_s"] / out["fp64"]["domains_per_s"]})
+    elif args.config == "c3":
+        # 2000 HEX08 domains, L ~ U{16,24,32,48,64}, BV/TV ~ U(0.05,0.45), mixed + MG, CUDA graphs,
+        # rotation search in the step
+        n = min(args.ndom, 2000)
+        rng = np.random.default_rng(syn.seed_for(3, 10_000))
+        Ls = rng.choice([16, 24, 32, 48, 64], size=n)
+        bv = rng.uniform(0.05, 0.45, size=n)
+        grays = [syn.bone_volume((int(L),) * 3, float(b), syn.seed_for(3, i)) for i, (L, b) in enumerate(zip(Ls, bv))]
+        doms = [dtc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=syn.modulus_of_gray(g),
+                           domain_number=i) for i, g in enumerate(grays)]
+        with dtc.Solver(precision="mixed", rtol=3e-5, rotation_search=True, device=local, estimator="energy",
+                        inner_precond="mg") as sv:
+            res = []
+
+            def step():
+                res[:] = sv.solve(doms)
+                return sv.stats()["ms_solve"]
+            dev, wall = _timed(step, steps, warm)
+        sample = [i for i in range(0, n, max(1, n // 12))]
+        with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device=local) as ref:
+            truth = ref.solve([doms[i] for i in sample])
+        ok = sum(r["status"] == 0 for r in res)
+        line.update({"workload": f"{n} HEX08 domains, L in {{16,24,32,48,64}}, BV/TV U(0.05,0.45), mixed+MG, "
+                                 "CUDA-graph CG chunks, rotation search",
+                     "domains_per_s_device": n / (dev / 1e3), "domains_per_s_wall": n / wall, "ms_device": dev,
+                     "ms_wall": wall, "domains_solved": ok,
+                     "max_rel_err_vs_fp64_1e-10": _err([res[i] for i in sample], truth),
+                     "voxels": int(sum(int(L) ** 3 for L in Ls))})
+    elif args.config == "c4":
+        # adjoint: 64 HEX08 domains of 48^3, loss ||C - C_target||_F^2, gradient vs one forward solve
+        n = min(args.ndom, 64)
+        grays = [syn.bone_volume((48, 48, 48), 0.25, syn.seed_for(4, i)) for i in range(n)]
+        E = [syn.modulus_of_gray(g) for g in grays]
+        doms = [dtc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=e) for g, e in zip(grays, E)]
+        rng = np.random.default_rng(syn.seed_for(4, 99))
+        target = np.zeros((n, 6, 6))
+        for i in range(n):
+            target[i][range(3), range(3)] = rng.uniform(3000, 15000, 3)
+            target[i][range(3, 6), range(3, 6)] = rng.uniform(1000, 5000, 3)
+        grads = [np.zeros(g.shape, np.float32) for g in grays]
+        with dtc.Solver(precision="mixed", rtol=1e-6, rotation_search=False, device=local, estimator="energy",
+                        inner_precond="mg", keep_displacements=True) as sv:
+            fwd, bwd = [], []
+            for k in range(warm + steps):
+                t0 = time.perf_counter()
+                res = sv.solve(doms)
+                t1 = time.perf_counter()
+                dc = np.stack([2.0 * (r["c"] - target[i]) for i, r in enumerate(res)])
+                sv.energy_grad(dc, grads)
+                t2 = time.perf_counter()
+                if k >= warm:
+                    fwd.append(t1 - t0)
+                    bwd.append(t2 - t1)
+        line.update({"workload": f"adjoint: {n} HEX08 domains of 48^3, BV/TV 0.25, per-voxel E, "
+                                 "loss ||C - C_target||_F^2, mixed+MG forward at rtol 1e-6",
+                     "forward_s": float(np.mean(fwd)), "adjoint_s": float(np.mean(bwd)),
+                     "adjoint_over_forward": float(np.mean(bwd) / np.mean(fwd)),
+                     "grad_abs_max": float(max(np.abs(g).max() for g in grads))})
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     dtc = ge.load_package()
     if args.impl == "reference":
         run_reference(args, dtc)
+        return
+    if args.config != "c1":
+        run_config(args, dtc)
         return
     import torch
     import torch.distributed as dist

@@ -88,7 +88,9 @@ typedef struct dtc_options {
   int32_t chunk_domains;   /* at most this many domains per device pass (0: as many as fit in
                               80% of the free device memory); the adjoint checkpoints the
                               displacements of every pass but the last to host memory */
-  int32_t reserved[3];
+  int32_t graph_chunks;    /* 0: each chunk of CG iterations is captured once and replayed as a
+                              CUDA graph; 1: kernels are launched one by one */
+  int32_t reserved[2];
 } dtc_options;
 
 typedef struct dtc_domain_in {
@@ -189,8 +191,10 @@ dtc_status dtc_element_stiffness(int32_t elem_type, double E, double a, double n
 dtc_status dtc_energy_grad(dtc_handle* handle, const double* dloss_dc, float* const* grad_e,
                            int64_t n);
 
-/* Timing and work counters of the last dtc_solve_batch: device solve wall time (ms),
- * kernels launched, and sum over domains of free DOFs x load cases x CG iterations. */
+/* Timing and work counters of the last dtc_solve_batch: device time of the solve in ms
+ * (CUDA events on the solver stream, from the uploaded voxel factors to the last kernel,
+ * summed over device passes; host meshing excluded), kernels launched, and the sum over
+ * domains of free DOFs x load cases x CG iterations. */
 dtc_status dtc_get_stats(const dtc_handle* handle, double* ms_solve, int64_t* kernel_launches,
                          double* dof_iterations);
 

@@ -94,7 +94,7 @@ class Solver:
     def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=0.0, max_refine=12,
                  rotation_search=True, device=0, host_threads=0, keep_displacements=False,
                  profile_kernels=False, mixed_matvec="simt", inner_precond="block", estimator="reaction",
-                 chunk_domains=0):
+                 chunk_domains=0, graphs=True):
         self.lib = capi.load()
         o = capi.Options()
         self.lib.dtc_default_options(C.byref(o))
@@ -107,6 +107,7 @@ class Solver:
         o.inner_precond = {"jacobi": 0, "block": 1, "mg": 2}[inner_precond]
         o.tensor_estimator = {"reaction": 0, "energy": 1}[estimator]
         o.chunk_domains = int(chunk_domains)
+        o.graph_chunks = 0 if graphs else 1
         self.options = o
         h = C.c_void_p()
         rc = self.lib.dtc_create(C.byref(h), C.byref(o))

@@ -27,7 +27,8 @@ class Options(C.Structure):
         ("rotation_search", C.c_int32), ("device", C.c_int32), ("host_threads", C.c_int32),
         ("keep_displacements", C.c_int32), ("profile_kernels", C.c_int32),
         ("mixed_matvec", C.c_int32), ("inner_precond", C.c_int32),
-        ("tensor_estimator", C.c_int32), ("chunk_domains", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("tensor_estimator", C.c_int32), ("chunk_domains", C.c_int32), ("graph_chunks", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

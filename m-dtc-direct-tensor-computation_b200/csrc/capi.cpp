@@ -135,7 +135,8 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
   if (!(o.rtol > 0 && o.rtol < 1) || o.max_it < 1 || (o.precision != DTC_PREC_FP64 && o.precision != DTC_PREC_MIXED))
     return DTC_ERR_INVALID_ARGUMENT;
   if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 1 ||
-      o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0)
+      o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0 || o.graph_chunks < 0 ||
+      o.graph_chunks > 1)
     return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
@@ -257,6 +258,7 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     if (rc != DTC_OK) return (dtc_status)rc;
     const SolverStats& ss = h->solver.stats();
     h->last.ms_solve += ss.ms_solve;
+    h->last.ms_wall += ss.ms_wall;
     h->last.kernel_launches += ss.kernel_launches;
     h->last.dof_iterations += ss.dof_iterations;
     for (int q = 0; q < kcNumClasses; ++q) {

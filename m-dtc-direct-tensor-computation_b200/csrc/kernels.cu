@@ -114,8 +114,10 @@ __device__ __forceinline__ void load_voxels(float (&sp)[2][2], const float* __re
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
 // node of the grid (reaction forces).
+// FP32: capped at 128 registers (4 CTAs per SM) -- a few spills, ~5% faster than 155 registers
 template <typename T, bool ALL, bool DOT>
-__global__ void __launch_bounds__(kThreads) k_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_matvec(const Tile* __restrict__ tiles,
+                                                                          const DomDev* __restrict__ doms,
                                                      const float* __restrict__ svox, const T* __restrict__ u,
                                                      T* __restrict__ y, double scale, double* __restrict__ acc,
                                                      const int* __restrict__ dom_active) {
@@ -747,6 +749,8 @@ struct DeviceSolver::Impl {
   int adj_nen = 0;
   double adj_nu = 0.3;
   bool tensor_matvec = false;   // FP32 inner solve on tcgen05
+  bool graphs = true;           // replay CG chunks as CUDA graphs
+  cudaEvent_t ev_solve[2] = {nullptr, nullptr};
   // kernel profiling with CUDA events (opt-in)
   bool profile = false;
   std::vector<cudaEvent_t> ev;
@@ -819,7 +823,8 @@ DeviceSolver::~DeviceSolver() {
   if (impl_) {
     if (impl_->device >= 0) cudaSetDevice(impl_->device);
     for (cudaEvent_t e : impl_->ev) cudaEventDestroy(e);
-    for (int i = 0; i < 32; ++i) if (impl_->bufs[i]) cudaFree(impl_->bufs[i]);
+    for (cudaEvent_t e : impl_->ev_solve) if (e) cudaEventDestroy(e);
+    for (void* b : impl_->bufs) if (b) cudaFree(b);
     if (impl_->stream) cudaStreamDestroy(impl_->stream);
     delete impl_;
   }
@@ -1179,8 +1184,10 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   const unsigned g = (unsigned)(3 * nsm);
   int q = fine ? I.begin(0) : -1;
   k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, P.omega, t, act);
+  if (fine) I.end(kcMgJacobi, q, 2 * vb + vb / 12, 0);   // b in, t out, 6 floats of D^-1 per node
+  q = fine ? I.begin(0) : -1;
   k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
-  if (fine) I.end(kcMgPre, q, mb + 2 * vb + vb / 3, mf);
+  if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
   ++launches;
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
   q = fine ? I.begin(0) : -1;
@@ -1200,10 +1207,43 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
     k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, zz, zr, act);
   else
     k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
-  if (fine) I.end(kcMgPost, q, mb + 2 * vb + vb / 3, mf);
+  if (fine) I.end(kcMgPost, q, mb + vb + vb / 12, mf);     // t in, z out (mb), b in, D^-1
   if (!fine) I.end(kcMgCoarse, q1, 0, 0);
   launches += 2;
 }
+
+// One chunk of CG iterations replayed as a CUDA graph: captured on first use (every kernel
+// argument is fixed for the whole solve), then one cudaGraphLaunch per chunk instead of a few
+// hundred launches.  Profiling runs launch directly so that their event records stay per kernel.
+struct ChunkGraph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;   // kernels in one chunk
+  ~ChunkGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  template <class Body>
+  int run(cudaStream_t s, bool direct, int64_t& counter, Body&& body, std::string& msg) {
+    if (direct) {
+      body(counter);
+      return DTC_OK;
+    }
+    if (!exec) {
+      cudaGraph_t g = nullptr;
+      DTC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int64_t n = 0;
+      body(n);
+      const cudaError_t ec = cudaStreamEndCapture(s, &g);
+      if (ec != cudaSuccess) { msg = std::string("chunk capture: ") + cudaGetErrorString(ec); return DTC_ERR_CUDA; }
+      const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) { exec = nullptr; msg = std::string("chunk graph: ") + cudaGetErrorString(ei); return DTC_ERR_CUDA; }
+      launches = n;
+    }
+    DTC_CUDA(cudaGraphLaunch(exec, s));
+    counter += launches;
+    return DTC_OK;
+  }
+};
 
 template <typename T, bool BLOCK, int NEN>
 int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* w, const T* dinv,
@@ -1229,32 +1269,37 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
   if (int e = launch_check(msg)) return e;
   const int chunk = 32;
   int h_count = 1;
+  ChunkGraph graph;
   for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
     const bool f32 = sizeof(T) == 4;
     const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(T) : 0;
     const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(T) : 0;
     const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
-    for (int k = 0; k < chunk; ++k) {
-      if (nti > 0) {
-        int q = I.begin(0);
-        k_direction<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
-        I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
-        q = I.begin(0);
-        if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
-          launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
-                           B<int>(I, bErr), s);
-        else
-          apply_k<T, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
-        I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
-        q = I.begin(0);
-        k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
-        I.end(f32 ? kcUpdate32 : kcUpdate64, q, 6 * vb, 0);
+    auto body = [&](int64_t& nl) {
+      for (int k = 0; k < chunk; ++k) {
+        if (nti > 0) {
+          int q = I.begin(0);
+          k_direction<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
+          I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
+          q = I.begin(0);
+          if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
+            launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
+                             B<int>(I, bErr), s);
+          else
+            apply_k<T, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
+          I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
+          q = I.begin(0);
+          k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
+          I.end(f32 ? kcUpdate32 : kcUpdate64, q, 6 * vb, 0);
+          nl += 3;
+        }
+        const int q = I.begin(0);
+        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+        I.end(kcColstate, q, 0, 0);
+        nl += 1;
       }
-      int q = I.begin(0);
-      k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
-      I.end(kcColstate, q, 0, 0);
-      launches += 4;
-    }
+    };
+    if (int e = graph.run(s, I.profile || !I.graphs, launches, body, msg)) return e;
     k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
     launches += 1;
     if (int e = launch_check(msg)) return e;
@@ -1296,29 +1341,33 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   if (int e = launch_check(msg)) return e;
   const int chunk = 16;
   int h_count = 1;
+  ChunkGraph graph;
   for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
     const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(float) : 0;
     const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(float) : 0;
     const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
-    for (int k = 0; k < chunk; ++k) {
-      if (nti > 0) {
-        int q = I.begin(0);
-        k_direction_z<<<grid, kThreads, 0, s>>>(ti, dd, fl, M.z0, p, st, act);
-        I.end(kcDirection32, q, 3 * vb, 0);
-        q = I.begin(0);
-        k_matvec<float, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
-        I.end(kcMatvec32, q, mb, mf);
-        q = I.begin(0);
-        k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, act);
-        I.end(kcUpdate32, q, 6 * vb, 0);
-        mg_vcycle(I, M, 0, r, zz, zr, act, launches);
-        launches += 3;
+    auto body = [&](int64_t& nl) {
+      for (int k = 0; k < chunk; ++k) {
+        if (nti > 0) {
+          int q = I.begin(0);
+          k_direction_z<<<grid, kThreads, 0, s>>>(ti, dd, fl, M.z0, p, st, act);
+          I.end(kcDirection32, q, 3 * vb, 0);
+          q = I.begin(0);
+          k_matvec<float, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+          I.end(kcMatvec32, q, mb, mf);
+          q = I.begin(0);
+          k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, act);
+          I.end(kcUpdate32, q, 6 * vb, 0);
+          mg_vcycle(I, M, 0, r, zz, zr, act, nl);
+          nl += 3;
+        }
+        const int q = I.begin(0);
+        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+        I.end(kcColstate, q, 0, 0);
+        nl += 1;
       }
-      const int q = I.begin(0);
-      k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
-      I.end(kcColstate, q, 0, 0);
-      launches += 1;
-    }
+    };
+    if (int e = graph.run(s, I.profile || !I.graphs, launches, body, msg)) return e;
     k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
     launches += 1;
     if (int e = launch_check(msg)) return e;
@@ -1343,12 +1392,13 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   stats_ = SolverStats();
   static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
                                              "direction_f32", "direction_f64", "colstate", "reaction_f64",
-                                             "project_f64", "mg_presmooth_f32", "mg_postsmooth_f32",
-                                             "mg_transfer_f32", "mg_coarse_levels_f32"};
+                                             "project_f64", "mg_jacobi_f32", "mg_residual_f32",
+                                             "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
   I.tensor_matvec = opt.mixed_matvec == 1;
+  I.graphs = opt.graph_chunks == 0;
   I.pending.clear();
   I.h_active.clear();
   I.dom_mv_bytes.clear(); I.dom_mv_flops.clear(); I.dom_vec_bytes.clear();
@@ -1521,6 +1571,13 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaMemsetAsync(I.bufs[bX], 0, vbytes64, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bR64], 0, vbytes64, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * 576 * ndom, s));
+  // device time of the solve, inputs resident: from here (voxel factors and work lists
+  // uploaded) to the last kernel, measured with CUDA events on the solver stream
+  if (!I.ev_solve[0]) {
+    DTC_CUDA(cudaEventCreate(&I.ev_solve[0]));
+    DTC_CUDA(cudaEventCreate(&I.ev_solve[1]));
+  }
+  DTC_CUDA(cudaEventRecord(I.ev_solve[0], s));
   const Tile* ti = B<Tile>(I, bTilesI);
   const Tile* ta = B<Tile>(I, bTilesA);
   const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba};
@@ -1671,6 +1728,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     L += 2;
   }
   if ((e = launch_check(msg))) return e;
+  DTC_CUDA(cudaEventRecord(I.ev_solve[1], s));
   std::vector<double> ff((size_t)576 * ndom);
   std::vector<ColState> cs(ncol);
   DTC_CUDA(cudaMemcpyAsync(ff.data(), I.bufs[bFf], sizeof(double) * ff.size(), cudaMemcpyDeviceToHost, s));
@@ -1690,7 +1748,12 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaStreamSynchronize(s));
   I.flush();
   if (h_err) { msg = "tensor-core matvec: an mbarrier wait timed out"; return DTC_ERR_INTERNAL; }
-  stats_.ms_solve = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  stats_.ms_wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  {
+    float ms = 0.f;
+    DTC_CUDA(cudaEventElapsedTime(&ms, I.ev_solve[0], I.ev_solve[1]));
+    stats_.ms_solve = ms;
+  }
   for (int d = 0; d < ndom; ++d) {
     DomainTask& t = tasks[tidx[d]];
     dtc_domain_out* o = t.out;

@@ -27,10 +27,12 @@ struct KernelClass {
 };
 
 enum KClassId { kcMatvec32, kcMatvec64, kcUpdate32, kcUpdate64, kcDirection32, kcDirection64, kcColstate,
-                kcReaction, kcProject, kcMgPre, kcMgPost, kcMgTransfer, kcMgCoarse, kcNumClasses };
+                kcReaction, kcProject, kcMgJacobi, kcMgResidual, kcMgPost, kcMgTransfer, kcMgCoarse, kcNumClasses };
 
 struct SolverStats {
-  double ms_solve = 0, ms_rotation = 0;
+  double ms_solve = 0;   // device time of the solve (CUDA events, inputs resident)
+  double ms_wall = 0;    // host wall time of the same section
+  double ms_rotation = 0;
   int64_t kernel_launches = 0;
   double dof_iterations = 0;  // sum over domains of free DOFs x load cases x iterations
   KernelClass kc[kcNumClasses];

@@ -229,3 +229,18 @@ def test_multigrid_uneven_sizes(dtc, orc):
     for r, ref in zip(res, refs):
         assert r["status"] == 0
         assert rel(r["c"], ref["c"]) <= TOL_MIXED
+
+
+@pytest.mark.parametrize("precision,precond,tol", [("fp64", "jacobi", 1e-7), ("mixed", "mg", 1e-5)])
+def test_graph_replay_matches_direct_launches(dtc, batch, precision, precond, tol):
+    """CG chunks replayed as CUDA graphs give the results of kernel-by-kernel launches (up to
+    the order of the atomic dot-product sums)."""
+    pairs, _ = batch
+    out = {}
+    for graphs in (True, False):
+        with dtc.Solver(precision=precision, rtol=1e-8, rotation_search=False, inner_precond=precond,
+                        graphs=graphs) as s:
+            out[graphs] = s.solve([p[0] for p in pairs])
+    for a, b in zip(out[True], out[False]):
+        assert rel(a["c"], b["c"]) <= tol
+        assert np.abs(a["iters"] - b["iters"]).max() <= 2
