@@ -31,7 +31,6 @@ __constant__ double c_khat64[576];   // unit voxel stiffness, column-major (symm
 __constant__ float c_khat32[576];
 __constant__ double c_uu[8 * 3 * kNLC];  // macro modes uu(8,3,24) for eps = 1e-6
 __constant__ double c_k20_64[3600];       // unit HEX20 element matrix (ring node order)
-__constant__ float c_k20_32[3600];
 
 template <typename T> struct KhatC;
 template <> struct KhatC<float> {
@@ -796,7 +795,7 @@ namespace {
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
-           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bNumBufs };
+           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -849,12 +848,12 @@ namespace {
 
 // CG on one precision: x (interior part), r = b on entry, p = 0 on entry.
 template <typename T, int NEN, bool ALL, bool DOT>
-void launch_ebe(const Tile* bricks, int64_t nb, const DomDev* dd, const float* svox, const uint8_t* fl, const T* u, T* y,
-                double scale, double* acc, const int* act, cudaStream_t s) {
+void launch_ebe(const Tile* bricks, int64_t nb, const DomDev* dd, const float* svox, const uint8_t* fl, const T* ke,
+                const T* u, T* y, double scale, double* acc, const int* act, cudaStream_t s) {
   using S = EbeShape<T, NEN>;
   if (nb <= 0) return;
-  k_ebe<T, NEN, ALL, DOT><<<(unsigned)(S::NGRP * nb), S::kThreadsEbe, S::smem, s>>>(bricks, dd, svox, fl, u, y, scale,
-                                                                                    acc, act);
+  k_ebe<T, NEN, ALL, DOT><<<(unsigned)(S::NGRP * nb), S::kThreadsEbe, S::smem, s>>>(bricks, dd, svox, fl, ke, u, y,
+                                                                                    scale, acc, act);
 }
 
 template <typename T, int NEN, bool ALL, bool DOT>
@@ -879,6 +878,8 @@ int allow_all_ebe(std::string& msg) {
 struct Work {
   const Tile *ti, *ta, *bi, *ba;
   int64_t nti, nta, nbi, nba;
+  const double* ke64;   // HEX20 unit element matrix (FP64, then its FP32 copy)
+  const float* ke32;
 };
 
 // y = scale * K u on the interior (ALL = false) or every node; DOT: acc[col] += u . y.
@@ -890,7 +891,10 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
     if (nt > 0)
       k_matvec<T, ALL, DOT><<<(unsigned)(3 * nt), kThreads, 0, s>>>(ALL ? W.ta : W.ti, dd, svox, u, y, scale, acc, act);
   } else {
-    launch_ebe<T, NEN, ALL, DOT>(ALL ? W.ba : W.bi, ALL ? W.nba : W.nbi, dd, svox, fl, u, y, scale, acc, act, s);
+    const T* ke;
+    if constexpr (sizeof(T) == 8) ke = W.ke64;
+    else ke = W.ke32;
+    launch_ebe<T, NEN, ALL, DOT>(ALL ? W.ba : W.bi, ALL ? W.nba : W.nbi, dd, svox, fl, ke, u, y, scale, acc, act, s);
   }
 }
 
@@ -1420,7 +1424,12 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       voxel_stiffness(20, nu, k20.data());
       for (int i = 0; i < 3600; ++i) k20f[i] = (float)k20[i];
       DTC_CUDA(cudaMemcpyToSymbolAsync(c_k20_64, k20.data(), sizeof(double) * 3600, 0, cudaMemcpyHostToDevice, s));
-      DTC_CUDA(cudaMemcpyToSymbolAsync(c_k20_32, k20f.data(), sizeof(float) * 3600, 0, cudaMemcpyHostToDevice, s));
+      // the element kernel stages the matrix from global memory: FP64 then FP32 copy
+      if (int e = ensure(I, bKe20, sizeof(double) * 3600 + sizeof(float) * 3600, msg)) return e;
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20], k20.data(), sizeof(double) * 3600, cudaMemcpyHostToDevice, s));
+      DTC_CUDA(cudaMemcpyAsync(B<double>(I, bKe20) + 3600, k20f.data(), sizeof(float) * 3600, cudaMemcpyHostToDevice,
+                               s));
+      DTC_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
     }
     if constexpr (NEN == 20)
       if (int e = allow_all_ebe<NEN>(msg)) return e;   // per device, cheap
@@ -1580,7 +1589,9 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaEventRecord(I.ev_solve[0], s));
   const Tile* ti = B<Tile>(I, bTilesI);
   const Tile* ta = B<Tile>(I, bTilesA);
-  const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba};
+  const double* ke64 = NEN == 20 ? B<double>(I, bKe20) : nullptr;
+  const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba, ke64,
+               ke64 ? reinterpret_cast<const float*>(ke64 + 3600) : nullptr};
   const DomDev* dd = B<DomDev>(I, bDoms);
   uint8_t* fl = B<uint8_t>(I, bFlags);
   double* X = B<double>(I, bX);
