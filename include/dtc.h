@@ -79,8 +79,8 @@ typedef struct dtc_options {
                               1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy) */
   int32_t inner_precond;   /* preconditioner of the FP32 inner solve: 0 = Jacobi (as PETSc's
                               PCJACOBI), 1 = node-block Jacobi (3x3 diagonal blocks),
-                              2 = geometric multigrid V-cycle on halved voxel grids (HEX08;
-                              HEX20 domains use 1) */
+                              2 = multigrid V-cycle on halved voxel grids (HEX20 domains are
+                              first coarsened to the HEX08 mesh of the same voxels) */
   int32_t tensor_estimator; /* how ff is formed from the solutions: 0 = projection of the
                               reaction forces (the reference, mod_struct_calcmat.f90:254-280),
                               error linear in the solve error; 1 = energy products

@@ -867,6 +867,7 @@ template <int NEN>
 int allow_all_ebe(std::string& msg) {
   int e;
   if ((e = allow_ebe_smem<float, NEN, false, true>(msg))) return e;
+  if ((e = allow_ebe_smem<float, NEN, false, false>(msg))) return e;   // multigrid residual sweeps
   if ((e = allow_ebe_smem<double, NEN, false, true>(msg))) return e;
   if ((e = allow_ebe_smem<double, NEN, false, false>(msg))) return e;
   if ((e = allow_ebe_smem<double, NEN, true, false>(msg))) return e;
@@ -907,7 +908,8 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
 // all tiles (node set-up), and the domains whose coarsest level it is (dense solve).
 struct MgPlan {
   int nlev = 0;
-  float omega = 0.f;
+  float omega = 0.f;                                // damping on the HEX08 levels
+  float omega0 = 0.f;                               // damping on the fine level (HEX08 or HEX20)
   std::vector<DomDev> doms;                         // nlev * ndom, level-major
   std::vector<Tile> tiles;
   std::vector<int64_t> sm_off, sm_n, in_off, in_n, all_off, all_n;
@@ -921,48 +923,49 @@ struct MgPlan {
 // Largest eigenvalue of Khat v = lambda De v, De the node-block (3x3) diagonal of the unit
 // voxel matrix: bounds lambda_max(D^-1 K) of every assembly of scaled voxels, D its node-block
 // diagonal (x^T K x = sum_v x_v^T K_v x_v <= lambda sum_v x_v^T De_v x_v = lambda x^T D x).
-double block_jacobi_bound(const double* kh) {
-  double inv[8][9];
-  for (int a = 0; a < 8; ++a) {
+double block_jacobi_bound(const double* kh, int nen) {
+  const int nd = 3 * nen;
+  std::vector<double> inv((size_t)nen * 9), v(nd), w(nd), kv(nd);
+  for (int a = 0; a < nen; ++a) {
     double m[9];
     for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) m[3 * i + j] = kh[(3 * a + i) + 24 * (3 * a + j)];
+      for (int j = 0; j < 3; ++j) m[3 * i + j] = kh[(3 * a + i) + nd * (3 * a + j)];
     const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[2] * m[7] - m[1] * m[8], c02 = m[1] * m[5] - m[2] * m[4];
     const double det = m[0] * c00 + m[3] * c01 + m[6] * c02;
-    inv[a][0] = c00 / det; inv[a][1] = c01 / det; inv[a][2] = c02 / det;
-    inv[a][3] = (m[5] * m[6] - m[3] * m[8]) / det; inv[a][4] = (m[0] * m[8] - m[2] * m[6]) / det;
-    inv[a][5] = (m[2] * m[3] - m[0] * m[5]) / det;
-    inv[a][6] = (m[3] * m[7] - m[4] * m[6]) / det; inv[a][7] = (m[1] * m[6] - m[0] * m[7]) / det;
-    inv[a][8] = (m[0] * m[4] - m[1] * m[3]) / det;
+    double* q = &inv[(size_t)a * 9];
+    q[0] = c00 / det; q[1] = c01 / det; q[2] = c02 / det;
+    q[3] = (m[5] * m[6] - m[3] * m[8]) / det; q[4] = (m[0] * m[8] - m[2] * m[6]) / det;
+    q[5] = (m[2] * m[3] - m[0] * m[5]) / det;
+    q[6] = (m[3] * m[7] - m[4] * m[6]) / det; q[7] = (m[1] * m[6] - m[0] * m[7]) / det;
+    q[8] = (m[0] * m[4] - m[1] * m[3]) / det;
   }
-  double v[24], w[24], lam = 0;
-  for (int i = 0; i < 24; ++i) v[i] = 1.0 + 0.01 * i;
+  double lam = 0;
+  for (int i = 0; i < nd; ++i) v[i] = 1.0 + 0.01 * i;
   for (int it = 0; it < 3000; ++it) {
-    double kv[24];
-    for (int i = 0; i < 24; ++i) {
+    for (int i = 0; i < nd; ++i) {
       double s = 0;
-      for (int j = 0; j < 24; ++j) s += kh[i + 24 * j] * v[j];
+      for (int j = 0; j < nd; ++j) s += kh[i + nd * j] * v[j];
       kv[i] = s;
     }
     double vkv = 0, vdv = 0;
-    for (int a = 0; a < 8; ++a)
+    for (int a = 0; a < nen; ++a)
       for (int i = 0; i < 3; ++i) {
         double dv = 0;
-        for (int j = 0; j < 3; ++j) dv += kh[(3 * a + i) + 24 * (3 * a + j)] * v[3 * a + j];
+        for (int j = 0; j < 3; ++j) dv += kh[(3 * a + i) + nd * (3 * a + j)] * v[3 * a + j];
         vdv += v[3 * a + i] * dv;
         vkv += v[3 * a + i] * kv[3 * a + i];
       }
     lam = vkv / vdv;
     double nrm = 0;
-    for (int a = 0; a < 8; ++a)
+    for (int a = 0; a < nen; ++a)
       for (int i = 0; i < 3; ++i) {
         double s = 0;
-        for (int j = 0; j < 3; ++j) s += inv[a][3 * i + j] * kv[3 * a + j];
+        for (int j = 0; j < 3; ++j) s += inv[(size_t)a * 9 + 3 * i + j] * kv[3 * a + j];
         w[3 * a + i] = s;
         nrm += s * s;
       }
     nrm = std::sqrt(nrm);
-    for (int i = 0; i < 24; ++i) v[i] = w[i] / nrm;
+    for (int i = 0; i < nd; ++i) v[i] = w[i] / nrm;
   }
   return lam;
 }
@@ -1035,17 +1038,29 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
 
 // Build the hierarchy on the host from the fine voxel factors.  fine_i: interior tiles of the
 // fine level (level-0 smoothing tiles are those of domains with a coarser level).
+// HEX20 fine grids (m = 2) get one p-coarsening first: level 1 is the HEX08 mesh of the same
+// voxels (corner nodes; the trilinear space is contained in the serendipity one, so the
+// exactly integrated HEX08 matrix is the Galerkin product of the HEX20 one), then the voxel
+// grids are halved as for HEX08.
 void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<float>& svox0,
-              const std::vector<Tile>& fine_i, double nu) {
+              const std::vector<Tile>& fine_i, double nu, int nen) {
   const int ndom = (int)doms0.size();
   double kh[576];
   voxel_stiffness(8, nu, kh);
-  const double lam = block_jacobi_bound(kh);
-  P.omega = (float)(1.0 / (0.5 * (1.1 + 1.0 / 30.0) * lam));
+  auto step = [](double lam) { return (float)(1.0 / (0.5 * (1.1 + 1.0 / 30.0) * lam)); };
+  P.omega = step(block_jacobi_bound(kh, 8));
+  if (nen == 20) {
+    std::vector<double> k20(3600);
+    voxel_stiffness(20, nu, k20.data());
+    P.omega0 = step(block_jacobi_bound(k20.data(), 20));
+  } else {
+    P.omega0 = P.omega;
+  }
   std::vector<int> nlev(ndom, 1);
   int nl = 1;
   for (int d = 0; d < ndom; ++d) {
     int L[3] = {doms0[d].L[0], doms0[d].L[1], doms0[d].L[2]};
+    if (doms0[d].m == 2) ++nlev[d];   // the HEX08 level of the same voxels
     while (std::max(L[0], std::max(L[1], L[2])) > kMgMaxCoarse) {
       for (int k = 0; k < 3; ++k) L[k] = (L[k] + 1) / 2;
       ++nlev[d];
@@ -1073,17 +1088,22 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
       if (nlev[d] <= l) continue;
       const DomDev& F = P.doms[(size_t)(l - 1) * ndom + d];
       DomDev C = F;
-      for (int k = 0; k < 3; ++k) { C.L[k] = (F.L[k] + 1) / 2; C.n[k] = C.L[k] + 1; }
+      const bool pc = F.m == 2;   // p-coarsening: same voxels, corner nodes
+      for (int k = 0; k < 3; ++k) { C.L[k] = pc ? F.L[k] : (F.L[k] + 1) / 2; C.n[k] = C.L[k] + 1; }
       C.m = 1;
-      C.scale = 2.0 * F.scale;
+      C.scale = pc ? F.scale : 2.0 * F.scale;
       C.vox_off = (int64_t)P.svox.size();
       C.node_off = P.nodes;
       std::vector<float> nv((size_t)C.L[0] * C.L[1] * C.L[2], 0.f);
-      for (int z = 0; z < F.L[2]; ++z)
-        for (int y = 0; y < F.L[1]; ++y)
-          for (int x = 0; x < F.L[0]; ++x)
-            nv[(x / 2) + (size_t)C.L[0] * ((y / 2) + (size_t)C.L[1] * (z / 2))] +=
-                0.125f * cur[d][x + (size_t)F.L[0] * (y + (size_t)F.L[1] * z)];
+      if (pc) {
+        nv = cur[d];
+      } else {
+        for (int z = 0; z < F.L[2]; ++z)
+          for (int y = 0; y < F.L[1]; ++y)
+            for (int x = 0; x < F.L[0]; ++x)
+              nv[(x / 2) + (size_t)C.L[0] * ((y / 2) + (size_t)C.L[1] * (z / 2))] +=
+                  0.125f * cur[d][x + (size_t)F.L[0] * (y + (size_t)F.L[1] * z)];
+      }
       P.svox.insert(P.svox.end(), nv.begin(), nv.end());
       P.nodes += (int64_t)C.n[0] * C.n[1] * C.n[2];
       P.doms[(size_t)l * ndom + d] = C;
@@ -1151,6 +1171,10 @@ struct MgDev {
   const int* lists;
   float *b, *t, *z;      // levels >= 1
   float *t0, *z0;        // fine level
+  int nen0;              // element of the fine level; HEX20 applies K with the brick kernel
+  const Tile* bricks0;   // fine-level interior bricks (HEX20)
+  int64_t nbricks0;
+  const float* ke32;     // HEX20 unit element matrix (FP32)
 };
 
 void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act,
@@ -1187,10 +1211,17 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   const Tile* tsm = M.tiles + P.sm_off[l];
   const unsigned g = (unsigned)(3 * nsm);
   int q = fine ? I.begin(0) : -1;
-  k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, P.omega, t, act);
+  k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, fine ? P.omega0 : P.omega, t, act);
   if (fine) I.end(kcMgJacobi, q, 2 * vb + vb / 12, 0);   // b in, t out, 6 floats of D^-1 per node
   q = fine ? I.begin(0) : -1;
-  k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+  const float om = fine ? P.omega0 : P.omega;
+  if (fine && M.nen0 == 20) {
+    launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
+    k_mg_combine<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, om, nullptr, nullptr, act);
+    ++launches;
+  } else {
+    k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
+  }
   if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
   ++launches;
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
@@ -1207,8 +1238,12 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, dc, M.z, t, act);
   if (fine) I.end(kcMgTransfer, q, vb * (2.0 + 1.0 / 8.0), 0);
   q = fine ? I.begin(0) : -1;
-  if (l == 0)
-    k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, zz, zr, act);
+  if (l == 0 && M.nen0 == 20) {
+    launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
+    k_mg_combine<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, P.omega0, zz, zr, act);
+    ++launches;
+  } else if (l == 0)
+    k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
   else
     k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
   if (fine) I.end(kcMgPost, q, mb + vb + vb / 12, mf);     // t in, z out (mb), b in, D^-1
@@ -1322,6 +1357,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
 
 // FP32 CG preconditioned by one multigrid V-cycle per iteration (same column state machine
 // and stopping rule as run_cg, with z = B r in place of the Jacobi z).
+template <int NEN>
 int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, float* x, float* r, float* p, float* w,
               double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
   cudaStream_t s = I.stream;
@@ -1357,7 +1393,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
           k_direction_z<<<grid, kThreads, 0, s>>>(ti, dd, fl, M.z0, p, st, act);
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
-          k_matvec<float, false, true><<<grid, kThreads, 0, s>>>(ti, dd, B<float>(I, bSvox), p, w, 1.0, pw, act);
+          apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
           k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, act);
@@ -1623,11 +1659,11 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
     DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
     // multigrid hierarchy (HEX08): built on the host from the voxel factors, set up on the device
-    const bool use_mg = NEN == 8 && opt.inner_precond == 2 && nti > 0;
+    const bool use_mg = opt.inner_precond == 2 && nti > 0;
     MgPlan mgp;
     MgDev mgd{};
     if (use_mg) {
-      build_mg(mgp, doms, svox, tiles_i, nu);
+      build_mg(mgp, doms, svox, tiles_i, nu, NEN);
       const int64_t cn = std::max<int64_t>(mgp.nodes, 1);
       if ((e = ensure(I, bZ32, vbytes32, msg)) || (e = ensure(I, bT32, vbytes32, msg)) ||
           (e = ensure(I, bMgDoms, sizeof(DomDev) * mgp.doms.size(), msg)) ||
@@ -1687,6 +1723,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.z = B<float>(I, bMgZ);
       mgd.t0 = B<float>(I, bT32);
       mgd.z0 = B<float>(I, bZ32);
+      mgd.nen0 = NEN;
+      mgd.bricks0 = W.bi;
+      mgd.nbricks0 = W.nbi;
+      mgd.ke32 = W.ke32;
     }
     // inner FP32 solves aim straight at the outer target when FP32 can reach it
     const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);
@@ -1711,7 +1751,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
       DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
       if (use_mg)
-        e = run_cg_mg(I, ndom, W, mgd, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
+        e = run_cg_mg<NEN>(I, ndom, W, mgd, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
                       inner, B<double>(I, bTarget), inner_budget, L, msg);
       else if (opt.inner_precond >= 1)
         e = run_cg<float, true, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),

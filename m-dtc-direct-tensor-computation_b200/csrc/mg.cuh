@@ -1,4 +1,5 @@
-// mg.cuh -- geometric multigrid V-cycle that preconditions the FP32 inner solve (HEX08).
+// mg.cuh -- multigrid V-cycle that preconditions the FP32 inner solve (HEX08 grids; a HEX20
+// fine level is first coarsened to the HEX08 mesh of the same voxels).
 //
 // Not a step of the reference (its KSP uses PCJACOBI, f-src/mod_dtc_main_subroutines.f90:
 // 995-1078); it only changes how fast the inner FP32 solve of the iterative refinement
@@ -139,6 +140,70 @@ __global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restric
       for (int b2 = 0; b2 < 2; ++b2)
 #pragma unroll
         for (int c2 = 0; c2 < 2; ++c2) sv[0][b2][c2] = sv[1][b2][c2];
+    }
+  }
+  if (DOT) {
+    const int64_t col = (int64_t)t.dom * kNLC + lc;
+    const double s1 = block_sum_lc<double>(szz, red);
+    __syncthreads();
+    const double s2 = block_sum_lc<double>(szr, red);
+    if (threadIdx.x < 8) {
+      atomicAdd(acc_zz + col, s1);
+      atomicAdd(acc_zr + col, s2);
+    }
+  }
+}
+
+// Node-local second half of the residual / smoother when K t was applied by the brick kernel
+// (HEX20 fine level), z holding -K t on entry:
+//   kMgRes : z = b + z
+//   kMgPost: z = t + omega D^-1 (b + z);  DOT: zz += z.z, zr += z.b
+template <int MODE, bool DOT>
+__global__ void __launch_bounds__(kThreads) k_mg_combine(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+                                                         const uint8_t* __restrict__ flags,
+                                                         const float* __restrict__ binv, const float* __restrict__ b,
+                                                         const float* __restrict__ t_in, float* __restrict__ z,
+                                                         float omega, double* __restrict__ acc_zz,
+                                                         double* __restrict__ acc_zr,
+                                                         const int* __restrict__ dom_active) {
+  __shared__ double red[32];
+  const Tile t = tiles[blockIdx.x / 3];
+  if (dom_active && !dom_active[t.dom]) return;
+  const DomDev D = doms[t.dom];
+  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
+  const int row = threadIdx.x >> 3;
+  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
+  double szz = 0.0, szr = 0.0;
+  if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
+    for (int i = 0; i < kTileX; ++i) {
+      const int x = t.x0 + i;
+      if (x > D.n[0] - 2) break;
+      const int64_t n = node_index(D, x, yy, zz);
+      if (!(flags[n] & kNodeActive)) continue;
+      const int64_t k0 = vec_index(n, 0, lc);
+      float bc[3], res[3], v[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        bc[c] = b[k0 + c * kNLC];
+        res[c] = bc[c] + z[k0 + c * kNLC];
+      }
+      if (MODE == kMgRes) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = res[c];
+      } else {
+        float dz[3];
+        block_jacobi(binv, n, omega, res, dz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = t_in[k0 + c * kNLC] + dz[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        z[k0 + c * kNLC] = v[c];
+        if (DOT) {
+          szz += (double)v[c] * (double)v[c];
+          szr += (double)v[c] * (double)bc[c];
+        }
+      }
     }
   }
   if (DOT) {

@@ -158,7 +158,7 @@ def test_hex20_fp64_matches_oracle(dtc, batch20):
         assert np.abs(r["iters"] - ref["iters"]).max() <= 2
 
 
-@pytest.mark.parametrize("precond", ["block", "jacobi"])
+@pytest.mark.parametrize("precond", ["block", "jacobi", "mg"])
 def test_hex20_mixed_matches_oracle(dtc, batch20, precond):
     pairs, refs = batch20
     with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, inner_precond=precond) as s:
@@ -244,3 +244,21 @@ def test_graph_replay_matches_direct_launches(dtc, batch, precision, precond, to
     for a, b in zip(out[True], out[False]):
         assert rel(a["c"], b["c"]) <= tol
         assert np.abs(a["iters"] - b["iters"]).max() <= 2
+
+
+def test_hex20_multigrid_cuts_inner_iterations(dtc):
+    """p-multigrid (HEX20 -> HEX08 of the same voxels -> halved grids) on a 16^3 HEX20 domain."""
+    syn = dtc.synth
+    gray = syn.bone_volume((16, 16, 16), 0.3, syn.seed_for(20, 30))
+    dom = dtc.Domain(gray, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA,
+                     E_voxel=syn.modulus_of_gray(gray))
+    out = {}
+    for pc in ("block", "mg"):
+        with dtc.Solver(precision="mixed", rtol=1e-6, rotation_search=False, inner_precond=pc) as s:
+            out[pc] = s.solve([dom])[0]
+    with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False) as s:
+        ref = s.solve([dom])[0]
+    for pc in ("block", "mg"):
+        assert out[pc]["status"] == 0
+        assert rel(out[pc]["c"], ref["c"]) <= TOL_MIXED
+    assert out["mg"]["iters"].max() * 4 < out["block"]["iters"].max()
