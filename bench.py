@@ -36,7 +36,8 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--ndom", type=int, default=512)
+    p.add_argument("--ndom", type=int, default=None,
+                   help="domains per GPU (default: 512; c2 256, c3 2000, c4 64)")
     p.add_argument("--L", type=int, default=32)
     p.add_argument("--rtol", type=float, default=0.0, help="0: calibrate per arm to the accuracy target")
     p.add_argument("--estimator", default="energy", choices=["energy", "reaction"])
@@ -48,9 +49,13 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     p.add_argument("--profile-step", action="store_true",
                    help="one warm-up and one timed-free mixed solve only (for ncu captures)")
+    p.add_argument("--elem", type=int, default=8, choices=[8, 20], help="element type of --profile-step")
     p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4"],
                    help="c1 (default): the headline line; c0/c2/c3/c4 print their own measurement lines")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.ndom is None:
+        a.ndom = {"c2": 256, "c3": 2000, "c4": 64}.get(a.config, 512)
+    return a
 
 
 def workload(args):
@@ -223,12 +228,12 @@ def run_config(args, dtc):
         orc.solve_batch(odoms, nthreads=cores)
         tcpu = time.perf_counter() - t0
         line.update({"workload": "27 HEX08 domains of 20^3 from a 62^3 volume (BV/TV 0.25), FP64 rtol 1e-10, "
-                                 "rotation search", "gpu_ms_device": dev, "gpu_ms_wall": wall,
+                                 "rotation search", "gpu_ms_device": dev, "gpu_ms_wall": 1e3 * wall,
                      "gpu_domains_per_s_wall": len(doms) / wall,
                      "cpu_oracle_s": tcpu, "cpu_cores": cores, "cpu_domains_per_s": len(doms) / tcpu})
     elif args.config == "c2":
         # 256 HEX20 domains of 24^3, BV/TV 0.25, mixed vs plain FP64
-        n = min(args.ndom, 256)
+        n = args.ndom
         grays = [syn.bone_volume((24, 24, 24), 0.25, syn.seed_for(2, i)) for i in range(n)]
         doms = [dtc.Domain(g, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA,
                            E_voxel=syn.modulus_of_gray(g)) for g in grays]
@@ -236,10 +241,16 @@ def run_config(args, dtc):
         with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device=local) as ref:
             truth = ref.solve(sample)
         out = {}
-        for arm, kw, rt in (("mixed", dict(precision="mixed", estimator="energy", inner_precond="block"), 3e-6),
-                            ("fp64", dict(precision="fp64"), 3e-7)):
+        ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8]
+        for arm, kw in (("mixed", dict(precision="mixed", estimator="energy", inner_precond="mg")),
+                        ("fp64", dict(precision="fp64"))):
+            # loosest rtol whose tensors stay within TARGET/2 of FP64 at 1e-10 on the sample
+            for rt in ladder:
+                with dtc.Solver(rtol=rt, rotation_search=False, device=local, **kw) as sv:
+                    err = _err(sv.solve(sample), truth)
+                if err <= 0.5 * TARGET:
+                    break
             with dtc.Solver(rtol=rt, rotation_search=False, device=local, **kw) as sv:
-                err = _err(sv.solve(sample), truth)
 
                 def step():
                     sv.solve(doms)
@@ -253,7 +264,7 @@ def run_config(args, dtc):
     elif args.config == "c3":
         # 2000 HEX08 domains, L ~ U{16,24,32,48,64}, BV/TV ~ U(0.05,0.45), mixed + MG, CUDA graphs,
         # rotation search in the step
-        n = min(args.ndom, 2000)
+        n = args.ndom
         rng = np.random.default_rng(syn.seed_for(3, 10_000))
         Ls = rng.choice([16, 24, 32, 48, 64], size=n)
         bv = rng.uniform(0.05, 0.45, size=n)
@@ -275,12 +286,12 @@ def run_config(args, dtc):
         line.update({"workload": f"{n} HEX08 domains, L in {{16,24,32,48,64}}, BV/TV U(0.05,0.45), mixed+MG, "
                                  "CUDA-graph CG chunks, rotation search",
                      "domains_per_s_device": n / (dev / 1e3), "domains_per_s_wall": n / wall, "ms_device": dev,
-                     "ms_wall": wall, "domains_solved": ok,
+                     "ms_wall": 1e3 * wall, "domains_solved": ok,
                      "max_rel_err_vs_fp64_1e-10": _err([res[i] for i in sample], truth),
                      "voxels": int(sum(int(L) ** 3 for L in Ls))})
     elif args.config == "c4":
         # adjoint: 64 HEX08 domains of 48^3, loss ||C - C_target||_F^2, gradient vs one forward solve
-        n = min(args.ndom, 64)
+        n = args.ndom
         grays = [syn.bone_volume((48, 48, 48), 0.25, syn.seed_for(4, i)) for i in range(n)]
         E = [syn.modulus_of_gray(g) for g in grays]
         doms = [dtc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=e) for g, e in zip(grays, E)]
@@ -340,13 +351,16 @@ def main():
         # one warm-up solve, then one solve of the mixed arm at --rtol (for ncu launch lists:
         # skip the first launches_per_solve launches)
         rt = args.rtol if args.rtol > 0 else 3e-5
+        if args.elem == 20:
+            doms = [dtc.Domain(g, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA,
+                               E_voxel=syn.modulus_of_gray(g)) for g in grays]
         with dtc.Solver(precision="mixed", rtol=rt, max_it=args.max_it, rotation_search=False, device=local,
                         estimator=args.estimator, inner_precond=args.precond) as sv:
             sv.solve(doms)
             n0 = sv.stats()["kernel_launches"]
             sv.solve(doms)
             torch.cuda.synchronize()
-            print(json.dumps({"profile_step": True, "ndom": args.ndom, "L": args.L, "rtol": rt,
+            print(json.dumps({"profile_step": True, "ndom": args.ndom, "L": args.L, "elem": args.elem, "rtol": rt,
                               "inner_precond": args.precond, "launches_per_solve": n0,
                               "launches_second": sv.stats()["kernel_launches"]}))
         return
