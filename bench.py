@@ -28,6 +28,12 @@ TARGET = 1e-5
 # rtol at which the reference algorithm (reaction projection, FP64) meets TARGET on this
 # workload, as calibrated on the GPU; the host-only reference arm cannot calibrate itself
 REF_RTOL = 1e-7
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the fine
+# sweeps, measured on 16 domains of 32^3 (profiles/k_matvec_k_mg_matvec_f32_16x32cubed.md)
+DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 0.96, "mg_residual_f32": 1.53}
+# FP32 SIMT FMA peak, nominal: 148 SMs x 128 lanes x 2 flop x 1.965 GHz (the sweeps run on the
+# FMA pipe, not on tensor cores; the measured peaks cover HBM and bf16 tensor only)
+FP32_NOMINAL_TFLOPS = 74.4
 
 
 def parse():
@@ -437,10 +443,12 @@ def main():
                     inner_precond=args.precond) as prof:
         prof.solve(doms)
         ks = prof.kernel_stats()
-    top = max(ks, key=lambda k: ks[k]["ms_total"])
+    top = max((k for k in ks if ks[k]["bytes_per_launch"] > 0), key=lambda k: ks[k]["ms_total"])
     kt = ks[top]
     t_launch = kt["ms_total"] / kt["launches"] / 1e3
     achieved = kt["bytes_per_launch"] / t_launch / 1e9
+    ratio = DRAM_PER_ALGORITHMIC_BYTE.get(top)
+    traffic = kt["bytes_per_launch"] * ratio if ratio else None
     share = {k: round(v["ms_total"] / sum(x["ms_total"] for x in ks.values()), 4) for k, v in ks.items()}
     cpu = cpu_baseline(args, dtc, grays, rtol_of["fp64"]) if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:
@@ -453,10 +461,14 @@ def main():
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None, "peak_source": src,
+                             "frac": achieved / peak, "traffic": traffic, "peak_source": src,
+                             "traffic_source": (f"ncu dram bytes / algorithmic bytes = {ratio} on the 16x32^3 case "
+                                                "(profiles/k_matvec_k_mg_matvec_f32_16x32cubed.md), scaled to this "
+                                                "launch" if ratio else None),
                              "kernel": top, "avg_launch_us": t_launch * 1e6,
                              "flops_per_launch": kt["flops_per_launch"],
                              "achieved_tflops": kt["flops_per_launch"] / t_launch / 1e12,
+                             "fp32_fma_frac_of_nominal": kt["flops_per_launch"] / t_launch / 1e12 / FP32_NOMINAL_TFLOPS,
                              "kernel_time_share": share},
                 "cpu_baseline": cpu,
                 "gpu_launches": st["kernel_launches"], "clocks": clk,
