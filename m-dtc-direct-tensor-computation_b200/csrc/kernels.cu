@@ -41,42 +41,56 @@ template <> struct KhatC<double> {
 };
 
 // -------------------------------------------------------------------------------------
-// HEX08: matrix-free K*u on one node tile (the default SIMT operator of the corner grid).  Window w[px][py][pz][c] holds u at x-1+px, y-1+py, z-1+pz;
-// sv[a][b][c] the scale of voxel (x-1+a, y-1+b, z-1+c).
-template <typename T>
-__device__ __forceinline__ void apply_node(const T (&w)[3][3][3][3], const float (&sv)[2][2][2], T (&acc)[3]) {
+// HEX08: matrix-free K*u on one node tile (the default SIMT operator of the corner grid).
+// A thread owns one (y, z) row of the tile for one load case and sweeps x.  Between node
+// planes x and x+1 lie the 4 voxels (x, y-1..y, z-1..z) of the row; each kept voxel
+// contributes s_v * Khat[rows of its corner, :] * u_v to node x (corner with offset 0 in x)
+// and to node x+1 (offset 1), both from one read of its 8 corner values held in the two
+// plane registers P0 (plane x) and P1 (plane x+1).  FIRST: the slab left of the tile, whose
+// contribution to the first node only is needed.
+template <typename T, bool FIRST>
+__device__ __forceinline__ void slab(const T (&P0)[3][3][3], const T (&P1)[3][3][3], const float (&sv)[2][2],
+                                     T (&cur)[3], T (&nxt)[3]) {
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int b = 0; b < 2; ++b)
 #pragma unroll
-    for (int b = 0; b < 2; ++b)
+    for (int c = 0; c < 2; ++c) {
+      const float s = sv[b][c];
+      if (s != 0.0f) {
+        const int l0 = corner_local(0, 1 - b, 1 - c), l1 = corner_local(1, 1 - b, 1 - c);
+        T t0 = 0, t1 = 0, t2 = 0, q0 = 0, q1 = 0, q2 = 0;
 #pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const float s = sv[a][b][c];
-        if (s != 0.0f) {
-          const int ln = corner_local(1 - a, 1 - b, 1 - c);
-          T t0 = 0, t1 = 0, t2 = 0;
+        for (int mz = 0; mz < 2; ++mz)
 #pragma unroll
-          for (int mz = 0; mz < 2; ++mz)
+          for (int my = 0; my < 2; ++my)
 #pragma unroll
-            for (int my = 0; my < 2; ++my)
+            for (int mx = 0; mx < 2; ++mx) {
+              const int lm = corner_local(mx, my, mz);
 #pragma unroll
-              for (int mx = 0; mx < 2; ++mx) {
-                const int lm = corner_local(mx, my, mz);
-#pragma unroll
-                for (int cj = 0; cj < 3; ++cj) {
-                  const T v = w[a + mx][b + my][c + mz][cj];
-                  const int col = 24 * (3 * lm + cj);
-                  t0 = fma(KhatC<T>::at(col + 3 * ln + 0), v, t0);
-                  t1 = fma(KhatC<T>::at(col + 3 * ln + 1), v, t1);
-                  t2 = fma(KhatC<T>::at(col + 3 * ln + 2), v, t2);
+              for (int cj = 0; cj < 3; ++cj) {
+                const T v = mx ? P1[b + my][c + mz][cj] : P0[b + my][c + mz][cj];
+                const int col = 24 * (3 * lm + cj);
+                if (!FIRST) {
+                  t0 = fma(KhatC<T>::at(col + 3 * l0 + 0), v, t0);
+                  t1 = fma(KhatC<T>::at(col + 3 * l0 + 1), v, t1);
+                  t2 = fma(KhatC<T>::at(col + 3 * l0 + 2), v, t2);
                 }
+                q0 = fma(KhatC<T>::at(col + 3 * l1 + 0), v, q0);
+                q1 = fma(KhatC<T>::at(col + 3 * l1 + 1), v, q1);
+                q2 = fma(KhatC<T>::at(col + 3 * l1 + 2), v, q2);
               }
-          const T ts = (T)s;
-          acc[0] = fma(ts, t0, acc[0]);
-          acc[1] = fma(ts, t1, acc[1]);
-          acc[2] = fma(ts, t2, acc[2]);
+            }
+        const T ts = (T)s;
+        if (!FIRST) {
+          cur[0] = fma(ts, t0, cur[0]);
+          cur[1] = fma(ts, t1, cur[1]);
+          cur[2] = fma(ts, t2, cur[2]);
         }
+        nxt[0] = fma(ts, q0, nxt[0]);
+        nxt[1] = fma(ts, q1, nxt[1]);
+        nxt[2] = fma(ts, q2, nxt[2]);
       }
+    }
 }
 
 template <typename T, bool GUARD>
@@ -113,7 +127,7 @@ __device__ __forceinline__ void load_voxels(float (&sp)[2][2], const float* __re
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
 // node of the grid (reaction forces).
-// FP32: capped at 128 registers (4 CTAs per SM) -- a few spills, ~5% faster than 155 registers
+// FP32: at most 128 registers (4 CTAs of 128 threads per SM)
 template <typename T, bool ALL, bool DOT>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_matvec(const Tile* __restrict__ tiles,
                                                                           const DomDev* __restrict__ doms,
@@ -131,43 +145,40 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_matvec(con
   const int xhi = ALL ? D.n[0] - 1 : D.n[0] - 2, yhi = ALL ? D.n[1] - 1 : D.n[1] - 2, zhi = ALL ? D.n[2] - 1 : D.n[2] - 2;
   double dot = 0.0;
   if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi) {
-    T w[3][3][3][3];
-    float sv[2][2][2];
-    load_plane<T, ALL>(w[0], u, D, t.x0 - 1, yy, zz, lc);
-    load_plane<T, ALL>(w[1], u, D, t.x0, yy, zz, lc);
-    load_voxels<ALL>(sv[0], svox, D, t.x0 - 1, yy, zz);
+    T P0[3][3][3], P1[3][3][3];
+    float sv[2][2];
+    T cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
+    load_plane<T, ALL>(P0, u, D, t.x0 - 1, yy, zz, lc);
+    load_plane<T, ALL>(P1, u, D, t.x0, yy, zz, lc);
+    load_voxels<ALL>(sv, svox, D, t.x0 - 1, yy, zz);
+    bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
+    slab<T, true>(P0, P1, sv, cur, nxt);
 #pragma unroll 1
     for (int i = 0; i < kTileX; ++i) {
       const int x = t.x0 + i;
       if (x > xhi) break;
-      load_plane<T, ALL>(w[2], u, D, x + 1, yy, zz, lc);
-      load_voxels<ALL>(sv[1], svox, D, x, yy, zz);
-      const bool any = (sv[0][0][0] != 0.f) | (sv[0][0][1] != 0.f) | (sv[0][1][0] != 0.f) | (sv[0][1][1] != 0.f) |
-                       (sv[1][0][0] != 0.f) | (sv[1][0][1] != 0.f) | (sv[1][1][0] != 0.f) | (sv[1][1][1] != 0.f);
-      if (any) {
-        T a3[3] = {0, 0, 0};
-        apply_node<T>(w, sv, a3);
-        const int64_t b = vec_index(node_index(D, x, yy, zz), 0, lc);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T v = (T)(scale * D.scale * (double)a3[c]);
-          y[b + c * kNLC] = v;
-          if (DOT) dot += (double)w[1][1][1][c] * (double)v;
-        }
-      }
 #pragma unroll
       for (int py = 0; py < 3; ++py)
 #pragma unroll
         for (int pz = 0; pz < 3; ++pz)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            w[0][py][pz][c] = w[1][py][pz][c];
-            w[1][py][pz][c] = w[2][py][pz][c];
-          }
+          for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
+      load_plane<T, ALL>(P1, u, D, x + 1, yy, zz, lc);
+      load_voxels<ALL>(sv, svox, D, x, yy, zz);
+      const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
-      for (int b2 = 0; b2 < 2; ++b2)
+      for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = T(0); }
+      slab<T, false>(P0, P1, sv, cur, nxt);
+      if (anyp | anyc) {
+        const int64_t b = vec_index(node_index(D, x, yy, zz), 0, lc);
 #pragma unroll
-        for (int c2 = 0; c2 < 2; ++c2) sv[0][b2][c2] = sv[1][b2][c2];
+        for (int c = 0; c < 3; ++c) {
+          const T v = (T)(scale * D.scale * (double)cur[c]);
+          y[b + c * kNLC] = v;
+          if (DOT) dot += (double)P0[1][1][c] * (double)v;
+        }
+      }
+      anyp = anyc;
     }
   }
   if (DOT) {

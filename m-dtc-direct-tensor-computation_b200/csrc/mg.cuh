@@ -66,7 +66,7 @@ __device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __
       sp[b][c] = __ldg(svox + D.vox_off + vx + (int64_t)D.L[0] * ((y - 1 + b) + (int64_t)D.L[1] * (z - 1 + c)));
 }
 
-// Residual / smoother on one level's interior tiles (same sweep as k_matvec).
+// Residual / smoother on one level's interior tiles (the slab sweep of k_matvec).
 //   kMgRes : y = b - K u
 //   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
 template <int MODE, bool DOT>
@@ -85,29 +85,38 @@ __global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restric
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   double szz = 0.0, szr = 0.0;
   if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
-    float w[3][3][3][3];
-    float sv[2][2][2];
-    load_plane_f(w[0], u, D, t.x0 - 1, yy, zz, lc);
-    load_plane_f(w[1], u, D, t.x0, yy, zz, lc);
-    load_voxels_f(sv[0], svox, D, t.x0 - 1, yy, zz);
+    float P0[3][3][3], P1[3][3][3];
+    float sv[2][2];
+    float cur[3] = {0.f, 0.f, 0.f}, nxt[3] = {0.f, 0.f, 0.f};
+    load_plane_f(P0, u, D, t.x0 - 1, yy, zz, lc);
+    load_plane_f(P1, u, D, t.x0, yy, zz, lc);
+    load_voxels_f(sv, svox, D, t.x0 - 1, yy, zz);
+    bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
+    slab<float, true>(P0, P1, sv, cur, nxt);
 #pragma unroll 1
     for (int i = 0; i < kTileX; ++i) {
       const int x = t.x0 + i;
       if (x > D.n[0] - 2) break;
-      load_plane_f(w[2], u, D, x + 1, yy, zz, lc);
-      load_voxels_f(sv[1], svox, D, x, yy, zz);
-      const bool any = (sv[0][0][0] != 0.f) | (sv[0][0][1] != 0.f) | (sv[0][1][0] != 0.f) | (sv[0][1][1] != 0.f) |
-                       (sv[1][0][0] != 0.f) | (sv[1][0][1] != 0.f) | (sv[1][1][0] != 0.f) | (sv[1][1][1] != 0.f);
-      if (any) {
-        float a3[3] = {0.f, 0.f, 0.f};
-        apply_node<float>(w, sv, a3);
+#pragma unroll
+      for (int py = 0; py < 3; ++py)
+#pragma unroll
+        for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
+      load_plane_f(P1, u, D, x + 1, yy, zz, lc);
+      load_voxels_f(sv, svox, D, x, yy, zz);
+      const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = 0.f; }
+      slab<float, false>(P0, P1, sv, cur, nxt);
+      if (anyp | anyc) {
         const int64_t n = node_index(D, x, yy, zz);
         const int64_t k0 = vec_index(n, 0, lc);
         float res[3], bc[3], v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           bc[c] = b[k0 + c * kNLC];
-          res[c] = bc[c] - (float)(D.scale * (double)a3[c]);
+          res[c] = bc[c] - (float)(D.scale * (double)cur[c]);
         }
         if (MODE == kMgRes) {
 #pragma unroll
@@ -116,7 +125,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restric
           float dz[3];
           block_jacobi(binv, n, omega, res, dz);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) v[c] = w[1][1][1][c] + dz[c];
+          for (int c = 0; c < 3; ++c) v[c] = P0[1][1][c] + dz[c];
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -127,19 +136,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restric
           }
         }
       }
-#pragma unroll
-      for (int py = 0; py < 3; ++py)
-#pragma unroll
-        for (int pz = 0; pz < 3; ++pz)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            w[0][py][pz][c] = w[1][py][pz][c];
-            w[1][py][pz][c] = w[2][py][pz][c];
-          }
-#pragma unroll
-      for (int b2 = 0; b2 < 2; ++b2)
-#pragma unroll
-        for (int c2 = 0; c2 < 2; ++c2) sv[0][b2][c2] = sv[1][b2][c2];
+      anyp = anyc;
     }
   }
   if (DOT) {
