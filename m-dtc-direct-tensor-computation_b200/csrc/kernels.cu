@@ -1188,8 +1188,9 @@ struct MgDev {
   const float* ke32;     // HEX20 unit element matrix (FP32)
 };
 
+// t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_xr)
 void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act,
-               int64_t& launches) {
+               int64_t& launches, bool t_ready = false) {
   cudaStream_t s = I.stream;
   const MgPlan& P = *M.P;
   const DomDev* dl = l == 0 ? M.doms0 : M.doms + (size_t)l * M.ndom;
@@ -1221,9 +1222,13 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   }
   const Tile* tsm = M.tiles + P.sm_off[l];
   const unsigned g = (unsigned)(3 * nsm);
-  int q = fine ? I.begin(0) : -1;
-  k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, fine ? P.omega0 : P.omega, t, act);
-  if (fine) I.end(kcMgJacobi, q, 2 * vb + vb / 12, 0);   // b in, t out, 6 floats of D^-1 per node
+  int q = -1;
+  if (!(fine && t_ready)) {
+    q = fine ? I.begin(0) : -1;
+    k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, fine ? P.omega0 : P.omega, t, act);
+    if (fine) I.end(kcMgJacobi, q, 2 * vb + vb / 12, 0);   // b in, t out, 6 floats of D^-1 per node
+    ++launches;
+  }
   q = fine ? I.begin(0) : -1;
   const float om = fine ? P.omega0 : P.omega;
   if (fine && M.nen0 == 20) {
@@ -1234,7 +1239,6 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
     k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
   }
   if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
-  ++launches;
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
   q = fine ? I.begin(0) : -1;
   if (P.in_n[l + 1] > 0)
@@ -1407,9 +1411,9 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
           apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
-          k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, act);
-          I.end(kcUpdate32, q, 6 * vb, 0);
-          mg_vcycle(I, M, 0, r, zz, zr, act, nl);
+          k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, M.binv0, M.P->omega0, M.t0, act);
+          I.end(kcUpdate32, q, 7 * vb + vb / 12, 0);
+          mg_vcycle(I, M, 0, r, zz, zr, act, nl, true);
           nl += 3;
         }
         const int q = I.begin(0);
