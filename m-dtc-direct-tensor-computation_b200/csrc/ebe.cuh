@@ -115,29 +115,39 @@ __global__ void __launch_bounds__(128) k_ebe(const Tile* __restrict__ tiles, con
   const int nv = nv_sh;
   const int lo = ALL ? 0 : 1;
   const int hx = ALL ? D.n[0] - 1 : D.n[0] - 2, hy = ALL ? D.n[1] - 1 : D.n[1] - 2, hz = ALL ? D.n[2] - 1 : D.n[2] - 2;
-  for (int it = tid; it < nv * LCG; it += NT) {
-    const int vi = it / LCG, l = it % LCG;
+  // work item = (kept voxel, LCT load cases, 1/SPLIT of the output nodes): every element-matrix
+  // row read from shared memory feeds LCT load cases, and there are enough items for the
+  // 128 threads even on bricks with few kept voxels
+  constexpr int LCT = sizeof(T) == 4 ? 2 : 1, SPLIT = 4, MPER = NEN / SPLIT, NLT = LCG / LCT;
+  for (int it = tid; it < nv * NLT * SPLIT; it += NT) {
+    const int vi = it / (NLT * SPLIT), l0 = (it % NLT) * LCT, m0 = ((it / NLT) % SPLIT) * MPER;
     const int q = vlist[vi];
     const T s = (T)vsc[vi];
     const int qx = q % (E::BX + 1), qy = (q / (E::BX + 1)) % (E::BY + 1), qz = q / ((E::BX + 1) * (E::BY + 1));
     // local input coordinates of the voxel's origin node; fine coordinates of the voxel
     const int bx = M * qx, by = M * qy, bz = M * qz;
     const int fx = ix0 + bx, fy = iy0 + by, fz = iz0 + bz;
-    T uv[ND];
+    T uv[ND][LCT];
 #pragma unroll
     for (int a = 0; a < NEN; ++a) {
       const int nl = (bx + E::off(a, 0)) + S::IX * ((by + E::off(a, 1)) + S::IY * (bz + E::off(a, 2)));
 #pragma unroll
-      for (int c = 0; c < 3; ++c) uv[3 * a + c] = sin[(nl * 3 + c) * LCG + l];
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < LCT; ++j) uv[3 * a + c][j] = sin[(nl * 3 + c) * LCG + l0 + j];
     }
 #pragma unroll 1
-    for (int m = 0; m < NEN; ++m) {
+    for (int m = m0; m < m0 + MPER; ++m) {
       const int ox = fx + E::off(m, 0), oy = fy + E::off(m, 1), oz = fz + E::off(m, 2);
       const int lx = ox - M * t.x0, ly = oy - M * t.y0, lz = oz - M * t.z0;
       const bool own = lx >= 0 && lx < S::OX && ly >= 0 && ly < S::OY && lz >= 0 && lz < S::OZ && ox >= lo &&
                        ox <= hx && oy >= lo && oy <= hy && oz >= lo && oz <= hz;
       if (!own) continue;
-      T r[3] = {T(0), T(0), T(0)};
+      T r[3][LCT];
+#pragma unroll
+      for (int ci = 0; ci < 3; ++ci)
+#pragma unroll
+        for (int j = 0; j < LCT; ++j) r[ci][j] = T(0);
       const T* krow = ske + (3 * m) * ND;
 #pragma unroll
       for (int k = 0; k < ND; k += 4) {
@@ -146,12 +156,16 @@ __global__ void __launch_bounds__(128) k_ebe(const Tile* __restrict__ tiles, con
           T kv[4];
           ke_quad(krow + ci * ND + k, kv);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) r[ci] = fma(kv[j], uv[k + j], r[ci]);
+          for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+            for (int j = 0; j < LCT; ++j) r[ci][j] = fma(kv[jj], uv[k + jj][j], r[ci][j]);
         }
       }
       const int on = lx + S::OX * (ly + S::OY * lz);
 #pragma unroll
-      for (int ci = 0; ci < 3; ++ci) atomicAdd(&sacc[(on * 3 + ci) * LCG + l], s * r[ci]);
+      for (int ci = 0; ci < 3; ++ci)
+#pragma unroll
+        for (int j = 0; j < LCT; ++j) atomicAdd(&sacc[(on * 3 + ci) * LCG + l0 + j], s * r[ci][j]);
     }
   }
   __syncthreads();
