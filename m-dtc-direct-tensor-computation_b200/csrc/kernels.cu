@@ -806,7 +806,7 @@ namespace {
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
-           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bNumBufs };
+           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -854,6 +854,12 @@ void launch_matvec_tc(const Tile* tiles, int64_t ntiles, const DomDev* doms, con
                       const uint8_t* flags, const float* u, float* y, double* acc_pw, const int* dom_active, int* err,
                       cudaStream_t s);
 int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg);
+void build_tc20_operand(const double* k20, float* img);
+size_t tc20_operand_bytes();
+int allow_ebe_tc(std::string& msg);
+void launch_ebe_tc(const Tile* bricks, int64_t nb, const DomDev* doms, const float* svox, const uint8_t* flags,
+                   const float* bsplit, const float* u, float* y, double scale, double* acc_pw, const int* dom_active,
+                   int* err, cudaStream_t s);
 
 namespace {
 
@@ -892,6 +898,8 @@ struct Work {
   int64_t nti, nta, nbi, nba;
   const double* ke64;   // HEX20 unit element matrix (FP64, then its FP32 copy)
   const float* ke32;
+  const float* ke20tc;  // HEX20 FP32 applications on tcgen05: split matrix in the B layout, else null
+  int* err;             // mbarrier time-out flag of the tensor-core kernels
 };
 
 // y = scale * K u on the interior (ALL = false) or every node; DOT: acc[col] += u . y.
@@ -906,6 +914,12 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
     const T* ke;
     if constexpr (sizeof(T) == 8) ke = W.ke64;
     else ke = W.ke32;
+    if constexpr (sizeof(T) == 4 && !ALL) {
+      if (W.ke20tc) {
+        launch_ebe_tc(W.bi, W.nbi, dd, svox, fl, W.ke20tc, u, y, scale, DOT ? acc : nullptr, act, W.err, s);
+        return;
+      }
+    }
     launch_ebe<T, NEN, ALL, DOT>(ALL ? W.ba : W.bi, ALL ? W.nba : W.nbi, dd, svox, fl, ke, u, y, scale, acc, act, s);
   }
 }
@@ -1186,6 +1200,8 @@ struct MgDev {
   const Tile* bricks0;   // fine-level interior bricks (HEX20)
   int64_t nbricks0;
   const float* ke32;     // HEX20 unit element matrix (FP32)
+  const float* ke20tc;   // its tensor-core operand, or null (brick SIMT kernel)
+  int* err;
 };
 
 // t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_xr)
@@ -1232,7 +1248,10 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   q = fine ? I.begin(0) : -1;
   const float om = fine ? P.omega0 : P.omega;
   if (fine && M.nen0 == 20) {
-    launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
+    if (M.ke20tc)
+      launch_ebe_tc(M.bricks0, M.nbricks0, dl, sv, fl, M.ke20tc, t, z, -1.0, nullptr, act, M.err, s);
+    else
+      launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
     k_mg_combine<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, om, nullptr, nullptr, act);
     ++launches;
   } else {
@@ -1254,7 +1273,10 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   if (fine) I.end(kcMgTransfer, q, vb * (2.0 + 1.0 / 8.0), 0);
   q = fine ? I.begin(0) : -1;
   if (l == 0 && M.nen0 == 20) {
-    launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
+    if (M.ke20tc)
+      launch_ebe_tc(M.bricks0, M.nbricks0, dl, sv, fl, M.ke20tc, t, z, -1.0, nullptr, act, M.err, s);
+    else
+      launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
     k_mg_combine<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, P.omega0, zz, zr, act);
     ++launches;
   } else if (l == 0)
@@ -1480,6 +1502,13 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20], k20.data(), sizeof(double) * 3600, cudaMemcpyHostToDevice, s));
       DTC_CUDA(cudaMemcpyAsync(B<double>(I, bKe20) + 3600, k20f.data(), sizeof(float) * 3600, cudaMemcpyHostToDevice,
                                s));
+      if (I.tensor_matvec) {   // HEX20 FP32 applications on the tensor cores
+        std::vector<float> img(tc20_operand_bytes() / sizeof(float));
+        build_tc20_operand(k20.data(), img.data());
+        if (int e = ensure(I, bKe20tc, tc20_operand_bytes(), msg)) return e;
+        DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20tc], img.data(), tc20_operand_bytes(), cudaMemcpyHostToDevice, s));
+        if (int e = allow_ebe_tc(msg)) return e;
+      }
       DTC_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
     }
     if constexpr (NEN == 20)
@@ -1641,8 +1670,9 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   const Tile* ti = B<Tile>(I, bTilesI);
   const Tile* ta = B<Tile>(I, bTilesA);
   const double* ke64 = NEN == 20 ? B<double>(I, bKe20) : nullptr;
+  const float* ke20tc = (NEN == 20 && I.tensor_matvec) ? B<float>(I, bKe20tc) : nullptr;
   const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba, ke64,
-               ke64 ? reinterpret_cast<const float*>(ke64 + 3600) : nullptr};
+               ke64 ? reinterpret_cast<const float*>(ke64 + 3600) : nullptr, ke20tc, B<int>(I, bErr)};
   const DomDev* dd = B<DomDev>(I, bDoms);
   uint8_t* fl = B<uint8_t>(I, bFlags);
   double* X = B<double>(I, bX);
@@ -1742,6 +1772,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.bricks0 = W.bi;
       mgd.nbricks0 = W.nbi;
       mgd.ke32 = W.ke32;
+      mgd.ke20tc = W.ke20tc;
+      mgd.err = W.err;
     }
     // inner FP32 solves aim straight at the outer target when FP32 can reach it
     const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);

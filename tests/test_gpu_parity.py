@@ -262,3 +262,15 @@ def test_hex20_multigrid_cuts_inner_iterations(dtc):
         assert out[pc]["status"] == 0
         assert rel(out[pc]["c"], ref["c"]) <= TOL_MIXED
     assert out["mg"]["iters"].max() * 4 < out["block"]["iters"].max()
+
+
+@pytest.mark.parametrize("precond", ["mg", "jacobi"])
+def test_hex20_tensor_core_matches_oracle(dtc, batch20, precond):
+    """HEX20 FP32 element contraction on tcgen05 (3xTF32): same tolerance as the SIMT kernel."""
+    pairs, refs = batch20
+    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, inner_precond=precond,
+                    mixed_matvec="tensor") as s:
+        res = s.solve([p[0] for p in pairs])
+    for r, ref in zip(res, refs):
+        assert r["status"] == 0
+        assert rel(r["c"], ref["c"]) <= TOL_MIXED
