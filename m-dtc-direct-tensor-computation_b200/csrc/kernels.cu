@@ -806,7 +806,7 @@ namespace {
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
-           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNumBufs };
+           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -896,6 +896,8 @@ int allow_all_ebe(std::string& msg) {
 struct Work {
   const Tile *ti, *ta, *bi, *ba;
   int64_t nti, nta, nbi, nba;
+  const int64_t* nodes;  // active interior nodes, (domain << kListShift) | node
+  int64_t nnodes;
   const double* ke64;   // HEX20 unit element matrix (FP64, then its FP32 copy)
   const float* ke32;
   const float* ke20tc;  // HEX20 FP32 applications on tcgen05: split matrix in the B layout, else null
@@ -1408,6 +1410,8 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   double* zr = B<double>(I, bZr);
   int* act = B<int>(I, bDomAct);
   int* cnt = B<int>(I, bCount);
+  const int64_t nitems = 6 * W.nnodes;
+  const unsigned gflat = (unsigned)std::max<int64_t>((nitems + 255) / 256, 1);
   const dim3 grid((unsigned)(3 * nti));
   DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
@@ -1427,13 +1431,13 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
       for (int k = 0; k < chunk; ++k) {
         if (nti > 0) {
           int q = I.begin(0);
-          k_direction_z<<<grid, kThreads, 0, s>>>(ti, dd, fl, M.z0, p, st, act);
+          k_direction_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, M.z0, p, st, act);
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
           apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
-          k_update_xr<<<grid, kThreads, 0, s>>>(ti, dd, fl, x, r, p, w, st, pw, M.binv0, M.P->omega0, M.t0, act);
+          k_update_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, x, r, p, w, st, pw, M.binv0, M.P->omega0, M.t0, act);
           I.end(kcUpdate32, q, 7 * vb + vb / 12, 0);
           mg_vcycle(I, M, 0, r, zz, zr, act, nl, true);
           nl += 3;
@@ -1519,6 +1523,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   constexpr int m = EL::M;
   std::vector<DomDev> doms;
   std::vector<Tile> tiles_i, tiles_a, bricks_i, bricks_a;
+  std::vector<int64_t> nodes_i;
   std::vector<float> svox;
   std::vector<int64_t> tidx;
   int64_t node_total = 0;
@@ -1581,6 +1586,13 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
             if (act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
       return false;
     };
+    // active interior nodes (flat vector kernels of the multigrid path)
+    for (int z = 1; z < nz - 1; ++z)
+      for (int y = 1; y < ny - 1; ++y)
+        for (int x = 1; x < nx - 1; ++x)
+          if (act[x + (size_t)nx * (y + (size_t)ny * z)])
+            nodes_i.push_back(((int64_t)dom << kListShift) |
+                              (node_total + x + (int64_t)nx * (y + (int64_t)ny * z)));
     // node tiles (vector kernels) over the interior / all nodes
     for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
       for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
@@ -1652,6 +1664,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   if (nti) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesI], tiles_i.data(), sizeof(Tile) * nti, cudaMemcpyHostToDevice, s));
   if (nta) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesA], tiles_a.data(), sizeof(Tile) * nta, cudaMemcpyHostToDevice, s));
   if (nbi) DTC_CUDA(cudaMemcpyAsync(I.bufs[bBricksI], bricks_i.data(), sizeof(Tile) * nbi, cudaMemcpyHostToDevice, s));
+  if ((e = ensure(I, bNodesI, sizeof(int64_t) * std::max<size_t>(nodes_i.size(), 1), msg))) return e;
+  if (!nodes_i.empty())
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bNodesI], nodes_i.data(), sizeof(int64_t) * nodes_i.size(), cudaMemcpyHostToDevice,
+                             s));
   if (nba) DTC_CUDA(cudaMemcpyAsync(I.bufs[bBricksA], bricks_a.data(), sizeof(Tile) * nba, cudaMemcpyHostToDevice, s));
   DTC_CUDA(cudaMemcpyAsync(I.bufs[bSvox], svox.data(), sizeof(float) * svox.size(), cudaMemcpyHostToDevice, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bFlags], 0, node_total, s));
@@ -1671,7 +1687,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   const Tile* ta = B<Tile>(I, bTilesA);
   const double* ke64 = NEN == 20 ? B<double>(I, bKe20) : nullptr;
   const float* ke20tc = (NEN == 20 && I.tensor_matvec) ? B<float>(I, bKe20tc) : nullptr;
-  const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba, ke64,
+  const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba,
+               B<int64_t>(I, bNodesI), (int64_t)nodes_i.size(), ke64,
                ke64 ? reinterpret_cast<const float*>(ke64 + 3600) : nullptr, ke20tc, B<int>(I, bErr)};
   const DomDev* dd = B<DomDev>(I, bDoms);
   uint8_t* fl = B<uint8_t>(I, bFlags);

@@ -441,4 +441,108 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(const Tile* __restrict__
   }
 }
 
+
+// -------------------------------------------------------------------------------------
+// Flat CG vector kernels of the multigrid path: one thread per (active interior node, 4 load
+// cases), 16-byte loads and stores, the list entry packs (domain << 40) | node.
+constexpr int kListShift = 40;
+constexpr int64_t kListNodeMask = (int64_t(1) << kListShift) - 1;
+
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// p = z + bfac p for the iterating columns (others keep p)
+__global__ void __launch_bounds__(256) k_direction_flat(const int64_t* __restrict__ list, int64_t nitems,
+                                                        const float* __restrict__ z, float* __restrict__ p,
+                                                        const ColState* __restrict__ st,
+                                                        const int* __restrict__ dom_active) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nitems) return;
+  const int64_t e = __ldg(list + i / 6);
+  const int dom = (int)(e >> kListShift);
+  if (dom_active && !dom_active[dom]) return;
+  const int64_t node = e & kListNodeMask;
+  const int lc0 = 4 * (int)(i % 6);
+  float bf[4];
+  bool on[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const ColState& c = st[(int64_t)dom * kNLC + lc0 + j];
+    on[j] = c.active != 0;
+    bf[j] = (float)c.bfac;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int64_t k = (node * 3 + c) * kNLC + lc0;
+    float zv[4], pv[4];
+    ld4(z + k, zv);
+    ld4(p + k, pv);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) pv[j] = on[j] ? zv[j] + bf[j] * pv[j] : pv[j];
+    st4(p + k, pv);
+  }
+}
+
+// x += alpha p ; r -= alpha w for the valid columns (alpha = beta / p.w as in k_update), and
+// t = omega D^-1 r (first step of the next V-cycle) for all four
+__global__ void __launch_bounds__(256) k_update_flat(const int64_t* __restrict__ list, int64_t nitems,
+                                                     float* __restrict__ x, float* __restrict__ r,
+                                                     const float* __restrict__ p, const float* __restrict__ w,
+                                                     const ColState* __restrict__ st,
+                                                     const double* __restrict__ acc_pw,
+                                                     const float* __restrict__ binv, float omega,
+                                                     float* __restrict__ t_out, const int* __restrict__ dom_active) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nitems) return;
+  const int64_t e = __ldg(list + i / 6);
+  const int dom = (int)(e >> kListShift);
+  if (dom_active && !dom_active[dom]) return;
+  const int64_t node = e & kListNodeMask;
+  const int lc0 = 4 * (int)(i % 6);
+  float a[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t col = (int64_t)dom * kNLC + lc0 + j;
+    const ColState s = st[col];
+    const double pw = acc_pw[col];
+    const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0) || pw == 0.0);
+    a[j] = (s.active && pw != 0.0 && !flip) ? (float)(s.beta / pw) : 0.f;
+  }
+  float rn[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int64_t k = (node * 3 + c) * kNLC + lc0;
+    float xv[4], pv[4], wv[4];
+    ld4(x + k, xv);
+    ld4(r + k, rn[c]);
+    ld4(p + k, pv);
+    ld4(w + k, wv);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      xv[j] = xv[j] + a[j] * pv[j];
+      rn[c][j] = rn[c][j] - a[j] * wv[j];
+    }
+    st4(x + k, xv);
+    st4(r + k, rn[c]);
+  }
+  const float* bq = binv + node * 6;
+  const float b0 = __ldg(bq), b1 = __ldg(bq + 1), b2 = __ldg(bq + 2), b3 = __ldg(bq + 3), b4 = __ldg(bq + 4),
+              b5 = __ldg(bq + 5);
+  float tv[3][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float r0 = rn[0][j], r1 = rn[1][j], r2 = rn[2][j];
+    tv[0][j] = omega * (b0 * r0 + b3 * r1 + b4 * r2);
+    tv[1][j] = omega * (b3 * r0 + b1 * r1 + b5 * r2);
+    tv[2][j] = omega * (b4 * r0 + b5 * r1 + b2 * r2);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) st4(t_out + (node * 3 + c) * kNLC + lc0, tv[c]);
+}
+
 }  // namespace dtc
