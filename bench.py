@@ -70,6 +70,17 @@ def workload(args):
             "l2": "inputs larger than L2 (vectors are GBs)", "parallelism": f"replicas{args.gpus}"}
 
 
+def reduce_over_ranks(vals, op="max", device="cuda"):
+    """Element-wise max (or min) of a list of floats over all ranks; identity on one process."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in vals]
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+    return [float(v) for v in t.tolist()]
+
+
 def make_inputs(dtc, ndom, L, rank=0):
     syn = dtc.synth
     rng = np.random.default_rng(syn.seed_for(1, 10_000 + rank))
@@ -395,6 +406,8 @@ def main():
         else:
             rtol_of[arm], err_of[arm] = ladder[-1], e
 
+    # every rank times the same configuration: the tightest rtol any rank calibrated
+    rtol_of["mixed"], rtol_of["fp64"] = reduce_over_ranks([rtol_of["mixed"], rtol_of["fp64"]], "min")
     mixed = dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
                        device=local, estimator=args.estimator, inner_precond=args.precond)
 
@@ -419,10 +432,7 @@ def main():
     st = mixed.stats()
     step_ms = float(np.mean(dev_ms))
     t_e2e = float(np.mean(e2e_t))
-    if world > 1:
-        tt = torch.tensor([step_ms, t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_ms, t_e2e = float(tt[0]), float(tt[1])
+    step_ms, t_e2e = reduce_over_ranks([step_ms, t_e2e], "max")
     value = world * args.ndom / (step_ms / 1e3)
     e2e = world * args.ndom / t_e2e
     idx = np.linspace(0, args.ndom - 1, nchk).astype(int)
@@ -433,6 +443,7 @@ def main():
                         device=local) as plain:
             plain.solve(doms)
             fp64_ms = plain.stats()["ms_solve"]
+        fp64_ms = reduce_over_ranks([fp64_ms], "max")[0]
         fp64 = {"value": world * args.ndom / (fp64_ms / 1e3), "ms_per_step": fp64_ms, "rtol": rtol_of["fp64"],
                 "max_rel_err": err_of["fp64"], "estimator": "reaction (reference)",
                 "speedup_mixed_over_fp64": fp64_ms / step_ms}
