@@ -30,7 +30,7 @@ TARGET = 1e-5
 REF_RTOL = 1e-7
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the fine
 # sweeps, measured on 16 domains of 32^3 (profiles/k_matvec_k_mg_matvec_f32_16x32cubed.md)
-DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 0.96, "mg_residual_f32": 1.53}
+DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 0.96, "mg_residual_f32": 1.53, "mg_postsmooth_f32": 1.53}
 # FP32 SIMT FMA peak, nominal: 148 SMs x 128 lanes x 2 flop x 1.965 GHz (the sweeps run on the
 # FMA pipe, not on tensor cores; the measured peaks cover HBM and bf16 tensor only)
 FP32_NOMINAL_TFLOPS = 74.4
