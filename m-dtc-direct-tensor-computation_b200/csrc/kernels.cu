@@ -1434,7 +1434,10 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
           k_direction_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, M.z0, p, st, act);
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
-          apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
+          if (NEN == 8 && I.tensor_matvec)
+            launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, p, w, pw, act, B<int>(I, bErr), s);
+          else
+            apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
           k_update_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, x, r, p, w, st, pw, M.binv0, M.P->omega0, M.t0, act);
