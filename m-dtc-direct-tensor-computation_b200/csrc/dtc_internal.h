@@ -11,8 +11,10 @@
 //    no FP64 quantity passes through float rounding;
 //  * per node one flag byte (active: touches a kept voxel; boundary: on the domain box).
 // Work is cut into tiles of 8 x 4 x 4 nodes; a CTA of 128 threads handles one tile for
-// 8 of the 24 load cases (blockIdx.y = load-case group), each thread one (y,z) row of the
-// tile and one load case, sweeping x with a 3-plane register window.
+// 8 of the 24 load cases (1-D grid, the three load-case groups of a tile adjacent), each
+// thread one (y,z) row of the tile and one load case, sweeping x with a 2-plane register
+// window (the slab sweep of the HEX08 operator).  HEX20 uses voxel bricks (ebe.cuh); the
+// multigrid CG vectors use a flat list of active interior nodes (mg.cuh).
 #pragma once
 #include <cstdint>
 

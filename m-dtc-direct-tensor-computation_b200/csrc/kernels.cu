@@ -1206,7 +1206,7 @@ struct MgDev {
   int* err;
 };
 
-// t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_xr)
+// t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_flat)
 void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act,
                int64_t& launches, bool t_ready = false) {
   cudaStream_t s = I.stream;

@@ -20,7 +20,7 @@
 // correction, so the V-cycle is a fixed SPD operator.
 //
 // One V-cycle per CG iteration, per level l that is not a domain's coarsest:
-//   t_l = omega D_l^-1 b_l                        k_mg_jacobi (fine level: k_update_xr)
+//   t_l = omega D_l^-1 b_l                        k_mg_jacobi (fine level: k_update_flat)
 //   r_l = b_l - K_l t_l                           k_mg_matvec<kMgRes>
 //   b_{l+1} = P^T r_l                             k_mg_restrict
 //   (level l+1: recurse, or z_{l+1} = K^-1 b)     ...  / k_mg_coarse
@@ -369,78 +369,6 @@ __global__ void __launch_bounds__(256) k_mg_coarse(const int* __restrict__ list,
     }
   }
 }
-
-// CG vectors with the preconditioned residual z given: p = z + bfac p
-__global__ void __launch_bounds__(kThreads) k_direction_z(const Tile* __restrict__ tiles,
-                                                          const DomDev* __restrict__ doms,
-                                                          const uint8_t* __restrict__ flags,
-                                                          const float* __restrict__ z, float* __restrict__ p,
-                                                          const ColState* __restrict__ st,
-                                                          const int* __restrict__ dom_active) {
-  const Tile t = tiles[blockIdx.x / 3];
-  if (dom_active && !dom_active[t.dom]) return;
-  const DomDev D = doms[t.dom];
-  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
-  const int row = threadIdx.x >> 3;
-  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
-  const int64_t col = (int64_t)t.dom * kNLC + lc;
-  if (yy < 1 || yy > D.n[1] - 2 || zz < 1 || zz > D.n[2] - 2 || !st[col].active) return;
-  const float bf = (float)st[col].bfac;
-  for (int i = 0; i < kTileX; ++i) {
-    const int x = t.x0 + i;
-    if (x > D.n[0] - 2) break;
-    const int64_t n = node_index(D, x, yy, zz);
-    if (!(flags[n] & kNodeActive)) continue;
-    const int64_t k0 = vec_index(n, 0, lc);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) p[k0 + c * kNLC] = z[k0 + c * kNLC] + bf * p[k0 + c * kNLC];
-  }
-}
-
-// x += alpha p ; r -= alpha w  (alpha = beta / p.w unless the column stopped or p.w flags an
-// indefinite operator, exactly as in k_update); also writes the first step of the next V-cycle,
-// t = omega D^-1 r, on the same nodes (the multigrid pre-smoothing from a zero guess).
-__global__ void __launch_bounds__(kThreads) k_update_xr(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
-                                                        const uint8_t* __restrict__ flags, float* __restrict__ x,
-                                                        float* __restrict__ r, const float* __restrict__ p,
-                                                        const float* __restrict__ w, const ColState* __restrict__ st,
-                                                        const double* __restrict__ acc_pw,
-                                                        const float* __restrict__ binv, float omega,
-                                                        float* __restrict__ t_out,
-                                                        const int* __restrict__ dom_active) {
-  const Tile t = tiles[blockIdx.x / 3];
-  if (dom_active && !dom_active[t.dom]) return;
-  const DomDev D = doms[t.dom];
-  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
-  const int row = threadIdx.x >> 3;
-  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
-  const int64_t col = (int64_t)t.dom * kNLC + lc;
-  if (yy < 1 || yy > D.n[1] - 2 || zz < 1 || zz > D.n[2] - 2) return;
-  const ColState s = st[col];
-  const double pw = acc_pw[col];
-  const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0) || pw == 0.0);
-  if (!s.active || pw == 0.0 || flip) return;   // r unchanged: its t from before still holds
-  const float a = (float)(s.beta / pw);
-  for (int i = 0; i < kTileX; ++i) {
-    const int xx = t.x0 + i;
-    if (xx > D.n[0] - 2) break;
-    const int64_t n = node_index(D, xx, yy, zz);
-    if (!(flags[n] & kNodeActive)) continue;
-    const int64_t k0 = vec_index(n, 0, lc);
-    float rn[3], tn[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t k = k0 + c * kNLC;
-      x[k] = x[k] + a * p[k];
-      rn[c] = r[k] - a * w[k];
-      r[k] = rn[c];
-    }
-    block_jacobi(binv, n, omega, rn, tn);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) t_out[k0 + c * kNLC] = tn[c];
-  }
-}
-
 
 // -------------------------------------------------------------------------------------
 // Flat CG vector kernels of the multigrid path: one thread per (active interior node, 4 load
