@@ -167,8 +167,8 @@ def run_reference(args, dtc):
     orc = ge.load_oracle()
     orc.build()
     syn = dtc.synth
-    cores = os.cpu_count() or 1
-    nsample = min(args.ndom, cores, 32)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    nsample = min(args.ndom, cores)   # every host thread it can use, one domain each
     grays, _ = make_inputs(dtc, nsample, args.L)
     rtol = args.rtol if args.rtol > 0 else REF_RTOL
     doms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=rtol, max_it=args.max_it,
