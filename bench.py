@@ -454,6 +454,7 @@ def main():
                     inner_precond=args.precond) as prof:
         prof.solve(doms)
         ks = prof.kernel_stats()
+    host = {k: ks.pop(k) for k in list(ks) if k.startswith("host_")}   # host phases, wall ms
     top = max((k for k in ks if ks[k]["bytes_per_launch"] > 0), key=lambda k: ks[k]["ms_total"])
     kt = ks[top]
     t_launch = kt["ms_total"] / kt["launches"] / 1e3
@@ -480,7 +481,8 @@ def main():
                              "flops_per_launch": kt["flops_per_launch"],
                              "achieved_tflops": kt["flops_per_launch"] / t_launch / 1e12,
                              "fp32_fma_frac_of_nominal": kt["flops_per_launch"] / t_launch / 1e12 / FP32_NOMINAL_TFLOPS,
-                             "kernel_time_share": share},
+                             "kernel_time_share": share,
+                             "host_ms_per_step": {k: v["ms_total"] for k, v in host.items()}},
                 "cpu_baseline": cpu,
                 "gpu_launches": st["kernel_launches"], "clocks": clk,
                 "e2e": {"value": e2e, "unit": "domains/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}

@@ -15,10 +15,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fe.h"
@@ -1065,12 +1067,32 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
 
 // Build the hierarchy on the host from the fine voxel factors.  fine_i: interior tiles of the
 // fine level (level-0 smoothing tiles are those of domains with a coarser level).
+// Runs f(i) for i in [0, n) on `threads` host threads (0: hardware concurrency).
+template <class F>
+void parallel_for(int64_t n, int threads, F&& f) {
+  int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
+  std::atomic<int64_t> next(0);
+  auto work = [&]() {
+    for (;;) {
+      const int64_t i = next.fetch_add(1);
+      if (i >= n) break;
+      f(i);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+}
+
 // HEX20 fine grids (m = 2) get one p-coarsening first: level 1 is the HEX08 mesh of the same
 // voxels (corner nodes; the trilinear space is contained in the serendipity one, so the
 // exactly integrated HEX08 matrix is the Galerkin product of the HEX20 one), then the voxel
-// grids are halved as for HEX08.
+// grids are halved as for HEX08.  Every domain's levels are built on their own host thread,
+// then concatenated in domain order (the layout does not depend on the thread count).
 void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<float>& svox0,
-              const std::vector<Tile>& fine_i, double nu, int nen) {
+              const std::vector<Tile>& fine_i, double nu, int nen, int threads) {
   const int ndom = (int)doms0.size();
   double kh[576];
   voxel_stiffness(8, nu, kh);
@@ -1094,46 +1116,37 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
     }
     nl = std::max(nl, nlev[d]);
   }
-  P.nlev = nl;
-  P.doms.assign((size_t)nl * ndom, DomDev{});
-  P.sm_off.assign(nl, 0); P.sm_n.assign(nl, 0); P.in_off.assign(nl, 0); P.in_n.assign(nl, 0);
-  P.all_off.assign(nl, 0); P.all_n.assign(nl, 0); P.list_off.assign(nl, 0); P.list_n.assign(nl, 0);
-  P.tiles.clear(); P.lists.clear(); P.svox.clear(); P.nodes = 0;
-  P.minv.assign((size_t)ndom * kMgDenseN * kMgDenseN, 0.f);
-  for (int d = 0; d < ndom; ++d) P.doms[d] = doms0[d];
-  // level 0 smoothing tiles
-  P.sm_off[0] = 0;
-  for (const Tile& t : fine_i) if (nlev[t.dom] > 1) P.tiles.push_back(t);
-  P.sm_n[0] = (int64_t)P.tiles.size();
-  std::vector<std::vector<float>> cur(ndom);   // voxel factors of the current level per domain
-  for (int d = 0; d < ndom; ++d) cur[d].assign(svox0.begin() + doms0[d].vox_off,
-                                               svox0.begin() + doms0[d].vox_off +
-                                                   (int64_t)doms0[d].L[0] * doms0[d].L[1] * doms0[d].L[2]);
-  for (int l = 1; l < nl; ++l) {
+  // per domain and level >= 1: grid, voxel factors, work lists (offsets filled in later)
+  struct Level {
+    DomDev C;
+    std::vector<float> sv;
     std::vector<Tile> t_in, t_sm, t_all;
-    for (int d = 0; d < ndom; ++d) {
-      if (nlev[d] <= l) continue;
-      const DomDev& F = P.doms[(size_t)(l - 1) * ndom + d];
+  };
+  std::vector<std::vector<Level>> lev(ndom);
+  P.minv.assign((size_t)ndom * kMgDenseN * kMgDenseN, 0.f);
+  parallel_for(ndom, threads, [&](int64_t dd) {
+    const int d = (int)dd;
+    std::vector<float> cur(svox0.begin() + doms0[d].vox_off,
+                           svox0.begin() + doms0[d].vox_off + (int64_t)doms0[d].L[0] * doms0[d].L[1] * doms0[d].L[2]);
+    DomDev F = doms0[d];
+    lev[d].resize(nlev[d]);
+    for (int l = 1; l < nlev[d]; ++l) {
+      Level& Lv = lev[d][l];
       DomDev C = F;
       const bool pc = F.m == 2;   // p-coarsening: same voxels, corner nodes
       for (int k = 0; k < 3; ++k) { C.L[k] = pc ? F.L[k] : (F.L[k] + 1) / 2; C.n[k] = C.L[k] + 1; }
       C.m = 1;
       C.scale = pc ? F.scale : 2.0 * F.scale;
-      C.vox_off = (int64_t)P.svox.size();
-      C.node_off = P.nodes;
       std::vector<float> nv((size_t)C.L[0] * C.L[1] * C.L[2], 0.f);
       if (pc) {
-        nv = cur[d];
+        nv = cur;
       } else {
         for (int z = 0; z < F.L[2]; ++z)
           for (int y = 0; y < F.L[1]; ++y)
             for (int x = 0; x < F.L[0]; ++x)
               nv[(x / 2) + (size_t)C.L[0] * ((y / 2) + (size_t)C.L[1] * (z / 2))] +=
-                  0.125f * cur[d][x + (size_t)F.L[0] * (y + (size_t)F.L[1] * z)];
+                  0.125f * cur[x + (size_t)F.L[0] * (y + (size_t)F.L[1] * z)];
       }
-      P.svox.insert(P.svox.end(), nv.begin(), nv.end());
-      P.nodes += (int64_t)C.n[0] * C.n[1] * C.n[2];
-      P.doms[(size_t)l * ndom + d] = C;
       // activity and tiles
       const int nx = C.n[0], ny = C.n[1], nz = C.n[2];
       std::vector<uint8_t> act((size_t)nx * ny * nz, 0);
@@ -1157,31 +1170,57 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
           for (int x0 = 1; x0 <= nx - 2; x0 += kTileX)
             if (any(x0, y0, z0, 1, nx - 2, ny - 2, nz - 2)) {
               const Tile t{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0};
-              t_in.push_back(t);
-              if (nlev[d] > l + 1) t_sm.push_back(t);
+              Lv.t_in.push_back(t);
+              if (nlev[d] > l + 1) Lv.t_sm.push_back(t);
             }
       for (int z0 = 0; z0 <= nz - 1; z0 += kTileZ)
         for (int y0 = 0; y0 <= ny - 1; y0 += kTileY)
           for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
-            if (any(x0, y0, z0, 0, nx - 1, ny - 1, nz - 1)) t_all.push_back(Tile{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
-      cur[d].swap(nv);
+            if (any(x0, y0, z0, 0, nx - 1, ny - 1, nz - 1))
+              Lv.t_all.push_back(Tile{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+      Lv.C = C;
+      Lv.sv = nv;
+      cur.swap(nv);
+      F = C;
     }
-    P.sm_off[l] = (int64_t)P.tiles.size(); P.sm_n[l] = (int64_t)t_sm.size();
-    P.tiles.insert(P.tiles.end(), t_sm.begin(), t_sm.end());
-    P.in_off[l] = (int64_t)P.tiles.size(); P.in_n[l] = (int64_t)t_in.size();
-    P.tiles.insert(P.tiles.end(), t_in.begin(), t_in.end());
-    P.all_off[l] = (int64_t)P.tiles.size(); P.all_n[l] = (int64_t)t_all.size();
-    P.tiles.insert(P.tiles.end(), t_all.begin(), t_all.end());
+    // coarsest level: dense inverse (its grid is lev[d].back().C, or the fine one)
+    const DomDev& Cc = nlev[d] > 1 ? lev[d][nlev[d] - 1].C : doms0[d];
+    coarse_inverse(Cc, cur.data(), kh, &P.minv[(size_t)d * kMgDenseN * kMgDenseN]);
+  });
+  // concatenate in domain order
+  P.nlev = nl;
+  P.doms.assign((size_t)nl * ndom, DomDev{});
+  P.sm_off.assign(nl, 0); P.sm_n.assign(nl, 0); P.in_off.assign(nl, 0); P.in_n.assign(nl, 0);
+  P.all_off.assign(nl, 0); P.all_n.assign(nl, 0); P.list_off.assign(nl, 0); P.list_n.assign(nl, 0);
+  P.tiles.clear(); P.lists.clear(); P.svox.clear(); P.nodes = 0;
+  for (int d = 0; d < ndom; ++d) P.doms[d] = doms0[d];
+  P.sm_off[0] = 0;
+  for (const Tile& t : fine_i) if (nlev[t.dom] > 1) P.tiles.push_back(t);
+  P.sm_n[0] = (int64_t)P.tiles.size();
+  for (int l = 1; l < nl; ++l) {
+    for (int d = 0; d < ndom; ++d) {
+      if (nlev[d] <= l) continue;
+      Level& Lv = lev[d][l];
+      Lv.C.vox_off = (int64_t)P.svox.size();
+      Lv.C.node_off = P.nodes;
+      P.svox.insert(P.svox.end(), Lv.sv.begin(), Lv.sv.end());
+      P.nodes += (int64_t)Lv.C.n[0] * Lv.C.n[1] * Lv.C.n[2];
+      P.doms[(size_t)l * ndom + d] = Lv.C;
+    }
+    auto append = [&](std::vector<Tile> Level::*member, int64_t& off, int64_t& cnt) {
+      off = (int64_t)P.tiles.size();
+      for (int d = 0; d < ndom; ++d)
+        if (nlev[d] > l) P.tiles.insert(P.tiles.end(), (lev[d][l].*member).begin(), (lev[d][l].*member).end());
+      cnt = (int64_t)P.tiles.size() - off;
+    };
+    append(&Level::t_sm, P.sm_off[l], P.sm_n[l]);
+    append(&Level::t_in, P.in_off[l], P.in_n[l]);
+    append(&Level::t_all, P.all_off[l], P.all_n[l]);
   }
-  // coarsest levels: domain lists and dense inverses
   for (int l = 0; l < nl; ++l) {
     P.list_off[l] = (int64_t)P.lists.size();
     for (int d = 0; d < ndom; ++d)
-      if (nlev[d] - 1 == l) {
-        P.lists.push_back(d);
-        const DomDev& C = P.doms[(size_t)l * ndom + d];
-        coarse_inverse(C, cur[d].data(), kh, &P.minv[(size_t)d * kMgDenseN * kMgDenseN]);
-      }
+      if (nlev[d] - 1 == l) P.lists.push_back(d);
     P.list_n[l] = (int64_t)P.lists.size() - P.list_off[l];
   }
 }
@@ -1477,7 +1516,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
                                              "direction_f32", "direction_f64", "colstate", "reaction_f64",
                                              "project_f64", "mg_jacobi_f32", "mg_residual_f32",
-                                             "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32"};
+                                             "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
+                                             "host_pack", "host_multigrid_build"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
@@ -1522,6 +1562,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       if (int e = allow_all_ebe<NEN>(msg)) return e;   // per device, cheap
   }
   // pack the batch (all solvable tasks at once; chunking by memory happens in the caller)
+  const auto tpack = std::chrono::steady_clock::now();
   using EL = Elem<NEN>;
   constexpr int m = EL::M;
   std::vector<DomDev> doms;
@@ -1530,16 +1571,38 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   std::vector<float> svox;
   std::vector<int64_t> tidx;
   int64_t node_total = 0;
-  for (size_t k = 0; k < tasks.size(); ++k) {
+  // which tasks are solved here, and each domain's voxel and node offsets (serial, cheap)
+  for (size_t k = 0; k < tasks.size(); ++k)
+    if (tasks[k].plan->status == DTC_DOMAIN_OK) tidx.push_back((int64_t)k);
+  const int ndom_p = (int)tidx.size();
+  std::vector<int64_t> vox_offs(ndom_p), node_offs(ndom_p);
+  int64_t vox_total = 0;
+  for (int d = 0; d < ndom_p; ++d) {
+    const dtc_domain_in& in = *tasks[tidx[d]].in;
+    vox_offs[d] = vox_total;
+    node_offs[d] = node_total;
+    vox_total += in.L[0] * in.L[1] * in.L[2];
+    node_total += (int64_t)(m * in.L[0] + 1) * (m * in.L[1] + 1) * (m * in.L[2] + 1);
+  }
+  svox.assign((size_t)vox_total, 0.f);
+  // per domain: voxel factors, node activity and work lists (host threads)
+  struct Packed {
+    DomDev D;
+    std::vector<Tile> ti, ta, bi, ba;
+    std::vector<int64_t> ni;
+    double vec = 0, mv = 0, fl = 0;
+  };
+  std::vector<Packed> packed(ndom_p);
+  auto pack_one = [&](int dom, Packed& out) {
+    const size_t k = (size_t)tidx[dom];
     DomainTask& t = tasks[k];
     const MeshPlan& mp = *t.plan;
-    if (mp.status != DTC_DOMAIN_OK) continue;
     const dtc_domain_in& in = *t.in;
     DomDev D{};
     D.m = m;
     for (int d = 0; d < 3; ++d) { D.L[d] = (int32_t)in.L[d]; D.n[d] = m * (int32_t)in.L[d] + 1; }
-    D.vox_off = (int64_t)svox.size();
-    D.node_off = node_total;
+    D.vox_off = vox_offs[dom];
+    D.node_off = node_offs[dom];
     D.delta = in.delta[0];
     for (int d = 0; d < 3; ++d) {
       D.min_c_off[d] = in.xa_n[d] - 1;
@@ -1549,8 +1612,6 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     const int64_t nvox = in.L[0] * in.L[1] * in.L[2];
     const double a = in.phdsize[0] * in.delta[0];
     D.scale = in.E_voxel ? a : a * in.E;
-    const int dom = (int)doms.size();
-    svox.resize(svox.size() + nvox);
     float* sv = svox.data() + D.vox_off;
     for (int64_t v = 0; v < nvox; ++v) sv[v] = mp.kept[v] ? (in.E_voxel ? in.E_voxel[v] : 1.0f) : 0.0f;
     // node activity on the (fine) grid for the work lists; kept voxels per node for the flop count
@@ -1578,9 +1639,9 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       for (int z = 1; z < nz - 1; ++z)
         for (int y = 1; y < ny - 1; ++y)
           for (int x = 1; x < nx - 1; ++x) nint += act[x + (size_t)nx * (y + (size_t)ny * z)];
-      I.dom_vec_bytes.push_back(72.0 * nint);
-      I.dom_mv_bytes.push_back(2 * 72.0 * nint + (double)nvox);
-      I.dom_mv_flops.push_back(kept * 2.0 * (3 * NEN) * (3 * NEN) * kNLC);
+      out.vec = 72.0 * nint;
+      out.mv = 2 * 72.0 * nint + (double)nvox;
+      out.fl = kept * 2.0 * (3 * NEN) * (3 * NEN) * kNLC;
     }
     auto any_active = [&](int x0, int y0, int z0, int sx, int sy, int sz, int lo, int hx, int hy, int hz) {
       for (int z = std::max(z0, lo); z < std::min(z0 + sz, hz + 1); ++z)
@@ -1594,32 +1655,44 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       for (int y = 1; y < ny - 1; ++y)
         for (int x = 1; x < nx - 1; ++x)
           if (act[x + (size_t)nx * (y + (size_t)ny * z)])
-            nodes_i.push_back(((int64_t)dom << kListShift) |
-                              (node_total + x + (int64_t)nx * (y + (int64_t)ny * z)));
+            out.ni.push_back(((int64_t)dom << kListShift) |
+                             (D.node_off + x + (int64_t)nx * (y + (int64_t)ny * z)));
     // node tiles (vector kernels) over the interior / all nodes
     for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
       for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
         for (int x0 = 1; x0 <= nx - 2; x0 += kTileX)
           if (any_active(x0, y0, z0, kTileX, kTileY, kTileZ, 1, nx - 2, ny - 2, nz - 2))
-            tiles_i.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+            out.ti.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
     for (int z0 = 0; z0 <= nz - 1; z0 += kTileZ)
       for (int y0 = 0; y0 <= ny - 1; y0 += kTileY)
         for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
           if (any_active(x0, y0, z0, kTileX, kTileY, kTileZ, 0, nx - 1, ny - 1, nz - 1))
-            tiles_a.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+            out.ta.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
     // voxel bricks (HEX20 operator): brick origin in voxels, owned nodes m*origin + [0, m*B)
     for (int bz = 0; NEN == 20 && m * bz <= nz - 1; bz += EL::BZ)
       for (int by = 0; m * by <= ny - 1; by += EL::BY)
         for (int bx = 0; m * bx <= nx - 1; bx += EL::BX) {
           const int ox = m * bx, oy = m * by, oz = m * bz;
           if (any_active(ox, oy, oz, m * EL::BX, m * EL::BY, m * EL::BZ, 1, nx - 2, ny - 2, nz - 2))
-            bricks_i.push_back(Tile{dom, (int16_t)bx, (int16_t)by, (int16_t)bz, 0});
+            out.bi.push_back(Tile{dom, (int16_t)bx, (int16_t)by, (int16_t)bz, 0});
           if (any_active(ox, oy, oz, m * EL::BX, m * EL::BY, m * EL::BZ, 0, nx - 1, ny - 1, nz - 1))
-            bricks_a.push_back(Tile{dom, (int16_t)bx, (int16_t)by, (int16_t)bz, 0});
+            out.ba.push_back(Tile{dom, (int16_t)bx, (int16_t)by, (int16_t)bz, 0});
         }
-    node_total += (int64_t)nx * ny * nz;
-    doms.push_back(D);
-    tidx.push_back((int64_t)k);
+    out.D = D;
+  };
+  parallel_for(ndom_p, opt.host_threads, [&](int64_t d) { pack_one((int)d, packed[d]); });
+  // concatenate in domain order
+  for (int d = 0; d < ndom_p; ++d) {
+    Packed& q = packed[d];
+    doms.push_back(q.D);
+    tiles_i.insert(tiles_i.end(), q.ti.begin(), q.ti.end());
+    tiles_a.insert(tiles_a.end(), q.ta.begin(), q.ta.end());
+    bricks_i.insert(bricks_i.end(), q.bi.begin(), q.bi.end());
+    bricks_a.insert(bricks_a.end(), q.ba.begin(), q.ba.end());
+    nodes_i.insert(nodes_i.end(), q.ni.begin(), q.ni.end());
+    I.dom_vec_bytes.push_back(q.vec);
+    I.dom_mv_bytes.push_back(q.mv);
+    I.dom_mv_flops.push_back(q.fl);
   }
   const int ndom = (int)doms.size();
   if (ndom == 0) return DTC_OK;
@@ -1662,6 +1735,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   if ((e = ensure(I, bErr, sizeof(int), msg))) return e;
   DTC_CUDA(cudaMemsetAsync(I.bufs[bErr], 0, sizeof(int), s));
 
+  stats_.kc[kcHostPack].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tpack).count();
+  stats_.kc[kcHostPack].launches += 1;
   auto t0 = std::chrono::steady_clock::now();
   DTC_CUDA(cudaMemcpyAsync(I.bufs[bDoms], doms.data(), sizeof(DomDev) * ndom, cudaMemcpyHostToDevice, s));
   if (nti) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesI], tiles_i.data(), sizeof(Tile) * nti, cudaMemcpyHostToDevice, s));
@@ -1728,7 +1803,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     MgPlan mgp;
     MgDev mgd{};
     if (use_mg) {
-      build_mg(mgp, doms, svox, tiles_i, nu, NEN);
+      const auto tb = std::chrono::steady_clock::now();
+      build_mg(mgp, doms, svox, tiles_i, nu, NEN, opt.host_threads);
+      stats_.kc[kcHostMgBuild].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+      stats_.kc[kcHostMgBuild].launches += 1;
       const int64_t cn = std::max<int64_t>(mgp.nodes, 1);
       if ((e = ensure(I, bZ32, vbytes32, msg)) || (e = ensure(I, bT32, vbytes32, msg)) ||
           (e = ensure(I, bMgDoms, sizeof(DomDev) * mgp.doms.size(), msg)) ||
