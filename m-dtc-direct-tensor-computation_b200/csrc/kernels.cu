@@ -1067,6 +1067,11 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
 
 // Build the hierarchy on the host from the fine voxel factors.  fine_i: interior tiles of the
 // fine level (level-0 smoothing tiles are those of domains with a coarser level).
+// Levels from this one down smooth twice per visit (pre and post): on 256 x 32^3 and on an
+// uneven batch (16^3-64^3) ~3.5% less solve time than once everywhere; twice already on
+// level 1 costs more than the iterations it saves.
+constexpr int kMgTwiceFrom = 2;
+
 // Runs f(i) for i in [0, n) on `threads` host threads (0: hardware concurrency).
 template <class F>
 void parallel_for(int64_t n, int threads, F&& f) {
@@ -1288,6 +1293,16 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   }
   q = fine ? I.begin(0) : -1;
   const float om = fine ? P.omega0 : P.omega;
+  // deeper levels smooth twice before and after their coarse correction (their grids are small)
+  const bool twice = !fine && l >= kMgTwiceFrom;
+  float* cur = t;                  // the smoothed iterate
+  float* rbuf = z;                 // the residual handed to the restriction
+  if (twice) {
+    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
+    ++launches;
+    cur = z;
+    rbuf = t;
+  }
   if (fine && M.nen0 == 20) {
     if (M.ke20tc)
       launch_ebe_tc(M.bricks0, M.nbricks0, dl, sv, fl, M.ke20tc, t, z, -1.0, nullptr, act, M.err, s);
@@ -1296,21 +1311,21 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
     k_mg_combine<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, om, nullptr, nullptr, act);
     ++launches;
   } else {
-    k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
+    k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   }
   if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
   q = fine ? I.begin(0) : -1;
   if (P.in_n[l + 1] > 0)
-    k_mg_restrict<<<(unsigned)(3 * P.in_n[l + 1]), kThreads, 0, s>>>(M.tiles + P.in_off[l + 1], dc, M.flags, dl, z,
-                                                                    M.b, act);
+    k_mg_restrict<<<(unsigned)(3 * P.in_n[l + 1]), kThreads, 0, s>>>(M.tiles + P.in_off[l + 1], dc, M.flags, dl,
+                                                                    rbuf, M.b, act);
   if (fine) I.end(kcMgTransfer, q, vb * (1.0 + 1.0 / 8.0), 0);
   launches += 2;
   if (!fine) I.end(kcMgCoarse, q0, 0, 0);
   mg_vcycle(I, M, l + 1, r0, zz, zr, act, launches);
   const int q1 = fine ? -1 : I.begin(0);
   q = fine ? I.begin(0) : -1;
-  k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, dc, M.z, t, act);
+  k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, dc, M.z, cur, act);
   if (fine) I.end(kcMgTransfer, q, vb * (2.0 + 1.0 / 8.0), 0);
   q = fine ? I.begin(0) : -1;
   if (l == 0 && M.nen0 == 20) {
@@ -1322,7 +1337,12 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
     ++launches;
   } else if (l == 0)
     k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
-  else
+  else if (twice) {
+    // z holds the corrected iterate: t = z + w D^-1 (b - K z), then z = t + w D^-1 (b - K t)
+    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, z, t, P.omega, nullptr, nullptr, act);
+    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+    ++launches;
+  } else
     k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
   if (fine) I.end(kcMgPost, q, mb + vb + vb / 12, mf);     // t in, z out (mb), b in, D^-1
   if (!fine) I.end(kcMgCoarse, q1, 0, 0);

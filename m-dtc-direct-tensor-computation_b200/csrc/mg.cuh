@@ -26,6 +26,7 @@
 //   (level l+1: recurse, or z_{l+1} = K^-1 b)     ...  / k_mg_coarse
 //   t_l += P z_{l+1}                              k_mg_prolong
 //   z_l = t_l + omega D_l^-1 (b_l - K_l t_l)      k_mg_matvec<kMgPost> (+ z.z, z.b on level 0)
+// Levels >= 2 apply the smoothing step twice before and twice after the coarse correction.
 #pragma once
 
 namespace dtc {
