@@ -339,6 +339,16 @@ def run_config(args, dtc):
     print(json.dumps(line), flush=True)
 
 
+def share_host_cpus(local, local_world):
+    """Pins this rank to its contiguous 1/local_world share of the host CPUs, so the host
+    phases of the solver (meshing, packing, multigrid build: one thread per CPU of the
+    affinity mask) of the ranks on one node do not oversubscribe it."""
+    cpus = sorted(os.sched_getaffinity(0))
+    k = len(cpus) // max(local_world, 1)
+    if k >= 1 and local_world > 1:
+        os.sched_setaffinity(0, cpus[local * k:(local + 1) * k])
+
+
 def main():
     args = parse()
     dtc = ge.load_package()
@@ -356,6 +366,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        share_host_cpus(local, int(os.environ.get("LOCAL_WORLD_SIZE", str(world))))
     torch.cuda.set_device(local)
     syn = dtc.synth
     grays, _ = make_inputs(dtc, args.ndom, args.L, rank)

@@ -70,7 +70,8 @@ typedef struct dtc_options {
   int32_t max_refine;      /* mixed path: cap on FP64 refinement steps (0 -> 12) */
   int32_t rotation_search; /* 1: run the CR1/CR2 rotation search (mod_struct_calcmat.f90:533-1603) */
   int32_t device;          /* CUDA device ordinal */
-  int32_t host_threads;    /* threads for host-side meshing (0 -> hardware concurrency) */
+  int32_t host_threads;    /* threads for the host phases: meshing, packing, multigrid
+                              build (0 -> the CPUs of the process affinity mask) */
   int32_t keep_displacements; /* 1: keep the converged displacements on the device for
                                  dtc_energy_grad (the adjoint); 0: release them */
   int32_t profile_kernels; /* 1: time every solver kernel with CUDA events on its stream

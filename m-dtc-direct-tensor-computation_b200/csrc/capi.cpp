@@ -40,7 +40,7 @@ int validate_domain(const dtc_domain_in& in, std::string& msg) {
 
 void plan_all(const dtc_domain_in* in, int64_t n, std::vector<MeshPlan>& plans, bool numbering, int threads) {
   plans.resize(n);
-  int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  int nt = host_thread_count(threads);
   nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
   std::atomic<int64_t> next(0);
   auto work = [&]() {

@@ -1072,10 +1072,10 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
 // level 1 costs more than the iterations it saves.
 constexpr int kMgTwiceFrom = 2;
 
-// Runs f(i) for i in [0, n) on `threads` host threads (0: hardware concurrency).
+// Runs f(i) for i in [0, n) on `threads` host threads (0: the CPUs of the affinity mask).
 template <class F>
 void parallel_for(int64_t n, int threads, F&& f) {
-  int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  int nt = host_thread_count(threads);
   nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
   std::atomic<int64_t> next(0);
   auto work = [&]() {

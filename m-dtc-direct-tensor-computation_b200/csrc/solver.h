@@ -1,13 +1,30 @@
 // solver.h -- device batch solver (kernels.cu) interface used by the C ABI layer.
 #pragma once
+#include <sched.h>
+
+#include <algorithm>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dtc.h"
 #include "mesher.h"
 
 namespace dtc {
+
+// Host threads for the per-domain host phases: the requested count, else the CPUs this
+// process may run on (its affinity mask, so ranks pinned to disjoint core sets do not
+// oversubscribe the node), else the hardware concurrency.
+inline int host_thread_count(int requested) {
+  if (requested > 0) return requested;
+  cpu_set_t set;
+  if (sched_getaffinity(0, sizeof(set), &set) == 0) {
+    const int n = CPU_COUNT(&set);
+    if (n > 0) return n;
+  }
+  return (int)std::max(1u, std::thread::hardware_concurrency());
+}
 
 struct DomainTask {
   const dtc_domain_in* in = nullptr;
