@@ -38,8 +38,7 @@ int validate_domain(const dtc_domain_in& in, std::string& msg) {
   return 0;
 }
 
-void plan_all(const dtc_domain_in* in, int64_t n, std::vector<MeshPlan>& plans, bool numbering, int threads) {
-  plans.resize(n);
+void plan_all(const dtc_domain_in* in, int64_t n, MeshPlan* plans, bool numbering, int threads) {
   int nt = host_thread_count(threads);
   nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
   std::atomic<int64_t> next(0);
@@ -212,62 +211,96 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     if (in[i].nu != in[0].nu) { h->err = "all domains of one call must share nu"; return DTC_ERR_INVALID_ARGUMENT; }
     if (in[i].elem_type != in[0].elem_type) { h->err = "all domains of one call must share elem_type"; return DTC_ERR_INVALID_ARGUMENT; }
   }
-  std::vector<MeshPlan> plans;
+  std::vector<MeshPlan> plans((size_t)n);
   bool want_fields = false;
   for (int64_t i = 0; i < n; ++i) want_fields = want_fields || out[i].displ || out[i].force;
-  plan_all(in, n, plans, want_fields, h->opt.host_threads);
-  std::vector<DomainTask> tasks;
-  for (int64_t i = 0; i < n; ++i) {
-    dtc_domain_out* o = &out[i];
-    double* keep_d = o->displ;
-    double* keep_f = o->force;
-    std::memset(o, 0, sizeof(*o));
-    o->displ = keep_d; o->force = keep_f;
-    o->domain_number = in[i].domain_number;
-    o->status = plans[i].status;
-    o->ne = plans[i].ne; o->nn = plans[i].nn; o->nb = plans[i].nb;
-    o->n_free_dof = plans[i].n_free_dof;
-    if (plans[i].status == DTC_DOMAIN_OK) tasks.push_back(DomainTask{&in[i], &plans[i], o, i});
-  }
-  // memory-bounded chunks
+  // Device passes: bounded by 80 % of the free device memory and chunk_domains.  A large batch
+  // also starts with a small pass (1/8 of it): the host phase of the rest (mesh planning,
+  // packing, multigrid plan) runs on a host thread while the device solves that first pass.
+  // Every pass repeats the latency-bound tail of the solve (its slowest domain, the coarse
+  // levels), so one cut, not more.  The adjoint keeps the last pass on the device: no extra
+  // cut with keep_displacements.
+  constexpr int64_t kPipelineMin = 256;
+  const bool keep = h->opt.keep_displacements != 0;
+  const int64_t pipe = (!keep && n >= kPipelineMin) ? std::max<int64_t>(32, n / 8) : 0;
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { h->err = "cudaMemGetInfo failed"; return DTC_ERR_CUDA; }
   const double budget = 0.80 * (double)free_b;
-  std::vector<size_t> cuts{0};
+  std::vector<int64_t> cuts{0};
   {
     double bytes = 0;
-    for (size_t k = 0; k < tasks.size(); ++k) {
-      const dtc_domain_in& d = *tasks[k].in;
+    for (int64_t k = 0; k < n; ++k) {
+      const dtc_domain_in& d = in[k];
       const int mg = d.elem_type == DTC_HEX20 ? 2 : 1;   // HEX20 nodes live on the doubled grid
       const double nb = (double)(mg * d.L[0] + 1) * (mg * d.L[1] + 1) * (mg * d.L[2] + 1) * device_bytes_per_node();
-      const bool full = h->opt.chunk_domains > 0 && (int64_t)(k - cuts.back()) >= h->opt.chunk_domains;
+      const int64_t cnt = k - cuts.back();
+      const bool full = (h->opt.chunk_domains > 0 && cnt >= h->opt.chunk_domains) ||
+                        (pipe > 0 && cuts.size() == 1 && cnt >= pipe);
       if (k > cuts.back() && (bytes + nb > budget || full)) { cuts.push_back(k); bytes = 0; }
       bytes += nb;
     }
-    cuts.push_back(tasks.size());
+    cuts.push_back(n);
   }
-  h->last = SolverStats();
-  const bool keep = h->opt.keep_displacements != 0;
-  h->solver.clear_kept();
-  for (size_t c = 0; c + 1 < cuts.size(); ++c) {
-    if (cuts[c] == cuts[c + 1]) continue;
-    std::vector<DomainTask> chunk(tasks.begin() + cuts[c], tasks.begin() + cuts[c + 1]);
-    // the adjoint keeps the last chunk on the device and checkpoints the others to the host
-    h->solver.set_keep(!keep ? kKeepNone : (c + 2 == cuts.size() ? kKeepDevice : kKeepHost));
-    int rc = h->solver.solve(chunk, h->opt, in[0].nu, h->err);
-    if (rc != DTC_OK) return (dtc_status)rc;
-    const SolverStats& ss = h->solver.stats();
-    h->last.ms_solve += ss.ms_solve;
-    h->last.ms_wall += ss.ms_wall;
-    h->last.kernel_launches += ss.kernel_launches;
-    h->last.dof_iterations += ss.dof_iterations;
-    for (int q = 0; q < kcNumClasses; ++q) {
-      h->last.kc[q].name = ss.kc[q].name;
-      h->last.kc[q].launches += ss.kc[q].launches;
-      h->last.kc[q].ms += ss.kc[q].ms;
-      h->last.kc[q].bytes += ss.kc[q].bytes;
-      h->last.kc[q].flops += ss.kc[q].flops;
+  // host phase of pass c: plans, output headers, solvable tasks, packed batch
+  struct Stage {
+    std::vector<DomainTask> tasks;
+    HostBatchPtr batch;
+    int rc = DTC_OK;
+    std::string msg;
+  };
+  auto host_stage = [&](size_t c, Stage& st) {
+    const int64_t a = cuts[c], b = cuts[c + 1];
+    plan_all(in + a, b - a, plans.data() + a, want_fields, h->opt.host_threads);
+    for (int64_t i = a; i < b; ++i) {
+      dtc_domain_out* o = &out[i];
+      double* keep_d = o->displ;
+      double* keep_f = o->force;
+      std::memset(o, 0, sizeof(*o));
+      o->displ = keep_d; o->force = keep_f;
+      o->domain_number = in[i].domain_number;
+      o->status = plans[i].status;
+      o->ne = plans[i].ne; o->nn = plans[i].nn; o->nb = plans[i].nb;
+      o->n_free_dof = plans[i].n_free_dof;
+      if (plans[i].status == DTC_DOMAIN_OK) st.tasks.push_back(DomainTask{&in[i], &plans[i], o, i});
     }
+    st.rc = DeviceSolver::prepare(st.tasks, h->opt, in[0].nu, st.batch, st.msg);
+  };
+  h->last = SolverStats();
+  h->solver.clear_kept();
+  std::vector<DomainTask> tasks;
+  const size_t npass = cuts.size() - 1;
+  Stage cur;
+  host_stage(0, cur);
+  for (size_t c = 0; c < npass; ++c) {
+    Stage next;
+    std::thread ahead;
+    if (c + 1 < npass) ahead = std::thread(host_stage, c + 1, std::ref(next));
+    int rc = cur.rc;
+    if (rc != DTC_OK) h->err = cur.msg;
+    const bool work = rc == DTC_OK && !cur.tasks.empty();
+    if (work) {
+      // the adjoint keeps the last pass on the device and checkpoints the others to the host
+      h->solver.set_keep(!keep ? kKeepNone : (c + 1 == npass ? kKeepDevice : kKeepHost));
+      rc = h->solver.solve(cur.tasks, h->opt, in[0].nu, std::move(cur.batch), h->err);
+    }
+    if (ahead.joinable()) ahead.join();
+    if (rc != DTC_OK) return (dtc_status)rc;
+    if (work) {
+      const SolverStats& ss = h->solver.stats();
+      h->last.ms_solve += ss.ms_solve;
+      h->last.ms_wall += ss.ms_wall;
+      h->last.kernel_launches += ss.kernel_launches;
+      h->last.dof_iterations += ss.dof_iterations;
+      for (int q = 0; q < kcNumClasses; ++q) {
+        h->last.kc[q].name = ss.kc[q].name;
+        h->last.kc[q].launches += ss.kc[q].launches;
+        h->last.kc[q].ms += ss.kc[q].ms;
+        h->last.kc[q].bytes += ss.kc[q].bytes;
+        h->last.kc[q].flops += ss.kc[q].flops;
+      }
+    }
+    tasks.insert(tasks.end(), cur.tasks.begin(), cur.tasks.end());
+    cur = std::move(next);
   }
   std::vector<const double*> ees;
   std::vector<dtc_domain_out*> rot_out;

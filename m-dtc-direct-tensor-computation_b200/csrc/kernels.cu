@@ -1527,70 +1527,36 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
 }
 }  // namespace
 
-template <int NEN>
-int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask>& tasks, const dtc_options& opt,
-              double nu, int keep, std::string& msg) {
-  DTC_CUDA(cudaSetDevice(I.device));
-  cudaStream_t s = I.stream;
-  stats_ = SolverStats();
-  static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
-                                             "direction_f32", "direction_f64", "colstate", "reaction_f64",
-                                             "project_f64", "mg_jacobi_f32", "mg_residual_f32",
-                                             "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
-                                             "host_pack", "host_multigrid_build"};
-  for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
-  I.stats = &stats_;
-  I.profile = opt.profile_kernels != 0;
-  I.tensor_matvec = opt.mixed_matvec == 1;
-  I.graphs = opt.graph_chunks == 0;
-  I.pending.clear();
-  I.h_active.clear();
-  I.dom_mv_bytes.clear(); I.dom_mv_flops.clear(); I.dom_vec_bytes.clear();
-  // constant tables
-  {
-    double kh[576];
-    float kh32[576];
-    voxel_stiffness(8, nu, kh);
-    for (int i = 0; i < 576; ++i) kh32[i] = (float)kh[i];
-    double uu[8 * 3 * 24];
-    macro_modes(1e-6, uu);   // the hard-coded boundary eps (mod_write_deck.f90:61)
-    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat64, kh, sizeof(kh), 0, cudaMemcpyHostToDevice, s));
-    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
-    DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
-    if (int e = upload_tc_operand(kh, s, msg)) return e;
-    if (NEN == 20) {
-      std::vector<double> k20(3600);
-      std::vector<float> k20f(3600);
-      voxel_stiffness(20, nu, k20.data());
-      for (int i = 0; i < 3600; ++i) k20f[i] = (float)k20[i];
-      DTC_CUDA(cudaMemcpyToSymbolAsync(c_k20_64, k20.data(), sizeof(double) * 3600, 0, cudaMemcpyHostToDevice, s));
-      // the element kernel stages the matrix from global memory: FP64 then FP32 copy
-      if (int e = ensure(I, bKe20, sizeof(double) * 3600 + sizeof(float) * 3600, msg)) return e;
-      DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20], k20.data(), sizeof(double) * 3600, cudaMemcpyHostToDevice, s));
-      DTC_CUDA(cudaMemcpyAsync(B<double>(I, bKe20) + 3600, k20f.data(), sizeof(float) * 3600, cudaMemcpyHostToDevice,
-                               s));
-      if (I.tensor_matvec) {   // HEX20 FP32 applications on the tensor cores
-        std::vector<float> img(tc20_operand_bytes() / sizeof(float));
-        build_tc20_operand(k20.data(), img.data());
-        if (int e = ensure(I, bKe20tc, tc20_operand_bytes(), msg)) return e;
-        DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20tc], img.data(), tc20_operand_bytes(), cudaMemcpyHostToDevice, s));
-        if (int e = allow_ebe_tc(msg)) return e;
-      }
-      DTC_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
-    }
-    if constexpr (NEN == 20)
-      if (int e = allow_all_ebe<NEN>(msg)) return e;   // per device, cheap
-  }
-  // pack the batch (all solvable tasks at once; chunking by memory happens in the caller)
-  const auto tpack = std::chrono::steady_clock::now();
-  using EL = Elem<NEN>;
-  constexpr int m = EL::M;
+// Host side of one device pass: the packed voxel factors, domain records and work lists of
+// the solvable tasks, and the multigrid plan of a mixed multigrid solve.  Built by
+// DeviceSolver::prepare, which touches no device state (it may run on a host thread while the
+// solver executes an earlier pass), and consumed by DeviceSolver::solve.
+struct HostBatch {
+  int nen = 0;
+  std::vector<int64_t> tidx;   // tasks solved in this pass
   std::vector<DomDev> doms;
   std::vector<Tile> tiles_i, tiles_a, bricks_i, bricks_a;
   std::vector<int64_t> nodes_i;
   std::vector<float> svox;
-  std::vector<int64_t> tidx;
   int64_t node_total = 0;
+  std::vector<double> dom_vec, dom_mv, dom_fl;   // per-domain algorithmic work of one launch
+  bool has_mg = false;
+  MgPlan mg;
+  double ms_pack = 0, ms_mg = 0;
+};
+void HostBatchDeleter::operator()(HostBatch* p) const { delete p; }
+
+template <int NEN>
+int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, HostBatch& hb) {
+  const auto tpack = std::chrono::steady_clock::now();
+  using EL = Elem<NEN>;
+  constexpr int m = EL::M;
+  std::vector<DomDev>& doms = hb.doms;
+  std::vector<Tile>&tiles_i = hb.tiles_i, &tiles_a = hb.tiles_a, &bricks_i = hb.bricks_i, &bricks_a = hb.bricks_a;
+  std::vector<int64_t>& nodes_i = hb.nodes_i;
+  std::vector<float>& svox = hb.svox;
+  std::vector<int64_t>& tidx = hb.tidx;
+  int64_t& node_total = hb.node_total;
   // which tasks are solved here, and each domain's voxel and node offsets (serial, cheap)
   for (size_t k = 0; k < tasks.size(); ++k)
     if (tasks[k].plan->status == DTC_DOMAIN_OK) tidx.push_back((int64_t)k);
@@ -1710,9 +1676,90 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     bricks_i.insert(bricks_i.end(), q.bi.begin(), q.bi.end());
     bricks_a.insert(bricks_a.end(), q.ba.begin(), q.ba.end());
     nodes_i.insert(nodes_i.end(), q.ni.begin(), q.ni.end());
-    I.dom_vec_bytes.push_back(q.vec);
-    I.dom_mv_bytes.push_back(q.mv);
-    I.dom_mv_flops.push_back(q.fl);
+    hb.dom_vec.push_back(q.vec);
+    hb.dom_mv.push_back(q.mv);
+    hb.dom_fl.push_back(q.fl);
+  }
+  hb.ms_pack = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tpack).count();
+  // multigrid plan of the mixed inner solve (HEX08 levels; HEX20 starts with p-coarsening)
+  if (opt.precision == DTC_PREC_MIXED && opt.inner_precond == 2 && !tiles_i.empty()) {
+    const auto tb = std::chrono::steady_clock::now();
+    build_mg(hb.mg, doms, svox, tiles_i, nu, NEN, opt.host_threads);
+    hb.has_mg = true;
+    hb.ms_mg = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+  }
+  return DTC_OK;
+}
+
+template <int NEN>
+int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask>& tasks, const dtc_options& opt,
+              double nu, int keep, HostBatch& hb, std::string& msg) {
+  DTC_CUDA(cudaSetDevice(I.device));
+  cudaStream_t s = I.stream;
+  stats_ = SolverStats();
+  static const char* kNames[kcNumClasses] = {"matvec_f32", "matvec_f64", "update_f32", "update_f64",
+                                             "direction_f32", "direction_f64", "colstate", "reaction_f64",
+                                             "project_f64", "mg_jacobi_f32", "mg_residual_f32",
+                                             "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
+                                             "host_pack", "host_multigrid_build"};
+  for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
+  I.stats = &stats_;
+  I.profile = opt.profile_kernels != 0;
+  I.tensor_matvec = opt.mixed_matvec == 1;
+  I.graphs = opt.graph_chunks == 0;
+  I.pending.clear();
+  I.h_active.clear();
+  I.dom_mv_bytes.clear(); I.dom_mv_flops.clear(); I.dom_vec_bytes.clear();
+  // constant tables
+  {
+    double kh[576];
+    float kh32[576];
+    voxel_stiffness(8, nu, kh);
+    for (int i = 0; i < 576; ++i) kh32[i] = (float)kh[i];
+    double uu[8 * 3 * 24];
+    macro_modes(1e-6, uu);   // the hard-coded boundary eps (mod_write_deck.f90:61)
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat64, kh, sizeof(kh), 0, cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
+    if (int e = upload_tc_operand(kh, s, msg)) return e;
+    if (NEN == 20) {
+      std::vector<double> k20(3600);
+      std::vector<float> k20f(3600);
+      voxel_stiffness(20, nu, k20.data());
+      for (int i = 0; i < 3600; ++i) k20f[i] = (float)k20[i];
+      DTC_CUDA(cudaMemcpyToSymbolAsync(c_k20_64, k20.data(), sizeof(double) * 3600, 0, cudaMemcpyHostToDevice, s));
+      // the element kernel stages the matrix from global memory: FP64 then FP32 copy
+      if (int e = ensure(I, bKe20, sizeof(double) * 3600 + sizeof(float) * 3600, msg)) return e;
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20], k20.data(), sizeof(double) * 3600, cudaMemcpyHostToDevice, s));
+      DTC_CUDA(cudaMemcpyAsync(B<double>(I, bKe20) + 3600, k20f.data(), sizeof(float) * 3600, cudaMemcpyHostToDevice,
+                               s));
+      if (I.tensor_matvec) {   // HEX20 FP32 applications on the tensor cores
+        std::vector<float> img(tc20_operand_bytes() / sizeof(float));
+        build_tc20_operand(k20.data(), img.data());
+        if (int e = ensure(I, bKe20tc, tc20_operand_bytes(), msg)) return e;
+        DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20tc], img.data(), tc20_operand_bytes(), cudaMemcpyHostToDevice, s));
+        if (int e = allow_ebe_tc(msg)) return e;
+      }
+      DTC_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
+    }
+    if constexpr (NEN == 20)
+      if (int e = allow_all_ebe<NEN>(msg)) return e;   // per device, cheap
+  }
+  // the host side of the pass (prepare_nen)
+  const auto tpack = std::chrono::steady_clock::now();
+  std::vector<DomDev>& doms = hb.doms;
+  std::vector<Tile>&tiles_i = hb.tiles_i, &tiles_a = hb.tiles_a, &bricks_i = hb.bricks_i, &bricks_a = hb.bricks_a;
+  std::vector<int64_t>& nodes_i = hb.nodes_i;
+  std::vector<float>& svox = hb.svox;
+  const std::vector<int64_t>& tidx = hb.tidx;
+  const int64_t node_total = hb.node_total;
+  I.dom_vec_bytes = hb.dom_vec;
+  I.dom_mv_bytes = hb.dom_mv;
+  I.dom_mv_flops = hb.dom_fl;
+  stats_.kc[kcHostPack].ms += hb.ms_pack;
+  if (hb.has_mg) {
+    stats_.kc[kcHostMgBuild].ms += hb.ms_mg;
+    stats_.kc[kcHostMgBuild].launches += 1;
   }
   const int ndom = (int)doms.size();
   if (ndom == 0) return DTC_OK;
@@ -1823,10 +1870,14 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     MgPlan mgp;
     MgDev mgd{};
     if (use_mg) {
-      const auto tb = std::chrono::steady_clock::now();
-      build_mg(mgp, doms, svox, tiles_i, nu, NEN, opt.host_threads);
-      stats_.kc[kcHostMgBuild].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
-      stats_.kc[kcHostMgBuild].launches += 1;
+      if (hb.has_mg) {
+        mgp = std::move(hb.mg);
+      } else {
+        const auto tb = std::chrono::steady_clock::now();
+        build_mg(mgp, doms, svox, tiles_i, nu, NEN, opt.host_threads);
+        stats_.kc[kcHostMgBuild].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+        stats_.kc[kcHostMgBuild].launches += 1;
+      }
       const int64_t cn = std::max<int64_t>(mgp.nodes, 1);
       if ((e = ensure(I, bZ32, vbytes32, msg)) || (e = ensure(I, bT32, vbytes32, msg)) ||
           (e = ensure(I, bMgDoms, sizeof(DomDev) * mgp.doms.size(), msg)) ||
@@ -2026,18 +2077,34 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   return DTC_OK;
 }
 
-int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg) {
+int DeviceSolver::prepare(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, HostBatchPtr& out,
+                          std::string& msg) {
   int nen = 0;
   for (const DomainTask& t : tasks) {
     if (t.plan->status != DTC_DOMAIN_OK) continue;
     if (nen && t.in->elem_type != nen) { msg = "all domains of one solve must share the element type"; return DTC_ERR_INVALID_ARGUMENT; }
     nen = t.in->elem_type;
   }
+  out.reset(new (std::nothrow) HostBatch());
+  if (!out) return DTC_ERR_OUT_OF_MEMORY;
+  out->nen = nen;
   if (nen == 0) return DTC_OK;
+  return nen == 20 ? prepare_nen<20>(tasks, opt, nu, *out) : prepare_nen<8>(tasks, opt, nu, *out);
+}
+
+int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, HostBatchPtr batch,
+                        std::string& msg) {
+  if (!batch || batch->nen == 0) return DTC_OK;
   DTC_CUDA(cudaSetDevice(impl_->device));
   impl_->adj_nu = nu;
-  return nen == 20 ? solve_nen<20>(*impl_, stats_, tasks, opt, nu, keep_, msg)
-                   : solve_nen<8>(*impl_, stats_, tasks, opt, nu, keep_, msg);
+  return batch->nen == 20 ? solve_nen<20>(*impl_, stats_, tasks, opt, nu, keep_, *batch, msg)
+                          : solve_nen<8>(*impl_, stats_, tasks, opt, nu, keep_, *batch, msg);
+}
+
+int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg) {
+  HostBatchPtr batch;
+  if (int e = prepare(tasks, opt, nu, batch, msg)) return e;
+  return solve(tasks, opt, nu, std::move(batch), msg);
 }
 
 void DeviceSolver::clear_kept() {

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -56,6 +57,13 @@ struct SolverStats {
   KernelClass kc[kcNumClasses];
 };
 
+// Host side of one device pass (packed domains, work lists, multigrid plan); kernels.cu.
+struct HostBatch;
+struct HostBatchDeleter {
+  void operator()(HostBatch* p) const;
+};
+using HostBatchPtr = std::unique_ptr<HostBatch, HostBatchDeleter>;
+
 class DeviceSolver {
  public:
   struct Impl;  // device buffers and stream (kernels.cu)
@@ -65,6 +73,13 @@ class DeviceSolver {
   int init(int device, std::string& msg);
   // Solve every task (status OK plans only), fill ff/iters/relres of the outputs.
   int solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, std::string& msg);
+  // The same in two phases.  prepare: host work only (voxel factors, work lists, multigrid
+  // plan), no device state, so it may run on another thread while a solver executes an
+  // earlier pass.  solve: the device work of a prepared pass of the same tasks.
+  static int prepare(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, HostBatchPtr& out,
+                     std::string& msg);
+  int solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, HostBatchPtr batch,
+            std::string& msg);
   // Adjoint: dL/dE_voxel for the domains of the last solve (kept displacements).
   int energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, std::string& msg);
   const SolverStats& stats() const { return stats_; }

@@ -274,3 +274,28 @@ def test_hex20_tensor_core_matches_oracle(dtc, batch20, precond):
     for r, ref in zip(res, refs):
         assert r["status"] == 0
         assert rel(r["c"], ref["c"]) <= TOL_MIXED
+
+
+@pytest.mark.parametrize("precision,precond,rtol", [("fp64", "block", 1e-10), ("mixed", "mg", 1e-8)])
+def test_pipelined_passes_match_one_pass(dtc, precision, precond, rtol):
+    """A batch of >= 256 domains is solved in 2 device passes, the host phase of the second
+    overlapping the device work of the first; keep_displacements keeps one pass.  Same tensors, FP64
+    iteration counts within 2, same statuses."""
+    syn = dtc.synth
+    rng = np.random.default_rng(17)
+    doms = [dtc.Domain(syn.bone_volume((8, 8, 8), float(rng.uniform(0.15, 0.45)), syn.seed_for(12, i)),
+                       E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, domain_number=i) for i in range(300)]
+    doms[7] = dtc.Domain(np.zeros((8, 8, 8), np.int16), E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, domain_number=7)
+    out = {}
+    for keep in (False, True):
+        with dtc.Solver(precision=precision, rtol=rtol, inner_precond=precond, rotation_search=True,
+                        keep_displacements=keep, estimator="energy" if precision == "mixed" else "reaction") as s:
+            out[keep] = s.solve(doms)
+    for a, b in zip(out[False], out[True]):
+        assert a["status"] == b["status"]
+        assert (a["ne"], a["nn"], a["nb"], a["domain_number"]) == (b["ne"], b["nn"], b["nb"], b["domain_number"])
+        if b["status"] == 0:
+            assert rel(a["c"], b["c"]) <= (1e-9 if precision == "fp64" else 1e-6)
+            if precision == "fp64":
+                assert np.abs(a["iters"] - b["iters"]).max() <= 2   # atomic reduction order, as vs the oracle
+    assert out[True][7]["status"] != 0
