@@ -460,7 +460,8 @@ __global__ void __launch_bounds__(kThreads) k_initial_dots(const Tile* __restric
 // Column state at the start of a solve (KSPSolve_CG before its loop + KSPConvergedDefault
 // at n = 0).  ttol = max(rtol * dp0, floor[col]) with floor = 1e-50 (abstol) when absent.
 __global__ void k_colstate_init(ColState* __restrict__ st, double* __restrict__ acc_zz, double* __restrict__ acc_zr,
-                                int* __restrict__ dom_active, double rtol, const double* __restrict__ floor_abs) {
+                                int* __restrict__ dom_active, double rtol, const double* __restrict__ floor_abs,
+                                float* __restrict__ dirf) {
   const int d = blockIdx.x, lc = threadIdx.x;
   int act = 0;
   if (lc < kNLC) {
@@ -479,6 +480,7 @@ __global__ void k_colstate_init(ColState* __restrict__ st, double* __restrict__ 
       else { s.reason = kIterating; s.active = 1; }
     }
     st[col] = s;
+    if (dirf) dirf[col] = s.active ? (float)s.bfac : NAN;
     acc_zz[col] = 0.0; acc_zr[col] = 0.0;
     act = s.active;
   }
@@ -488,7 +490,8 @@ __global__ void k_colstate_init(ColState* __restrict__ st, double* __restrict__ 
 
 // End of one CG iteration for every column (the tail of KSPSolve_CG's loop body).
 __global__ void k_colstate(ColState* __restrict__ st, double* __restrict__ acc_pw, double* __restrict__ acc_zz,
-                           double* __restrict__ acc_zr, int* __restrict__ dom_active, int64_t max_it) {
+                           double* __restrict__ acc_zr, int* __restrict__ dom_active, int64_t max_it,
+                           float* __restrict__ dirf) {
   const int d = blockIdx.x, lc = threadIdx.x;
   int act = 0;
   if (lc < kNLC) {
@@ -517,11 +520,25 @@ __global__ void k_colstate(ColState* __restrict__ st, double* __restrict__ acc_p
       }
       st[col] = s;
     }
+    if (dirf) dirf[col] = s.active ? (float)s.bfac : NAN;
     acc_pw[col] = 0.0; acc_zz[col] = 0.0; acc_zr[col] = 0.0;
     act = s.active;
   }
   act = __syncthreads_or(act);
   if (threadIdx.x == 0) dom_active[d] = act;
+}
+
+// Step length of every column once p.w is complete (KSPSolve_CG: a = beta / (p.w), 0 for
+// columns that stopped or whose curvature changed sign), as floats for the flat update.
+__global__ void k_alpha(const ColState* __restrict__ st, const double* __restrict__ acc_pw, float* __restrict__ alphaf,
+                        const int* __restrict__ dom_active) {
+  const int d = blockIdx.x, lc = threadIdx.x;
+  if (lc >= kNLC || (dom_active && !dom_active[d])) return;
+  const int64_t col = (int64_t)d * kNLC + lc;
+  const ColState s = st[col];
+  const double pw = acc_pw[col];
+  const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0) || pw == 0.0);
+  alphaf[col] = (s.active && pw != 0.0 && !flip) ? (float)(s.beta / pw) : 0.f;
 }
 
 __global__ void k_count_active(const int* __restrict__ dom_active, int ndom, int* __restrict__ count) {
@@ -808,7 +825,7 @@ namespace {
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
-           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bNumBufs };
+           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -1401,7 +1418,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
   if (nti > 0) k_initial_dots<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, zz, zr, nullptr);
-  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs);
+  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs, nullptr);
   launches += 2;
   if (int e = launch_check(msg)) return e;
   const int chunk = 32;
@@ -1431,7 +1448,7 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
           nl += 3;
         }
         const int q = I.begin(0);
-        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it, nullptr);
         I.end(kcColstate, q, 0, 0);
         nl += 1;
       }
@@ -1469,6 +1486,8 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   double* zr = B<double>(I, bZr);
   int* act = B<int>(I, bDomAct);
   int* cnt = B<int>(I, bCount);
+  float* dirf = B<float>(I, bDirF);      // per column: direction factor (NaN: column stopped)
+  float* alphaf = B<float>(I, bAlphaF);  // per column: step length of the current iteration
   const int64_t nitems = 6 * W.nnodes;
   const unsigned gflat = (unsigned)std::max<int64_t>((nitems + 255) / 256, 1);
   const dim3 grid((unsigned)(3 * nti));
@@ -1476,7 +1495,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
   mg_vcycle(I, M, 0, r, zz, zr, nullptr, launches);
-  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs);
+  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs, dirf);
   launches += 1;
   if (int e = launch_check(msg)) return e;
   const int chunk = 16;
@@ -1490,7 +1509,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
       for (int k = 0; k < chunk; ++k) {
         if (nti > 0) {
           int q = I.begin(0);
-          k_direction_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, M.z0, p, st, act);
+          k_direction_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, M.z0, p, dirf, act);
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
           if (NEN == 8 && I.tensor_matvec)
@@ -1499,13 +1518,14 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
             apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
-          k_update_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, x, r, p, w, st, pw, M.binv0, M.P->omega0, M.t0, act);
+          k_alpha<<<ndom, 32, 0, s>>>(st, pw, alphaf, act);
+          k_update_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, x, r, p, w, alphaf, M.binv0, M.P->omega0, M.t0, act);
           I.end(kcUpdate32, q, 7 * vb + vb / 12, 0);
           mg_vcycle(I, M, 0, r, zz, zr, act, nl, true);
-          nl += 3;
+          nl += 4;
         }
         const int q = I.begin(0);
-        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it);
+        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it, dirf);
         I.end(kcColstate, q, 0, 0);
         nl += 1;
       }
@@ -1796,6 +1816,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   if ((e = ensure(I, bZz, sizeof(double) * ncol, msg))) return e;
   if ((e = ensure(I, bZr, sizeof(double) * ncol, msg))) return e;
   if ((e = ensure(I, bTarget, sizeof(double) * ncol, msg))) return e;
+  if ((e = ensure(I, bDirF, sizeof(float) * ncol, msg))) return e;
+  if ((e = ensure(I, bAlphaF, sizeof(float) * ncol, msg))) return e;
   if ((e = ensure(I, bDomAct, sizeof(int) * ndom, msg))) return e;
   if ((e = ensure(I, bCount, sizeof(int), msg))) return e;
   if ((e = ensure(I, bFf, sizeof(double) * 576 * ndom, msg))) return e;

@@ -385,10 +385,11 @@ __device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// p = z + bfac p for the iterating columns (others keep p)
+// p = z + bfac p for the iterating columns (others keep p); dirf: bfac per column, NaN for a
+// column that stopped
 __global__ void __launch_bounds__(256) k_direction_flat(const int64_t* __restrict__ list, int64_t nitems,
                                                         const float* __restrict__ z, float* __restrict__ p,
-                                                        const ColState* __restrict__ st,
+                                                        const float* __restrict__ dirf,
                                                         const int* __restrict__ dom_active) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nitems) return;
@@ -398,13 +399,10 @@ __global__ void __launch_bounds__(256) k_direction_flat(const int64_t* __restric
   const int64_t node = e & kListNodeMask;
   const int lc0 = 4 * (int)(i % 6);
   float bf[4];
+  ld4(dirf + (int64_t)dom * kNLC + lc0, bf);
   bool on[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const ColState& c = st[(int64_t)dom * kNLC + lc0 + j];
-    on[j] = c.active != 0;
-    bf[j] = (float)c.bfac;
-  }
+  for (int j = 0; j < 4; ++j) on[j] = !isnan(bf[j]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const int64_t k = (node * 3 + c) * kNLC + lc0;
@@ -417,13 +415,12 @@ __global__ void __launch_bounds__(256) k_direction_flat(const int64_t* __restric
   }
 }
 
-// x += alpha p ; r -= alpha w for the valid columns (alpha = beta / p.w as in k_update), and
-// t = omega D^-1 r (first step of the next V-cycle) for all four
+// x += alpha p ; r -= alpha w (alpha per column from k_alpha, 0 for the columns that stopped),
+// and t = omega D^-1 r (first step of the next V-cycle) for all four
 __global__ void __launch_bounds__(256) k_update_flat(const int64_t* __restrict__ list, int64_t nitems,
                                                      float* __restrict__ x, float* __restrict__ r,
                                                      const float* __restrict__ p, const float* __restrict__ w,
-                                                     const ColState* __restrict__ st,
-                                                     const double* __restrict__ acc_pw,
+                                                     const float* __restrict__ alphaf,
                                                      const float* __restrict__ binv, float omega,
                                                      float* __restrict__ t_out, const int* __restrict__ dom_active) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -434,14 +431,7 @@ __global__ void __launch_bounds__(256) k_update_flat(const int64_t* __restrict__
   const int64_t node = e & kListNodeMask;
   const int lc0 = 4 * (int)(i % 6);
   float a[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int64_t col = (int64_t)dom * kNLC + lc0 + j;
-    const ColState s = st[col];
-    const double pw = acc_pw[col];
-    const bool flip = s.its > 0 && ((pw > 0) != (s.dpi > 0) || pw == 0.0);
-    a[j] = (s.active && pw != 0.0 && !flip) ? (float)(s.beta / pw) : 0.f;
-  }
+  ld4(alphaf + (int64_t)dom * kNLC + lc0, a);
   float rn[3][4];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -459,9 +449,9 @@ __global__ void __launch_bounds__(256) k_update_flat(const int64_t* __restrict__
     st4(x + k, xv);
     st4(r + k, rn[c]);
   }
-  const float* bq = binv + node * 6;
-  const float b0 = __ldg(bq), b1 = __ldg(bq + 1), b2 = __ldg(bq + 2), b3 = __ldg(bq + 3), b4 = __ldg(bq + 4),
-              b5 = __ldg(bq + 5);
+  const float2* bq = reinterpret_cast<const float2*>(binv + node * 6);   // 8-byte aligned
+  const float2 q0 = __ldg(bq), q1 = __ldg(bq + 1), q2 = __ldg(bq + 2);
+  const float b0 = q0.x, b1 = q0.y, b2 = q1.x, b3 = q1.y, b4 = q2.x, b5 = q2.y;
   float tv[3][4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
