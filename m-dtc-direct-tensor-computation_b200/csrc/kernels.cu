@@ -825,7 +825,8 @@ namespace {
 enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, bP64, bW64, bR32, bX32, bP32, bW32,
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
-           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF, bNumBufs };
+           bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF,
+           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -1372,8 +1373,10 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
 struct ChunkGraph {
   cudaGraphExec_t exec = nullptr;
   int64_t launches = 0;   // kernels in one chunk
-  ~ChunkGraph() {
+  ~ChunkGraph() { reset(); }
+  void reset() {   // the next run captures again (the work lists changed)
     if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
   }
   template <class Body>
   int run(cudaStream_t s, bool direct, int64_t& counter, Body&& body, std::string& msg) {
@@ -1472,12 +1475,109 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
 
 // FP32 CG preconditioned by one multigrid V-cycle per iteration (same column state machine
 // and stopping rule as run_cg, with z = B r in place of the Jacobi z).
+__device__ __forceinline__ int list_dom(const Tile& t) { return t.dom; }
+__device__ __forceinline__ int list_dom(int64_t e) { return (int)(e >> kListShift); }
+__device__ __forceinline__ int list_dom(int d) { return d; }
+
+// dst = the entries of src whose domain is still active; *count += their number.  The order
+// is kept inside a block of 256 entries (one atomic per block), not across blocks.
+template <typename E>
+__global__ void __launch_bounds__(256) k_compact(const E* __restrict__ src, int64_t n, const int* __restrict__ dom_active,
+                                                 E* __restrict__ dst, int* __restrict__ count) {
+  __shared__ int wbase[8];
+  __shared__ int base;
+  const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  E e{};
+  bool keep = false;
+  if (i < n) {
+    e = src[i];
+    keep = dom_active[list_dom(e)] != 0;
+  }
+  const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) wbase[warp] = __popc(ballot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int k = 0; k < 8; ++k) {
+      const int c = wbase[k];
+      wbase[k] = tot;
+      tot += c;
+    }
+    base = tot ? atomicAdd(count, tot) : 0;
+  }
+  __syncthreads();
+  if (keep) dst[base + wbase[warp] + __popc(ballot & ((1u << lane) - 1u))] = e;
+}
+
+template <typename E>
+void launch_compact(const E* src, int64_t n, const int* act, E* dst, int* count, cudaStream_t s) {
+  if (n > 0) k_compact<E><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, n, act, dst, count);
+}
+
+// The inner solve's work lists restricted to the domains still iterating, so that the CTAs of
+// converged domains are no longer launched (each launch of the full lists costs ~0.3 ms of
+// immediately returning CTAs on a 512-domain batch).  From the original lists (W, M) into the
+// compacted copies (Wc, Pc counts, Mc pointers); returns the launches made.
+int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev& M, const int* act, Work& Wc, MgPlan& Pc,
+                  MgDev& Mc, int64_t& launches, std::string& msg) {
+  cudaStream_t s = I.stream;
+  const MgPlan& P = *M.P;
+  const int nseg = 3 + 3 * P.nlev;
+  int e;
+  if ((e = ensure(I, bCompactCnt, sizeof(int) * nseg, msg))) return e;
+  if ((e = ensure(I, bTilesIc, sizeof(Tile) * std::max<int64_t>(W.nti, 1), msg))) return e;
+  if ((e = ensure(I, bNodesIc, sizeof(int64_t) * std::max<int64_t>(W.nnodes, 1), msg))) return e;
+  if ((e = ensure(I, bBricksIc, sizeof(Tile) * std::max<int64_t>(W.nbi, 1), msg))) return e;
+  if ((e = ensure(I, bMgTilesC, sizeof(Tile) * std::max<size_t>(P.tiles.size(), 1), msg))) return e;
+  if ((e = ensure(I, bMgListC, sizeof(int) * std::max<size_t>(P.lists.size(), 1), msg))) return e;
+  int* cnt = B<int>(I, bCompactCnt);
+  DTC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * nseg, s));
+  Tile* tc = B<Tile>(I, bTilesIc);
+  int64_t* nc = B<int64_t>(I, bNodesIc);
+  Tile* bc = B<Tile>(I, bBricksIc);
+  Tile* mt = B<Tile>(I, bMgTilesC);
+  int* ml = B<int>(I, bMgListC);
+  launch_compact(W.ti, W.nti, act, tc, cnt + 0, s);
+  launch_compact(W.nodes, W.nnodes, act, nc, cnt + 1, s);
+  launch_compact(W.bi, W.nbi, act, bc, cnt + 2, s);
+  for (int l = 0; l < P.nlev; ++l) {
+    launch_compact(M.tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 3 + 3 * l, s);
+    launch_compact(M.tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 4 + 3 * l, s);
+    launch_compact(M.lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 5 + 3 * l, s);
+  }
+  launches += nseg;
+  if ((e = launch_check(msg))) return e;
+  std::vector<int> h(nseg);
+  DTC_CUDA(cudaMemcpyAsync(h.data(), cnt, sizeof(int) * nseg, cudaMemcpyDeviceToHost, s));
+  DTC_CUDA(cudaStreamSynchronize(s));
+  Wc.ti = tc; Wc.nti = h[0];
+  Wc.nodes = nc; Wc.nnodes = h[1];
+  Wc.bi = bc; Wc.nbi = h[2];
+  Mc.bricks0 = bc; Mc.nbricks0 = h[2];
+  Mc.tiles = mt;
+  Mc.lists = ml;
+  for (int l = 0; l < P.nlev; ++l) {
+    Pc.sm_n[l] = h[3 + 3 * l];
+    Pc.in_n[l] = h[4 + 3 * l];
+    Pc.list_n[l] = h[5 + 3 * l];
+  }
+  return DTC_OK;
+}
+
 template <int NEN>
 int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, float* x, float* r, float* p, float* w,
               double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
   cudaStream_t s = I.stream;
-  const Tile* ti = W.ti;
-  const int64_t nti = W.nti;
+  // work lists: the full ones until half the domains have converged, then compacted copies
+  Work Wc = W;
+  MgPlan Pc;   // offsets and counts of the multigrid lists (no bulk data)
+  Pc.nlev = M.P->nlev; Pc.omega = M.P->omega; Pc.omega0 = M.P->omega0;
+  Pc.sm_off = M.P->sm_off; Pc.sm_n = M.P->sm_n; Pc.in_off = M.P->in_off; Pc.in_n = M.P->in_n;
+  Pc.list_off = M.P->list_off; Pc.list_n = M.P->list_n;
+  MgDev Mc = M;
+  Mc.P = &Pc;
+  int64_t listed = ndom;   // domains the current lists were compacted to
   const DomDev* dd = B<DomDev>(I, bDoms);
   const uint8_t* fl = B<uint8_t>(I, bFlags);
   ColState* st = B<ColState>(I, bSt);
@@ -1488,9 +1588,6 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   int* cnt = B<int>(I, bCount);
   float* dirf = B<float>(I, bDirF);      // per column: direction factor (NaN: column stopped)
   float* alphaf = B<float>(I, bAlphaF);  // per column: step length of the current iteration
-  const int64_t nitems = 6 * W.nnodes;
-  const unsigned gflat = (unsigned)std::max<int64_t>((nitems + 255) / 256, 1);
-  const dim3 grid((unsigned)(3 * nti));
   DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
@@ -1505,23 +1602,25 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
     const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(float) : 0;
     const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(float) : 0;
     const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
+    const int64_t nitems = 6 * Wc.nnodes;
+    const unsigned gflat = (unsigned)std::max<int64_t>((nitems + 255) / 256, 1);
     auto body = [&](int64_t& nl) {
       for (int k = 0; k < chunk; ++k) {
-        if (nti > 0) {
+        if (Wc.nti > 0) {
           int q = I.begin(0);
-          k_direction_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, M.z0, p, dirf, act);
+          k_direction_flat<<<gflat, 256, 0, s>>>(Wc.nodes, nitems, Mc.z0, p, dirf, act);
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
           if (NEN == 8 && I.tensor_matvec)
-            launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, p, w, pw, act, B<int>(I, bErr), s);
+            launch_matvec_tc(Wc.ti, Wc.nti, dd, B<float>(I, bSvox), fl, p, w, pw, act, B<int>(I, bErr), s);
           else
-            apply_k<float, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
+            apply_k<float, NEN, false, true>(Wc, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
           k_alpha<<<ndom, 32, 0, s>>>(st, pw, alphaf, act);
-          k_update_flat<<<gflat, 256, 0, s>>>(W.nodes, nitems, x, r, p, w, alphaf, M.binv0, M.P->omega0, M.t0, act);
+          k_update_flat<<<gflat, 256, 0, s>>>(Wc.nodes, nitems, x, r, p, w, alphaf, Mc.binv0, Pc.omega0, Mc.t0, act);
           I.end(kcUpdate32, q, 7 * vb + vb / 12, 0);
-          mg_vcycle(I, M, 0, r, zz, zr, act, nl, true);
+          mg_vcycle(I, Mc, 0, r, zz, zr, act, nl, true);
           nl += 4;
         }
         const int q = I.begin(0);
@@ -1541,6 +1640,11 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
     }
     DTC_CUDA(cudaStreamSynchronize(s));
     I.flush();
+    if (h_count > 0 && 2 * (int64_t)h_count <= listed) {
+      if (int e = compact_lists(I, W, M, act, Wc, Pc, Mc, launches, msg)) return e;
+      graph.reset();
+      listed = h_count;
+    }
   }
   I.h_active.clear();
   return DTC_OK;
