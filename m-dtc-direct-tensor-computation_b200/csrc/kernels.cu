@@ -1402,79 +1402,6 @@ struct ChunkGraph {
   }
 };
 
-template <typename T, bool BLOCK, int NEN>
-int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* w, const T* dinv,
-           double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
-  cudaStream_t s = I.stream;
-  const Tile* ti = W.ti;
-  const int64_t nti = W.nti;
-  const DomDev* dd = B<DomDev>(I, bDoms);
-  const uint8_t* fl = B<uint8_t>(I, bFlags);
-  ColState* st = B<ColState>(I, bSt);
-  double* pw = B<double>(I, bPw);
-  double* zz = B<double>(I, bZz);
-  double* zr = B<double>(I, bZr);
-  int* act = B<int>(I, bDomAct);
-  int* cnt = B<int>(I, bCount);
-  const dim3 grid((unsigned)(3 * nti));
-  DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
-  DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
-  DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
-  if (nti > 0) k_initial_dots<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, zz, zr, nullptr);
-  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs, nullptr);
-  launches += 2;
-  if (int e = launch_check(msg)) return e;
-  const int chunk = 32;
-  int h_count = 1;
-  ChunkGraph graph;
-  for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
-    const bool f32 = sizeof(T) == 4;
-    const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(T) : 0;
-    const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(T) : 0;
-    const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
-    auto body = [&](int64_t& nl) {
-      for (int k = 0; k < chunk; ++k) {
-        if (nti > 0) {
-          int q = I.begin(0);
-          k_direction<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
-          I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
-          q = I.begin(0);
-          if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
-            launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
-                             B<int>(I, bErr), s);
-          else
-            apply_k<T, NEN, false, true>(W, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
-          I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
-          q = I.begin(0);
-          k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
-          I.end(f32 ? kcUpdate32 : kcUpdate64, q, 6 * vb, 0);
-          nl += 3;
-        }
-        const int q = I.begin(0);
-        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it, nullptr);
-        I.end(kcColstate, q, 0, 0);
-        nl += 1;
-      }
-    };
-    if (int e = graph.run(s, I.profile || !I.graphs, launches, body, msg)) return e;
-    k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
-    launches += 1;
-    if (int e = launch_check(msg)) return e;
-    DTC_CUDA(cudaMemcpyAsync(&h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
-    if (I.profile) {
-      I.h_active.resize(ndom);
-      DTC_CUDA(cudaMemcpyAsync(I.h_active.data(), act, sizeof(int) * ndom, cudaMemcpyDeviceToHost, s));
-    }
-    DTC_CUDA(cudaStreamSynchronize(s));
-    I.flush();
-  }
-  I.h_active.clear();
-  return DTC_OK;
-}
-
-
-// FP32 CG preconditioned by one multigrid V-cycle per iteration (same column state machine
-// and stopping rule as run_cg, with z = B r in place of the Jacobi z).
 __device__ __forceinline__ int list_dom(const Tile& t) { return t.dom; }
 __device__ __forceinline__ int list_dom(int64_t e) { return (int)(e >> kListShift); }
 __device__ __forceinline__ int list_dom(int d) { return d; }
@@ -1515,14 +1442,15 @@ void launch_compact(const E* src, int64_t n, const int* act, E* dst, int* count,
   if (n > 0) k_compact<E><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, n, act, dst, count);
 }
 
-// The inner solve's work lists restricted to the domains still iterating, so that the CTAs of
-// converged domains are no longer launched (each launch of the full lists costs ~0.3 ms of
-// immediately returning CTAs on a 512-domain batch).  From the original lists (W, M) into the
-// compacted copies (Wc, Pc counts, Mc pointers); returns the launches made.
-int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev& M, const int* act, Work& Wc, MgPlan& Pc,
-                  MgDev& Mc, int64_t& launches, std::string& msg) {
+// The CG work lists restricted to the domains still iterating, so that the CTAs of converged
+// domains are no longer launched (each launch of the full lists costs ~0.3 ms of immediately
+// returning CTAs on a 512-domain batch).  From the original lists (W, and the multigrid lists
+// of M when given) into the compacted copies (Wc; Pc counts and Mc pointers).
+int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const int* act, Work& Wc, MgPlan* Pc,
+                  MgDev* Mc, int64_t& launches, std::string& msg) {
   cudaStream_t s = I.stream;
-  const MgPlan& P = *M.P;
+  static const MgPlan kNoLevels;
+  const MgPlan& P = M ? *M->P : kNoLevels;
   const int nseg = 3 + 3 * P.nlev;
   int e;
   if ((e = ensure(I, bCompactCnt, sizeof(int) * nseg, msg))) return e;
@@ -1542,9 +1470,9 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev& M, const in
   launch_compact(W.nodes, W.nnodes, act, nc, cnt + 1, s);
   launch_compact(W.bi, W.nbi, act, bc, cnt + 2, s);
   for (int l = 0; l < P.nlev; ++l) {
-    launch_compact(M.tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 3 + 3 * l, s);
-    launch_compact(M.tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 4 + 3 * l, s);
-    launch_compact(M.lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 5 + 3 * l, s);
+    launch_compact(M->tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 3 + 3 * l, s);
+    launch_compact(M->tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 4 + 3 * l, s);
+    launch_compact(M->lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 5 + 3 * l, s);
   }
   launches += nseg;
   if ((e = launch_check(msg))) return e;
@@ -1554,17 +1482,101 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev& M, const in
   Wc.ti = tc; Wc.nti = h[0];
   Wc.nodes = nc; Wc.nnodes = h[1];
   Wc.bi = bc; Wc.nbi = h[2];
-  Mc.bricks0 = bc; Mc.nbricks0 = h[2];
-  Mc.tiles = mt;
-  Mc.lists = ml;
-  for (int l = 0; l < P.nlev; ++l) {
-    Pc.sm_n[l] = h[3 + 3 * l];
-    Pc.in_n[l] = h[4 + 3 * l];
-    Pc.list_n[l] = h[5 + 3 * l];
+  if (M) {
+    Mc->bricks0 = bc; Mc->nbricks0 = h[2];
+    Mc->tiles = mt;
+    Mc->lists = ml;
+    for (int l = 0; l < P.nlev; ++l) {
+      Pc->sm_n[l] = h[3 + 3 * l];
+      Pc->in_n[l] = h[4 + 3 * l];
+      Pc->list_n[l] = h[5 + 3 * l];
+    }
   }
   return DTC_OK;
 }
 
+template <typename T, bool BLOCK, int NEN>
+int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* w, const T* dinv,
+           double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
+  cudaStream_t s = I.stream;
+  // work lists: the full ones until half the domains have converged, then compacted copies
+  Work Wc = W;
+  int64_t listed = ndom;
+  const DomDev* dd = B<DomDev>(I, bDoms);
+  const uint8_t* fl = B<uint8_t>(I, bFlags);
+  ColState* st = B<ColState>(I, bSt);
+  double* pw = B<double>(I, bPw);
+  double* zz = B<double>(I, bZz);
+  double* zr = B<double>(I, bZr);
+  int* act = B<int>(I, bDomAct);
+  int* cnt = B<int>(I, bCount);
+  DTC_CUDA(cudaMemsetAsync(zz, 0, sizeof(double) * ndom * kNLC, s));
+  DTC_CUDA(cudaMemsetAsync(zr, 0, sizeof(double) * ndom * kNLC, s));
+  DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
+  if (W.nti > 0)
+    k_initial_dots<T, BLOCK><<<(unsigned)(3 * W.nti), kThreads, 0, s>>>(W.ti, dd, fl, dinv, r, zz, zr, nullptr);
+  k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs, nullptr);
+  launches += 2;
+  if (int e = launch_check(msg)) return e;
+  const int chunk = 32;
+  int h_count = 1;
+  ChunkGraph graph;
+  for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
+    const bool f32 = sizeof(T) == 4;
+    const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(T) : 0;
+    const double mb = I.profile ? I.active_sum(I.dom_mv_bytes) * sizeof(T) : 0;
+    const double mf = I.profile ? I.active_sum(I.dom_mv_flops) : 0;
+    const Tile* ti = Wc.ti;
+    const int64_t nti = Wc.nti;
+    const dim3 grid((unsigned)(3 * std::max<int64_t>(nti, 1)));
+    auto body = [&](int64_t& nl) {
+      for (int k = 0; k < chunk; ++k) {
+        if (nti > 0) {
+          int q = I.begin(0);
+          k_direction<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, r, p, st, act);
+          I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
+          q = I.begin(0);
+          if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
+            launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
+                             B<int>(I, bErr), s);
+          else
+            apply_k<T, NEN, false, true>(Wc, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
+          I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
+          q = I.begin(0);
+          k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
+          I.end(f32 ? kcUpdate32 : kcUpdate64, q, 6 * vb, 0);
+          nl += 3;
+        }
+        const int q = I.begin(0);
+        k_colstate<<<ndom, 32, 0, s>>>(st, pw, zz, zr, act, max_it, nullptr);
+        I.end(kcColstate, q, 0, 0);
+        nl += 1;
+      }
+    };
+    if (int e = graph.run(s, I.profile || !I.graphs, launches, body, msg)) return e;
+    k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
+    launches += 1;
+    if (int e = launch_check(msg)) return e;
+    DTC_CUDA(cudaMemcpyAsync(&h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (I.profile) {
+      I.h_active.resize(ndom);
+      DTC_CUDA(cudaMemcpyAsync(I.h_active.data(), act, sizeof(int) * ndom, cudaMemcpyDeviceToHost, s));
+    }
+    DTC_CUDA(cudaStreamSynchronize(s));
+    I.flush();
+    if (h_count > 0 && 2 * (int64_t)h_count <= listed) {
+      if (int e = compact_lists(I, W, nullptr, act, Wc, nullptr, nullptr, launches, msg)) return e;
+      graph.reset();
+      listed = h_count;
+    }
+  }
+  I.h_active.clear();
+  return DTC_OK;
+}
+
+
+// FP32 CG preconditioned by one multigrid V-cycle per iteration (same column state machine
+// and stopping rule as run_cg, with z = B r in place of the Jacobi z).
 template <int NEN>
 int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, float* x, float* r, float* p, float* w,
               double rtol, const double* floor_abs, int64_t max_it, int64_t& launches, std::string& msg) {
@@ -1593,10 +1605,18 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   DTC_CUDA(cudaMemsetAsync(pw, 0, sizeof(double) * ndom * kNLC, s));
   mg_vcycle(I, M, 0, r, zz, zr, nullptr, launches);
   k_colstate_init<<<ndom, 32, 0, s>>>(st, zz, zr, act, rtol, floor_abs, dirf);
-  launches += 1;
+  k_count_active<<<1, 256, 0, s>>>(act, ndom, cnt);
+  launches += 2;
   if (int e = launch_check(msg)) return e;
   const int chunk = 16;
   int h_count = 1;
+  DTC_CUDA(cudaMemcpyAsync(&h_count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DTC_CUDA(cudaStreamSynchronize(s));
+  // a later refinement pass often starts with few domains still refining: lists to those
+  if (h_count > 0 && 2 * (int64_t)h_count <= listed) {
+    if (int e = compact_lists(I, W, &M, act, Wc, &Pc, &Mc, launches, msg)) return e;
+    listed = h_count;
+  }
   ChunkGraph graph;
   for (int64_t it = 0; it < max_it + 2 && h_count > 0; it += chunk) {
     const double vb = I.profile ? I.active_sum(I.dom_vec_bytes) * sizeof(float) : 0;
@@ -1641,7 +1661,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
     DTC_CUDA(cudaStreamSynchronize(s));
     I.flush();
     if (h_count > 0 && 2 * (int64_t)h_count <= listed) {
-      if (int e = compact_lists(I, W, M, act, Wc, Pc, Mc, launches, msg)) return e;
+      if (int e = compact_lists(I, W, &M, act, Wc, &Pc, &Mc, launches, msg)) return e;
       graph.reset();
       listed = h_count;
     }
