@@ -65,27 +65,37 @@ class Domain:
         self.elem_type = elem_type
 
 
-def _result(o, fields):
-    r = {
-        "status": o.status, "refine_steps": o.refine_steps, "domain_number": o.domain_number,
-        "ne": o.ne, "nn": o.nn, "nb": o.nb, "n_free_dof": o.n_free_dof,
-        "iters": np.array(o.iters[:]), "relres": np.array(o.relres[:]),
-        "ff": np.array(o.ff[:]).reshape(24, 24, order="F"),
-        "kmacro": np.array(o.kmacro[:]).reshape(24, 24, order="F"), "sym_k": o.sym_k,
-        "c": np.array(o.c[:]).reshape(6, 6, order="F"), "sym_c": o.sym_c,
-        "ee": np.array(o.ee[:]).reshape(6, 6, order="F"), "sym_ee": o.sym_ee,
-        "density": o.density,
-    }
-    for k in ("cr1", "cr2"):
-        r[k] = {"angle": getattr(o, k + "_angle"), "n": np.array(getattr(o, k + "_n")[:]),
-                "aa": np.array(getattr(o, k + "_aa")[:]).reshape(3, 3, order="F"),
-                "ee": np.array(getattr(o, k + "_ee")[:]).reshape(6, 6, order="F"),
-                "crit": getattr(o, k + "_crit"), "iters": getattr(o, k + "_iters")}
-    if fields is not None:
-        nn = o.nn
-        r["displ"] = fields[0][: 24 * 3 * nn].reshape(24, 3 * nn)
-        r["force"] = fields[1][: 24 * 3 * nn].reshape(24, 3 * nn)
-    return r
+_OUT_DTYPE = capi.numpy_dtype(capi.DomainOut)
+
+
+def _results(outs, keep):
+    """Result dicts of a dtc_domain_out array: each field copied once for the whole batch, then
+    per-domain rows (the 24 x 24 / 6 x 6 / 3 x 3 leaves are column-major, as in the record)."""
+    raw = (C.c_char * C.sizeof(outs)).from_buffer(outs)
+    a = np.frombuffer(raw, dtype=_OUT_DTYPE)
+    n = len(a)
+    sc = {k: a[k].tolist() for k in ("status", "refine_steps", "domain_number", "ne", "nn", "nb", "n_free_dof",
+                                      "sym_k", "sym_c", "sym_ee", "density", "cr1_angle", "cr1_crit", "cr1_iters",
+                                      "cr2_angle", "cr2_crit", "cr2_iters")}
+    ar = {k: np.array(a[k]) for k in ("iters", "relres", "cr1_n", "cr2_n")}
+    mat = {k: np.array(a[k]).reshape((n,) + shape[::-1]).transpose(0, 2, 1)
+           for k, shape in (("ff", (24, 24)), ("kmacro", (24, 24)), ("c", (6, 6)), ("ee", (6, 6)),
+                            ("cr1_aa", (3, 3)), ("cr1_ee", (6, 6)), ("cr2_aa", (3, 3)), ("cr2_ee", (6, 6)))}
+    res = []
+    for i in range(n):
+        r = {k: sc[k][i] for k in ("status", "refine_steps", "domain_number", "ne", "nn", "nb", "n_free_dof",
+                                    "sym_k", "sym_c", "sym_ee", "density")}
+        r.update(iters=ar["iters"][i], relres=ar["relres"][i], ff=mat["ff"][i], kmacro=mat["kmacro"][i],
+                 c=mat["c"][i], ee=mat["ee"][i])
+        for k in ("cr1", "cr2"):
+            r[k] = {"angle": sc[k + "_angle"][i], "n": ar[k + "_n"][i], "aa": mat[k + "_aa"][i],
+                    "ee": mat[k + "_ee"][i], "crit": sc[k + "_crit"][i], "iters": sc[k + "_iters"][i]}
+        if keep:
+            nn = r["nn"]
+            r["displ"] = keep[i][0][: 24 * 3 * nn].reshape(24, 3 * nn)
+            r["force"] = keep[i][1][: 24 * 3 * nn].reshape(24, 3 * nn)
+        res.append(r)
+    return res
 
 
 class Solver:
@@ -147,7 +157,7 @@ class Solver:
                 outs[i].displ = fd.ctypes.data_as(C.POINTER(C.c_double))
                 outs[i].force = ff_.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.dtc_solve_batch(self.handle, ins, n, outs))
-        return [_result(outs[i], keep[i] if want_fields else None) for i in range(n)]
+        return _results(outs, keep if want_fields else None)
 
     def stats(self):
         ms, launches, dofit = C.c_double(), C.c_int64(), C.c_double()

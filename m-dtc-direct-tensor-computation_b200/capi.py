@@ -4,6 +4,8 @@ The library is the product: if libdtc.so is missing or cannot be loaded this mod
 raises, it never falls back to a CPU implementation.
 """
 import ctypes as C
+
+import numpy as np
 from pathlib import Path
 
 PKG_DIR = Path(__file__).resolve().parent
@@ -56,6 +58,22 @@ class DomainOut(C.Structure):
         ("cr1_iters", C.c_int32), ("cr2_iters", C.c_int32), ("density", C.c_double),
         ("displ", C.POINTER(C.c_double)), ("force", C.POINTER(C.c_double)),
     ]
+
+
+def numpy_dtype(struct):
+    """numpy structured dtype with the field offsets of a ctypes Structure (pointers as uintp)."""
+    names, formats, offsets = [], [], []
+    scalar = {C.c_int32: "<i4", C.c_int64: "<i8", C.c_double: "<f8", C.c_float: "<f4", C.c_char: "S1"}
+    for name, ct in struct._fields_:
+        names.append(name)
+        offsets.append(getattr(struct, name).offset)
+        if hasattr(ct, "_length_") and hasattr(ct, "_type_") and ct._type_ in scalar:
+            formats.append((scalar[ct._type_], (ct._length_,)))
+        elif ct in scalar:
+            formats.append(scalar[ct])
+        else:   # pointer
+            formats.append("<u8")
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": C.sizeof(struct)})
 
 
 class KernelStats(C.Structure):
