@@ -83,3 +83,51 @@ def test_create_reports_missing_device_or_abi(dtc):
         assert lib.dtc_create(C.byref(h), C.byref(o)) == dtc.capi.DTC_ERR_NO_DEVICE
         with pytest.raises(dtc.DTCError):
             dtc.Solver()
+
+
+def test_result_records_convert_fieldwise(dtc):
+    """The batch conversion of dtc_domain_out records (one numpy view per field) gives what
+    element-wise reads of the ctypes records give; 24 x 24 / 6 x 6 / 3 x 3 leaves column-major."""
+    import sys
+    pkg = sys.modules[dtc.__name__]
+    cap = dtc.capi
+    dt = cap.numpy_dtype(cap.DomainOut)
+    assert dt.itemsize == C.sizeof(cap.DomainOut)
+    for name, _ in cap.DomainOut._fields_:
+        assert dt.fields[name][1] == getattr(cap.DomainOut, name).offset, name
+    n = 7
+    outs = (cap.DomainOut * n)()
+    rng = np.random.default_rng(2)
+    for i in range(n):
+        o = outs[i]
+        o.status, o.refine_steps, o.domain_number, o.ne, o.nn = -i, i + 1, 100 + i, 1000 * i, 77 + i
+        for k in range(576):
+            o.ff[k] = rng.standard_normal()
+            o.kmacro[k] = rng.standard_normal()
+        for k in range(24):
+            o.iters[k] = int(rng.integers(0, 1000))
+            o.relres[k] = rng.random()
+        for k in range(36):
+            o.c[k], o.ee[k], o.cr1_ee[k], o.cr2_ee[k] = rng.standard_normal(4)
+        for k in range(9):
+            o.cr1_aa[k], o.cr2_aa[k] = rng.standard_normal(2)
+        for k in range(3):
+            o.cr1_n[k], o.cr2_n[k] = rng.standard_normal(2)
+        o.density, o.sym_c, o.cr1_angle, o.cr2_crit, o.cr2_iters = rng.random(), rng.random(), 1.5, 2.5, 3 + i
+    res = pkg._results(outs, None)
+    for i, r in enumerate(res):
+        o = outs[i]
+        assert (r["status"], r["refine_steps"], r["domain_number"], r["ne"], r["nn"]) == (
+            o.status, o.refine_steps, o.domain_number, o.ne, o.nn)
+        assert np.array_equal(r["ff"], np.array(o.ff[:]).reshape(24, 24, order="F"))
+        assert np.array_equal(r["kmacro"], np.array(o.kmacro[:]).reshape(24, 24, order="F"))
+        assert np.array_equal(r["iters"], np.array(o.iters[:])) and r["iters"].dtype == np.int64
+        assert np.array_equal(r["relres"], np.array(o.relres[:]))
+        for k in ("c", "ee"):
+            assert np.array_equal(r[k], np.array(getattr(o, k)[:]).reshape(6, 6, order="F"))
+        for k in ("cr1", "cr2"):
+            assert np.array_equal(r[k]["ee"], np.array(getattr(o, k + "_ee")[:]).reshape(6, 6, order="F"))
+            assert np.array_equal(r[k]["aa"], np.array(getattr(o, k + "_aa")[:]).reshape(3, 3, order="F"))
+            assert np.array_equal(r[k]["n"], np.array(getattr(o, k + "_n")[:]))
+        assert r["density"] == o.density and r["sym_c"] == o.sym_c
+        assert r["cr1"]["angle"] == 1.5 and r["cr2"]["crit"] == 2.5 and r["cr2"]["iters"] == 3 + i
