@@ -5,6 +5,8 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -248,7 +250,7 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     int rc = DTC_OK;
     std::string msg;
   };
-  auto host_stage = [&](size_t c, Stage& st) {
+  auto host_stage_body = [&](size_t c, Stage& st) {
     const int64_t a = cuts[c], b = cuts[c + 1];
     plan_all(in + a, b - a, plans.data() + a, want_fields, h->opt.host_threads);
     for (int64_t i = a; i < b; ++i) {
@@ -264,6 +266,18 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
       if (plans[i].status == DTC_DOMAIN_OK) st.tasks.push_back(DomainTask{&in[i], &plans[i], o, i});
     }
     st.rc = DeviceSolver::prepare(st.tasks, h->opt, in[0].nu, st.batch, st.msg);
+  };
+  // the host stage may run on a worker thread: an exception there becomes the pass's status
+  auto host_stage = [&](size_t c, Stage& st) {
+    try {
+      host_stage_body(c, st);
+    } catch (const std::bad_alloc&) {
+      st.rc = DTC_ERR_OUT_OF_MEMORY;
+      st.msg = "host memory exhausted while preparing a device pass";
+    } catch (const std::exception& ex) {
+      st.rc = DTC_ERR_INTERNAL;
+      st.msg = std::string("preparing a device pass: ") + ex.what();
+    }
   };
   h->last = SolverStats();
   h->solver.clear_kept();
