@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import capi, synth
+from . import capi, puredat, synth
 from .capi import (DOMAIN_BREAKDOWN, DOMAIN_EMPTY, DOMAIN_FEW_NODES, DOMAIN_MAX_IT, DOMAIN_NO_STRUCTURE,
                    DOMAIN_NONFINITE, DOMAIN_OK, HEX08, HEX20, PREC_FP64, PREC_MIXED, DTCError)
 
