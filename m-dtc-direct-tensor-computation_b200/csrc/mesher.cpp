@@ -66,6 +66,28 @@ bool grid_on_boundary(const int64_t L[3], int nen, int64_t g) {
   return ix == 0 || ix == m * L[0] || iy == 0 || iy == m * L[1] || iz == 0 || iz == m * L[2];
 }
 
+namespace {
+
+// Bone voxels (gray >= llimit) in x-fastest scan order: their voxel index and coordinates,
+// and the element index of every voxel (-1 for none).
+template <typename P>
+void scan_bone(const P* phi, int64_t llimit, const int64_t L[3], std::vector<int32_t>& elem_of,
+               std::vector<int64_t>& evox, std::vector<int32_t>& exyz) {
+  int64_t v = 0;
+  for (int64_t z = 0; z < L[2]; ++z)
+    for (int64_t y = 0; y < L[1]; ++y)
+      for (int64_t x = 0; x < L[0]; ++x, ++v)
+        if ((int64_t)phi[v] >= llimit) {
+          elem_of[v] = (int32_t)evox.size();
+          evox.push_back(v);
+          exyz.push_back((int32_t)x);
+          exyz.push_back((int32_t)y);
+          exyz.push_back((int32_t)z);
+        }
+}
+
+}  // namespace
+
 int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp) {
   mp = MeshPlan();
   const int nen = in.elem_type;
@@ -76,30 +98,45 @@ int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp) {
   std::memcpy(mp.L, in.L, sizeof(mp.L));
   const int64_t L0 = in.L[0], L1 = in.L[1], L2 = in.L[2], nvox = L0 * L1 * L2;
 
-  // bone voxels in scan order = element order
+  // bone voxels in scan order = element order, with their coordinates
   std::vector<int32_t> elem_of(nvox, -1);
   std::vector<int64_t> evox;
-  for (int64_t v = 0; v < nvox; ++v)
-    if (gray_value(in, v) >= in.llimit) { elem_of[v] = (int32_t)evox.size(); evox.push_back(v); }
+  std::vector<int32_t> exyz;
+  evox.reserve(nvox);
+  exyz.reserve(3 * nvox);
+  switch (in.phi_type) {
+    case 1: scan_bone(static_cast<const int8_t*>(in.phi), in.llimit, in.L, elem_of, evox, exyz); break;
+    case 2: scan_bone(static_cast<const int16_t*>(in.phi), in.llimit, in.L, elem_of, evox, exyz); break;
+    default: scan_bone(static_cast<const int32_t*>(in.phi), in.llimit, in.L, elem_of, evox, exyz); break;
+  }
   if (evox.empty()) { mp.status = DTC_DOMAIN_EMPTY; return DTC_OK; }
   const int64_t ne0 = (int64_t)evox.size();
 
-  // node ids by first appearance
+  // node ids by first appearance; a node's boundary flag is known when its id is given
   const int64_t m = (nen == 8) ? 1 : 2;
   const int64_t gx = m * L0 + 1, gy = m * L1 + 1, gz = m * L2 + 1;
   std::vector<int64_t> id_of(gx * gy * gz, 0);
   std::vector<int64_t> grid_of_id(1, -1);   // 1-based
   std::vector<int32_t> first_elem_of_id(1, -1);
+  std::vector<uint8_t> bnd_of_id(1, 0);
+  const size_t nn_est = (size_t)std::min<int64_t>(gx * gy * gz, (int64_t)nen * ne0) + 1;
+  grid_of_id.reserve(nn_est);
+  first_elem_of_id.reserve(nn_est);
+  bnd_of_id.reserve(nn_est);
   const signed char(*loc)[3] = (nen == 8) ? kCorner : kRing;
   for (int64_t e = 0; e < ne0; ++e) {
-    const int64_t v = evox[e];
-    const int64_t vz = v / (L0 * L1), vy = (v / L0) % L1, vx = v % L0;
+    const int64_t vx = exyz[3 * e], vy = exyz[3 * e + 1], vz = exyz[3 * e + 2];
+    // the corners at the element's low x face were numbered by its x - 1 neighbour in the row
+    const bool run = vx > 0 && elem_of[evox[e] - 1] >= 0;
     for (int a = 0; a < nen; ++a) {
-      int64_t g = (m * vx + loc[a][0]) + gx * ((m * vy + loc[a][1]) + gy * (m * vz + loc[a][2]));
+      if (run && loc[a][0] == 0) continue;
+      const int64_t ix = m * vx + loc[a][0], iy = m * vy + loc[a][1], iz = m * vz + loc[a][2];
+      const int64_t g = ix + gx * (iy + gy * iz);
       if (id_of[g] == 0) {
         id_of[g] = (int64_t)grid_of_id.size();
         grid_of_id.push_back(g);
         first_elem_of_id.push_back((int32_t)e);
+        bnd_of_id.push_back(ix == 0 || ix == gx - 1 || iy == 0 || iy == gy - 1 || iz == 0 || iz == gz - 1);
       }
     }
   }
@@ -109,18 +146,30 @@ int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp) {
   UnionFind uf(ne0);
   int64_t bmin[3] = {L0, L1, L2}, bmax[3] = {-1, -1, -1};
   for (int64_t e = 0; e < ne0; ++e) {
-    const int64_t v = evox[e];
-    const int64_t vz = v / (L0 * L1), vy = (v / L0) % L1, vx = v % L0;
+    const int64_t vx = exyz[3 * e], vy = exyz[3 * e + 1], vz = exyz[3 * e + 2];
     const int64_t c[3] = {vx, vy, vz};
     for (int d = 0; d < 3; ++d) { bmin[d] = std::min(bmin[d], c[d]); bmax[d] = std::max(bmax[d], c[d]); }
+    int32_t root = (int32_t)e;   // e's root so far (it only joins sets of smaller roots)
+    // inside a run along x the neighbours at x - 1 and x are already in the set of the element
+    // before: join it, then only the neighbours at x + 1 are new
+    const bool run = vx > 0 && elem_of[evox[e] - 1] >= 0;
+    if (run) {
+      uf.unite(root, (int32_t)e - 1);
+      root = uf.find(root);
+    }
     for (int dz = -1; dz <= 0; ++dz)
       for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
+        for (int dx = run ? 1 : -1; dx <= 1; ++dx) {
           if (dz == 0 && (dy > 0 || (dy == 0 && dx >= 0))) continue;  // only earlier neighbours
-          int64_t x = vx + dx, y = vy + dy, z = vz + dz;
+          const int64_t x = vx + dx, y = vy + dy, z = vz + dz;
           if (x < 0 || y < 0 || z < 0 || x >= L0 || y >= L1) continue;
-          int32_t o = elem_of[x + L0 * (y + L1 * z)];
-          if (o >= 0) uf.unite((int32_t)e, o);
+          const int32_t o = elem_of[x + L0 * (y + L1 * z)];
+          if (o < 0) continue;
+          const int32_t ro = uf.find(o);
+          if (ro != root) {
+            uf.unite(root, ro);
+            root = uf.find(root);
+          }
         }
   }
   std::vector<int32_t> comp(ne0);
@@ -128,10 +177,8 @@ int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp) {
   // keep a region if it touches the bone bounding box; the first region always
   std::vector<uint8_t> keep_comp(ne0, 0);
   for (int64_t e = 0; e < ne0; ++e) {
-    const int64_t v = evox[e];
-    const int64_t c[3] = {v % L0, (v / L0) % L1, v / (L0 * L1)};
     bool touch = false;
-    for (int d = 0; d < 3; ++d) touch = touch || c[d] == bmin[d] || c[d] == bmax[d];
+    for (int d = 0; d < 3; ++d) touch = touch || exyz[3 * e + d] == bmin[d] || exyz[3 * e + d] == bmax[d];
     if (touch) keep_comp[comp[e]] = 1;
   }
   keep_comp[comp[0]] = 1;
@@ -151,16 +198,15 @@ int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp) {
   for (int64_t id = 1; id <= nn0; ++id) {
     if (keep_comp[comp[first_elem_of_id[id]]] || id == nn0) {
       new_id[id] = ++nn;
-      if (grid_on_boundary(in.L, nen, grid_of_id[id])) ++nb;
+      nb += bnd_of_id[id];
     }
   }
   if (mp.last_partial) {
     mp.last_grid = grid_of_id[nn0];
-    mp.last_on_boundary = grid_on_boundary(in.L, nen, mp.last_grid);
-    const int64_t v = evox[elast];
-    const int64_t vz = v / (L0 * L1), vy = (v / L0) % L1, vx = v % L0;
+    mp.last_on_boundary = bnd_of_id[nn0] != 0;
+    const int64_t vx = exyz[3 * elast], vy = exyz[3 * elast + 1], vz = exyz[3 * elast + 2];
     for (int a = 0; a < nen; ++a) {
-      int64_t g = (m * vx + loc[a][0]) + gx * ((m * vy + loc[a][1]) + gy * (m * vz + loc[a][2]));
+      const int64_t g = (m * vx + loc[a][0]) + gx * ((m * vy + loc[a][1]) + gy * (m * vz + loc[a][2]));
       if (g == mp.last_grid) mp.last_local = a;
     }
   }
@@ -173,10 +219,9 @@ int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp) {
     mp.elems.reserve(nen * ne);
     for (int64_t e = 0; e < ne0; ++e) {
       if (!keep_comp[comp[e]] && e != elast) continue;
-      const int64_t v = evox[e];
-      const int64_t vz = v / (L0 * L1), vy = (v / L0) % L1, vx = v % L0;
+      const int64_t vx = exyz[3 * e], vy = exyz[3 * e + 1], vz = exyz[3 * e + 2];
       for (int a = 0; a < nen; ++a) {
-        int64_t g = (m * vx + loc[a][0]) + gx * ((m * vy + loc[a][1]) + gy * (m * vz + loc[a][2]));
+        const int64_t g = (m * vx + loc[a][0]) + gx * ((m * vy + loc[a][1]) + gy * (m * vz + loc[a][2]));
         mp.elems.push_back(new_id[id_of[g]]);
       }
     }
