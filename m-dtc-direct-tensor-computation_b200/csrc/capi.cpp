@@ -217,14 +217,17 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
   bool want_fields = false;
   for (int64_t i = 0; i < n; ++i) want_fields = want_fields || out[i].displ || out[i].force;
   // Device passes: bounded by 80 % of the free device memory and chunk_domains.  A large batch
-  // also starts with a small pass (1/8 of it): the host phase of the rest (mesh planning,
-  // packing, multigrid plan) runs on a host thread while the device solves that first pass.
-  // Every pass repeats the latency-bound tail of the solve (its slowest domain, the coarse
-  // levels), so one cut, not more.  The adjoint keeps the last pass on the device: no extra
-  // cut with keep_displacements.
+  // also starts with a small pass: the host phase of the rest (mesh planning, packing,
+  // multigrid plan) runs on host threads while the device solves that first pass.  Every pass
+  // repeats the latency-bound tail of the solve (its slowest domain, the coarse levels), so one
+  // cut, not more.  Its size f n covers the host phase of the rest, f >= h / (d + h) with a
+  // margin of 1.5, for ~1.3 ms of host work per domain and host thread against ~3 ms of device
+  // time per domain (32^3 HEX08): f = 0.65 / (T + 0.43) for T host threads, in [1/8, 1/2].
+  // The adjoint keeps the last pass on the device: no extra cut with keep_displacements.
   constexpr int64_t kPipelineMin = 256;
   const bool keep = h->opt.keep_displacements != 0;
-  const int64_t pipe = (!keep && n >= kPipelineMin) ? std::max<int64_t>(32, n / 8) : 0;
+  const double frac = std::clamp(0.65 / (host_thread_count(h->opt.host_threads) + 0.43), 0.125, 0.5);
+  const int64_t pipe = (!keep && n >= kPipelineMin) ? std::max<int64_t>(32, (int64_t)(frac * (double)n)) : 0;
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { h->err = "cudaMemGetInfo failed"; return DTC_ERR_CUDA; }
   const double budget = 0.80 * (double)free_b;

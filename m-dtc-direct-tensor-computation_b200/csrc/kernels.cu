@@ -1064,23 +1064,26 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
       Lc[i * N + j] = s / ljj;
     }
   }
-  // inverse column by column: L L^T x = e_c on the kept DOFs
-  for (int c = 0; c < N; ++c) {
-    double y[N];
-    for (int i = 0; i < N; ++i) {
-      if (!keep[i]) { y[i] = 0; continue; }
-      double s = (i == c) ? 1.0 : 0.0;
-      for (int k = 0; k < i; ++k) s -= Lc[i * N + k] * y[k];
-      y[i] = s / Lc[i * N + i];
+  // A^-1 = L^-T L^-1 on the kept DOFs: the lower-triangular inverse column by column, then the
+  // symmetric product (rows and columns of dropped DOFs are zero)
+  double Li[N * N];
+  std::memset(Li, 0, sizeof(Li));
+  for (int j = 0; j < N; ++j) {
+    if (!keep[j]) continue;
+    Li[j * N + j] = 1.0 / Lc[j * N + j];
+    for (int i = j + 1; i < N; ++i) {
+      if (!keep[i]) continue;
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s -= Lc[i * N + k] * Li[k * N + j];
+      Li[i * N + j] = s / Lc[i * N + i];
     }
-    for (int i = N - 1; i >= 0; --i) {
-      if (!keep[i]) { y[i] = 0; continue; }
-      double s = y[i];
-      for (int k = i + 1; k < N; ++k) s -= Lc[k * N + i] * y[k];
-      y[i] = s / Lc[i * N + i];
-    }
-    for (int i = 0; i < N; ++i) out[i * N + c] = keep[c] ? (float)y[i] : 0.f;
   }
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c <= i; ++c) {
+      double s = 0.0;
+      for (int k = i; k < N; ++k) s += Li[k * N + i] * Li[k * N + c];
+      out[i * N + c] = out[c * N + i] = (float)s;
+    }
 }
 
 // Build the hierarchy on the host from the fine voxel factors.  fine_i: interior tiles of the
@@ -1748,18 +1751,20 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
     const int nx = D.n[0], ny = D.n[1], nz = D.n[2];
     std::vector<uint8_t> act((size_t)nx * ny * nz, 0);
     double kept = 0;
-    for (int64_t v = 0; v < nvox; ++v) {
-      if (sv[v] == 0.0f) continue;
-      kept += 1;
-      const int vx = (int)(v % in.L[0]), vy = (int)((v / in.L[0]) % in.L[1]), vz = (int)(v / (in.L[0] * in.L[1]));
-      for (int c = 0; c <= m; ++c)
-        for (int b2 = 0; b2 <= m; ++b2)
-          for (int a2 = 0; a2 <= m; ++a2) {
-            const int odd = (a2 == 1) + (b2 == 1) + (c == 1);
-            if (m == 2 && odd > 1) continue;   // HEX20 has no face or body nodes
-            act[(m * vx + a2) + (size_t)nx * ((m * vy + b2) + (size_t)ny * (m * vz + c))] = 1;
-          }
-    }
+    int64_t v = 0;
+    for (int vz = 0; vz < (int)in.L[2]; ++vz)
+      for (int vy = 0; vy < (int)in.L[1]; ++vy)
+        for (int vx = 0; vx < (int)in.L[0]; ++vx, ++v) {
+          if (sv[v] == 0.0f) continue;
+          kept += 1;
+          for (int c = 0; c <= m; ++c)
+            for (int b2 = 0; b2 <= m; ++b2)
+              for (int a2 = 0; a2 <= m; ++a2) {
+                const int odd = (a2 == 1) + (b2 == 1) + (c == 1);
+                if (m == 2 && odd > 1) continue;   // HEX20 has no face or body nodes
+                act[(m * vx + a2) + (size_t)nx * ((m * vy + b2) + (size_t)ny * (m * vz + c))] = 1;
+              }
+        }
     // algorithmic work of one launch on this domain, in elements of T per vector (bytes later)
     // and flops: vector kernels touch 72 values per active interior node per vector; the
     // stiffness application reads the input and writes the output (2 vectors) plus one
@@ -1770,6 +1775,7 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
         for (int y = 1; y < ny - 1; ++y)
           for (int x = 1; x < nx - 1; ++x) nint += act[x + (size_t)nx * (y + (size_t)ny * z)];
       out.vec = 72.0 * nint;
+      out.ni.reserve((size_t)nint);
       out.mv = 2 * 72.0 * nint + (double)nvox;
       out.fl = kept * 2.0 * (3 * NEN) * (3 * NEN) * kNLC;
     }
