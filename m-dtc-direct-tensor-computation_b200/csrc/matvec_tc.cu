@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(128, 4)
   }
   if (fail) {
     if (tid == 0) atomicExch(err, 1);
-    mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this round's MMAs
+    mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this iteration's MMAs
   }
   __syncthreads();
   if (warp == 0) {
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(128, 2)
   }
   if (fail) {
     if (tid == 0) atomicExch(err, 1);
-    tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this round's MMAs
+    tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this iteration's MMAs
   }
   __syncthreads();
   if (warp == 0) {
