@@ -8,6 +8,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -291,7 +292,13 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
   for (size_t c = 0; c < npass; ++c) {
     Stage next;
     std::thread ahead;
-    if (c + 1 < npass) ahead = std::thread(host_stage, c + 1, std::ref(next));
+    bool ahead_done = c + 1 >= npass;
+    if (!ahead_done) {
+      try {
+        ahead = std::thread(host_stage, c + 1, std::ref(next));
+      } catch (const std::system_error&) {   // no thread: prepare the next pass after this one
+      }
+    }
     int rc = cur.rc;
     if (rc != DTC_OK) h->err = cur.msg;
     const bool work = rc == DTC_OK && !cur.tasks.empty();
@@ -301,6 +308,7 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
       rc = h->solver.solve(cur.tasks, h->opt, in[0].nu, std::move(cur.batch), h->err);
     }
     if (ahead.joinable()) ahead.join();
+    else if (!ahead_done && rc == DTC_OK) host_stage(c + 1, next);
     if (rc != DTC_OK) return (dtc_status)rc;
     if (work) {
       const SolverStats& ss = h->solver.stats();
