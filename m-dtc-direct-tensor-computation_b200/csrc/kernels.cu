@@ -1769,13 +1769,18 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
     // and flops: vector kernels touch 72 values per active interior node per vector; the
     // stiffness application reads the input and writes the output (2 vectors) plus one
     // float per voxel, and costs 2 * (3 NEN)^2 flops per kept voxel and load case.
+    // the active interior nodes (flat vector kernels of the multigrid path) in one pass
+    out.ni.reserve((size_t)kept * (m == 1 ? 2 : 8) + 64);
+    for (int z = 1; z < nz - 1; ++z)
+      for (int y = 1; y < ny - 1; ++y) {
+        const size_t row = (size_t)nx * (y + (size_t)ny * z);
+        for (int x = 1; x < nx - 1; ++x)
+          if (act[x + row])
+            out.ni.push_back(((int64_t)dom << kListShift) | (D.node_off + x + (int64_t)row));
+      }
     {
-      double nint = 0;
-      for (int z = 1; z < nz - 1; ++z)
-        for (int y = 1; y < ny - 1; ++y)
-          for (int x = 1; x < nx - 1; ++x) nint += act[x + (size_t)nx * (y + (size_t)ny * z)];
+      const double nint = (double)out.ni.size();
       out.vec = 72.0 * nint;
-      out.ni.reserve((size_t)nint);
       out.mv = 2 * 72.0 * nint + (double)nvox;
       out.fl = kept * 2.0 * (3 * NEN) * (3 * NEN) * kNLC;
     }
@@ -1786,13 +1791,6 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
             if (act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
       return false;
     };
-    // active interior nodes (flat vector kernels of the multigrid path)
-    for (int z = 1; z < nz - 1; ++z)
-      for (int y = 1; y < ny - 1; ++y)
-        for (int x = 1; x < nx - 1; ++x)
-          if (act[x + (size_t)nx * (y + (size_t)ny * z)])
-            out.ni.push_back(((int64_t)dom << kListShift) |
-                             (D.node_off + x + (int64_t)nx * (y + (int64_t)ny * z)));
     // node tiles (vector kernels) over the interior / all nodes
     for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
       for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
