@@ -25,9 +25,10 @@ import __graft_entry__ as ge  # noqa: E402
 
 METRIC = "domains/sec at ≤1e-5 rel tensor err: mixed+batched vs plain FP64, 1 B200"
 TARGET = 1e-5
-# rtol at which the reference algorithm (reaction projection, FP64) meets TARGET on this
-# workload, as calibrated on the GPU; the host-only reference arm cannot calibrate itself
-REF_RTOL = 1e-7
+# rtol at which the reference algorithm (reaction projection, FP64) meets TARGET/2 on this
+# workload: what the plain FP64 GPU arm calibrates to on the 512 x 32^3 batch (3e-7, measured);
+# the host-only reference arm cannot calibrate itself
+REF_RTOL = 3e-7
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the fine
 # sweeps, measured on 16 domains of 32^3 (profiles/k_matvec_k_mg_matvec_f32_16x32cubed.md)
 DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 0.96, "mg_residual_f32": 1.53, "mg_postsmooth_f32": 1.53}
@@ -141,9 +142,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(args, dtc, grays, rtol):
+def cpu_baseline(args, dtc, grays, rtol, gpu_res=None):
     """The FP64 CPU oracle on a bounded sample of the same workload: one domain per host
-    thread, the domains of the first step of the GPU batch."""
+    thread, the first domains of the GPU batch.  With gpu_res (the timed arm's results of the
+    same domains) it also reports their largest relative tensor difference from the oracle."""
     orc = ge.load_oracle()
     syn = dtc.synth
     cores = os.cpu_count() or 1
@@ -151,11 +153,17 @@ def cpu_baseline(args, dtc, grays, rtol):
     doms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=rtol, max_it=args.max_it,
                        E_voxel=syn.modulus_of_gray(g)) for g in grays[:nsample]]
     t0 = time.perf_counter()
-    orc.solve_batch(doms, nthreads=nsample)
+    ref = orc.solve_batch(doms, nthreads=nsample)
     dt = time.perf_counter() - t0
-    return {"value": nsample / dt, "unit": "domains/s", "cores": nsample, "kind": "port",
-            "sample": f"first {nsample} domains of the batch ({args.L}^3, rtol {rtol}), one per thread, "
-                      f"{dt:.1f} s"}
+    out = {"value": nsample / dt, "unit": "domains/s", "cores": nsample, "kind": "port",
+           "sample": f"first {nsample} domains of the batch ({args.L}^3, rtol {rtol}), one per thread, "
+                     f"{dt:.1f} s"}
+    if gpu_res is not None:
+        out["max_rel_err_vs_oracle"] = _err(gpu_res[:nsample], ref)
+        out["oracle_rtol"] = rtol
+        out["oracle_note"] = ("normwise max|C - C_oracle| / max|C_oracle| over the sample; the oracle runs at "
+                              "the plain FP64 arm's calibrated rtol, so the figure includes its own solve error")
+    return out
 
 
 def run_reference(args, dtc):
@@ -242,12 +250,24 @@ def run_config(args, dtc):
                  for _, xa, sub in parts]
         cores = min(len(odoms), os.cpu_count() or 1)
         t0 = time.perf_counter()
-        orc.solve_batch(odoms, nthreads=cores)
+        ref = orc.solve_batch(odoms, nthreads=cores)
         tcpu = time.perf_counter() - t0
+        with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=True, device=local) as sv:
+            res = sv.solve(doms)
+
+        def rel(a, b):
+            return float(np.abs(a - b).max() / np.abs(b).max())
         line.update({"workload": "27 HEX08 domains of 20^3 from a 62^3 volume (BV/TV 0.25), FP64 rtol 1e-10, "
                                  "rotation search", "gpu_ms_device": dev, "gpu_ms_wall": 1e3 * wall,
                      "gpu_domains_per_s_wall": len(doms) / wall,
-                     "cpu_oracle_s": tcpu, "cpu_cores": cores, "cpu_domains_per_s": len(doms) / tcpu})
+                     "cpu_oracle_s": tcpu, "cpu_cores": cores, "cpu_domains_per_s": len(doms) / tcpu,
+                     "vs_oracle": {"max_rel_err_c": max(rel(r["c"], t["c"]) for r, t in zip(res, ref)),
+                                   "max_rel_err_ff": max(rel(r["ff"], t["ff"]) for r, t in zip(res, ref)),
+                                   "max_rel_err_kmacro": max(rel(r["kmacro"], t["kmacro"]) for r, t in zip(res, ref)),
+                                   "counts_equal": all((r["ne"], r["nn"], r["nb"]) == (t["ne"], t["nn"], t["nb"])
+                                                       for r, t in zip(res, ref)),
+                                   "max_abs_iter_diff": int(max(np.abs(r["iters"] - t["iters"]).max()
+                                                                for r, t in zip(res, ref)))}})
     elif args.config == "c2":
         # 256 HEX20 domains of 24^3, BV/TV 0.25, mixed vs plain FP64
         n = args.ndom
@@ -473,7 +493,8 @@ def main():
     ratio = DRAM_PER_ALGORITHMIC_BYTE.get(top)
     traffic = kt["bytes_per_launch"] * ratio if ratio else None
     share = {k: round(v["ms_total"] / sum(x["ms_total"] for x in ks.values()), 4) for k, v in ks.items()}
-    cpu = cpu_baseline(args, dtc, grays, rtol_of["fp64"]) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    cpu = (cpu_baseline(args, dtc, grays, rtol_of["fp64"], res) if (rank == 0 and world == 1 and not args.no_cpu)
+           else None)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "domains/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",

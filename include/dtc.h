@@ -91,7 +91,12 @@ typedef struct dtc_options {
                               displacements of every pass but the last to host memory */
   int32_t graph_chunks;    /* 0: each chunk of CG iterations is captured once and replayed as a
                               CUDA graph; 1: kernels are launched one by one */
-  int32_t reserved[2];
+  int32_t tc_wait_spins;   /* tensor-core kernels: polls of a round's completion barrier before
+                              the kernel gives up and the call returns DTC_ERR_INTERNAL
+                              (0 -> 2^26).  Only for testing that error path: a small value
+                              makes the wait run out; the drain before tensor memory is freed
+                              keeps the full bound */
+  int32_t reserved[1];
 } dtc_options;
 
 typedef struct dtc_domain_in {
@@ -199,6 +204,15 @@ dtc_status dtc_energy_grad(dtc_handle* handle, const double* dloss_dc, float* co
 dtc_status dtc_get_stats(const dtc_handle* handle, double* ms_solve, int64_t* kernel_launches,
                          double* dof_iterations);
 
+/* Rotation search of given tensors (f-src/mod_struct_calcmat.f90:533-1603, criteria also
+ * f-src/mod_tensor_opt.f90:40-603): the CR1/CR2 sweep and refinement on the handle's device,
+ * then the angle, axis, frame and rotated tensor of each criterion on the host, exactly as
+ * dtc_solve_batch does with rotation_search = 1.
+ *   ee  : n x 36 doubles in host memory (6x6 column-major, symmetric: the "Averaged
+ *         Effective stiffness" leaf)
+ *   out : n records; only the cr1_* and cr2_* fields are written. */
+dtc_status dtc_rotation_search(dtc_handle* handle, const double* ee, int64_t n, dtc_domain_out* out);
+
 /* Rotation search (CR1/CR2 sweep and refinement, f-src/mod_struct_calcmat.f90:533-1603) on
  * tensors already in device memory, without allocating anything.  For callers that cannot
  * allocate device memory at the point of the call -- e.g. a host code that runs this step
@@ -213,9 +227,12 @@ dtc_status dtc_get_stats(const dtc_handle* handle, double* ms_solve, int64_t* ke
  *          not synchronise.
  * n must not exceed 1024: the scratch is one fixed 2 MiB device array per device, kept until
  * the process exits, shared by all calls; calls that overlap on the GPU race on it.
- * The first call on a device resolves that array's address and uploads two small tables, so
- * it synchronises and should come before any stream capture.  Sizes beyond the maximum
- * return DTC_ERR_INVALID_ARGUMENT. */
+ * The first call on a device resolves that array's address and uploads two small tables
+ * (unless dtc_solve_batch or dtc_rotation_search uploaded them already), then waits for the
+ * device, so it should come before any stream capture.  The tables are written once per
+ * device and process, never again, and the address is kept for the life of the process:
+ * do not use this entry point across a cudaDeviceReset.  Sizes beyond the maximum return
+ * DTC_ERR_INVALID_ARGUMENT. */
 dtc_status dtc_rotation_search_noalloc(const double* ee, int64_t n, int64_t* ang, int32_t* jj, double* crit,
                                        void* stream);
 

@@ -104,7 +104,7 @@ class Solver:
     def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=0.0, max_refine=12,
                  rotation_search=True, device=0, host_threads=0, keep_displacements=False,
                  profile_kernels=False, mixed_matvec="simt", inner_precond="block", estimator="reaction",
-                 chunk_domains=0, graphs=True):
+                 chunk_domains=0, graphs=True, tc_wait_spins=0):
         self.lib = capi.load()
         o = capi.Options()
         self.lib.dtc_default_options(C.byref(o))
@@ -118,6 +118,7 @@ class Solver:
         o.tensor_estimator = {"reaction": 0, "energy": 1}[estimator]
         o.chunk_domains = int(chunk_domains)
         o.graph_chunks = 0 if graphs else 1
+        o.tc_wait_spins = int(tc_wait_spins)
         self.options = o
         h = C.c_void_p()
         rc = self.lib.dtc_create(C.byref(h), C.byref(o))
@@ -158,6 +159,16 @@ class Solver:
                 outs[i].force = ff_.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.dtc_solve_batch(self.handle, ins, n, outs))
         return _results(outs, keep if want_fields else None)
+
+    def rotation_search(self, ee):
+        """CR1/CR2 rotation search of given symmetric 6x6 tensors (n x 6 x 6): result dicts with
+        the "cr1" and "cr2" entries of solve()."""
+        ee = np.asarray(ee, dtype=np.float64).reshape(-1, 6, 6)
+        n = ee.shape[0]
+        flat = np.ascontiguousarray(ee.transpose(0, 2, 1))   # column-major per tensor
+        outs = (capi.DomainOut * n)()
+        self._check(self.lib.dtc_rotation_search(self.handle, flat.ctypes.data_as(C.POINTER(C.c_double)), n, outs))
+        return [{k: r[k] for k in ("cr1", "cr2")} for r in _results(outs, None)]
 
     def stats(self):
         ms, launches, dofit = C.c_double(), C.c_int64(), C.c_double()

@@ -30,7 +30,7 @@ class Options(C.Structure):
         ("keep_displacements", C.c_int32), ("profile_kernels", C.c_int32),
         ("mixed_matvec", C.c_int32), ("inner_precond", C.c_int32),
         ("tensor_estimator", C.c_int32), ("chunk_domains", C.c_int32), ("graph_chunks", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("tc_wait_spins", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 
@@ -103,6 +103,7 @@ SIGNATURES = {
     "dtc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "dtc_element_stiffness": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "dtc_get_kernel_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStats), C.c_int32, C.POINTER(C.c_int32)]),
+    "dtc_rotation_search": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POINTER(DomainOut)]),
     "dtc_rotation_search_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),
     "dtc_last_error": (C.c_char_p, [C.c_void_p]),

@@ -42,20 +42,7 @@ int validate_domain(const dtc_domain_in& in, std::string& msg) {
 }
 
 void plan_all(const dtc_domain_in* in, int64_t n, MeshPlan* plans, bool numbering, int threads) {
-  int nt = host_thread_count(threads);
-  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
-  std::atomic<int64_t> next(0);
-  auto work = [&]() {
-    for (;;) {
-      int64_t i = next.fetch_add(1);
-      if (i >= n) break;
-      plan_mesh(in[i], numbering, plans[i]);
-    }
-  };
-  std::vector<std::thread> pool;
-  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
-  work();
-  for (auto& th : pool) th.join();
+  parallel_for(n, threads, [&](int64_t i) { plan_mesh(in[i], numbering, plans[i]); });
 }
 
 // The last element kept only by the compaction quirk contributes its 3x3 diagonal block at
@@ -138,7 +125,7 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
     return DTC_ERR_INVALID_ARGUMENT;
   if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 1 ||
       o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0 || o.graph_chunks < 0 ||
-      o.graph_chunks > 1)
+      o.graph_chunks > 1 || o.tc_wait_spins < 0)
     return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
@@ -348,6 +335,31 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
       finish_rotation(ees[d], 1, &ang[6 * d], jj[2 * d], crit[2 * d], rot_out[d]);
       finish_rotation(ees[d], 2, &ang[6 * d + 3], jj[2 * d + 1], crit[2 * d + 1], rot_out[d]);
     }
+  }
+  return DTC_OK;
+}
+
+dtc_status dtc_rotation_search(dtc_handle* h, const double* ee, int64_t n, dtc_domain_out* out) {
+  if (!h) return DTC_ERR_INVALID_ARGUMENT;
+  h->err.clear();
+  if (n < 0 || (n > 0 && (!ee || !out))) { h->err = "ee/out must be non-NULL for n > 0"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (n == 0) return DTC_OK;
+  if (cudaSetDevice(h->opt.device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
+  std::vector<const double*> ees((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    ees[i] = ee + 36 * i;
+    for (int q = 0; q < 36; ++q)
+      if (!std::isfinite(ee[36 * i + q])) { h->err = "tensor " + std::to_string(i) + " is not finite"; return DTC_ERR_INVALID_ARGUMENT; }
+  }
+  std::vector<int64_t> ang;
+  std::vector<int> jj;
+  std::vector<double> crit;
+  int64_t launches = 0;
+  int rc = rotation_search_device(ees, ang, jj, crit, nullptr, launches, h->err);
+  if (rc != DTC_OK) return (dtc_status)rc;
+  for (int64_t d = 0; d < n; ++d) {
+    finish_rotation(ees[d], 1, &ang[6 * d], jj[2 * d], crit[2 * d], &out[d]);
+    finish_rotation(ees[d], 2, &ang[6 * d + 3], jj[2 * d + 1], crit[2 * d + 1], &out[d]);
   }
   return DTC_OK;
 }

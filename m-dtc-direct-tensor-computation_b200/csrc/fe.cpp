@@ -1,6 +1,8 @@
 // fe.cpp -- host-side FE and homogenisation helpers (FP64).
 #include "fe.h"
 
+#include "ddmath.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -303,11 +305,12 @@ void finish_rotation(const double ee[36], int which, const int64_t ang[3], int j
   }
 }
 
+// cos and sin of k degrees, k = 0..180, correctly rounded (ddmath.h), as the device
+// computes the refinement levels
 void degree_tables(double* c, double* s) {
   for (int k = 0; k <= 180; ++k) {
     double a = (double)k * kPiDiv180;
-    c[k] = std::cos(a);
-    s[k] = std::sin(a);
+    dd::sincos_cr(a, &s[k], &c[k]);
   }
 }
 

@@ -874,6 +874,7 @@ void launch_matvec_tc(const Tile* tiles, int64_t ntiles, const DomDev* doms, con
                       const uint8_t* flags, const float* u, float* y, double* acc_pw, const int* dom_active, int* err,
                       cudaStream_t s);
 int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg);
+int set_tc_spin_limit(long long spins, cudaStream_t s, std::string& msg);
 void build_tc20_operand(const double* k20, float* img);
 size_t tc20_operand_bytes();
 int allow_ebe_tc(std::string& msg);
@@ -1092,25 +1093,6 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
 // uneven batch (16^3-64^3) ~3.5% less solve time than once everywhere; twice already on
 // level 1 costs more than the iterations it saves.
 constexpr int kMgTwiceFrom = 2;
-
-// Runs f(i) for i in [0, n) on `threads` host threads (0: the CPUs of the affinity mask).
-template <class F>
-void parallel_for(int64_t n, int threads, F&& f) {
-  int nt = host_thread_count(threads);
-  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
-  std::atomic<int64_t> next(0);
-  auto work = [&]() {
-    for (;;) {
-      const int64_t i = next.fetch_add(1);
-      if (i >= n) break;
-      f(i);
-    }
-  };
-  std::vector<std::thread> pool;
-  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
-  work();
-  for (auto& th : pool) th.join();
-}
 
 // HEX20 fine grids (m = 2) get one p-coarsening first: level 1 is the HEX08 mesh of the same
 // voxels (corner nodes; the trilinear space is contained in the serendipity one, so the
@@ -1870,6 +1852,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
     if (int e = upload_tc_operand(kh, s, msg)) return e;
+    if (I.tensor_matvec)
+      if (int e = set_tc_spin_limit(opt.tc_wait_spins, s, msg)) return e;
     if (NEN == 20) {
       std::vector<double> k20(3600);
       std::vector<float> k20f(3600);

@@ -77,9 +77,19 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
       : "r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < kSpinLimit; ++i) {
-    uint32_t done;
+// Waits until the mbarrier phase of the given parity has completed: one immediate test, then
+// up to limit - 1 potentially suspending polls.  Returns false when the limit runs out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = kSpinLimit) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  if (done) return true;
+  for (long long i = 1; i < limit; ++i) {
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -93,6 +103,17 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 }
 
 }  // namespace tc
+
+// Polls of the per-round completion wait before a kernel gives up (the drain wait before the
+// tensor memory is freed always keeps the full bound).  dtc_options.tc_wait_spins sets it.
+__device__ long long g_tc_spin_limit = tc::kSpinLimit;
+
+int set_tc_spin_limit(long long spins, cudaStream_t s, std::string& msg) {
+  const long long v = spins > 0 ? spins : tc::kSpinLimit;
+  DTC_CUDA(cudaMemcpyToSymbolAsync(g_tc_spin_limit, &v, sizeof(v), 0, cudaMemcpyHostToDevice, s));
+  DTC_CUDA(cudaStreamSynchronize(s));   // v lives on this stack frame
+  return DTC_OK;
+}
 
 // Khat split into tf32 hi / lo, laid out as 6 canonical B chunks (hi k0..2, lo k0..2).
 __constant__ float c_bsplit[6 * tc::kN * tc::kKc];
@@ -217,7 +238,7 @@ __global__ void __launch_bounds__(128, 4)
                        smem_u32(&mbar))
                    : "memory");
     }
-    if (!mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1))) atomicOr(&fail, 1);
+    if (!mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1), g_tc_spin_limit)) atomicOr(&fail, 1);
     __syncthreads();
     if (fail) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -491,7 +512,7 @@ __global__ void __launch_bounds__(128, 2)
                        tc::smem_u32(&mbar))
                    : "memory");
     }
-    if (!tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)(rd & 1))) atomicOr(&fail, 1);
+    if (!tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)(rd & 1), g_tc_spin_limit)) atomicOr(&fail, 1);
     __syncthreads();
     if (fail) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

@@ -8,6 +8,11 @@
 // Here one thread evaluates one candidate; a block argmin keeps MINLOC's tie rule (smallest
 // linear index, alpha fastest).  This file is compiled with --fmad=false so every
 // criterion is evaluated with the same rounding steps as the written expression.
+//
+// Sines and cosines: the 1-degree sweep reads two tables built on the host, each refinement
+// level builds its 3 x 21 values in shared memory; all of them are the correctly rounded
+// values (ddmath.h), the same on the host and the device, so the argmin indices do not
+// depend on which math library evaluated them.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -16,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "ddmath.h"
 #include "fe.h"
 #include "kernels.cuh"
 #include "solver.h"
@@ -135,6 +141,7 @@ __global__ void __launch_bounds__(kRotThreads) k_rot_refine(const double* __rest
                                                             double* __restrict__ crit_out) {
   __shared__ double E[36];
   __shared__ ArgMin sh[kRotThreads];
+  __shared__ double tsin[3][21], tcos[3][21];
   const int dom = blockIdx.x, which = blockIdx.y;
   if (threadIdx.x < 36) E[threadIdx.x] = ee[(int64_t)dom * 36 + threadIdx.x];
   ArgMin m{INFINITY, INT64_MAX};
@@ -153,15 +160,19 @@ __global__ void __launch_bounds__(kRotThreads) k_rot_refine(const double* __rest
   for (;;) {
     const int64_t lo[3] = {(a[0] - 1) * 10, (a[1] - 1) * 10, (a[2] - 1) * 10};
     div = div * 0.1;
+    if (threadIdx.x < 63) {
+      const int d = threadIdx.x / 21, i = threadIdx.x % 21;
+      double sv, cv;
+      dd::sincos_cr((double)(lo[d] + i) * div, &sv, &cv);
+      tsin[d][i] = sv;
+      tcos[d][i] = cv;
+    }
+    __syncthreads();
     ArgMin w{INFINITY, INT64_MAX};
     for (int t = threadIdx.x; t < 21 * 21 * 21; t += kRotThreads) {
-      const int64_t ia = lo[0] + t % 21, ip = lo[1] + (t / 21) % 21, ie = lo[2] + t / 441;
-      double sa, ca, sp, cp, se, ce;
-      sincos((double)ia * div, &sa, &ca);
-      sincos((double)ip * div, &sp, &cp);
-      sincos((double)ie * div, &se, &ce);
+      const int i0 = t % 21, i1 = (t / 21) % 21, i2 = t / 441;
       double c1, c2;
-      criteria(E, ca, sa, cp, sp, ce, se, c1, c2);
+      criteria(E, tcos[0][i0], tsin[0][i0], tcos[1][i1], tsin[1][i1], tcos[2][i2], tsin[2][i2], c1, c2);
       const double c = which == 0 ? c1 : c2;
       if (c < w.v) { w.v = c; w.i = t; }
     }
@@ -182,14 +193,35 @@ __global__ void __launch_bounds__(kRotThreads) k_rot_refine(const double* __rest
 
 }  // namespace
 
+namespace {
+std::mutex g_tables_mu;
+bool g_tables_loaded[256] = {false};   // c_cosd / c_sind written on this device ordinal
+}  // namespace
+
+// Loads the sweep's degree tables into the current device's constant memory once per device
+// and process.  Waits until the copy has landed (a later kernel may run on any stream), so
+// the first call must not come inside a stream capture.  Later calls do nothing, so calls
+// already in flight on other streams never see the tables being rewritten.
+int ensure_degree_tables(std::string& msg) {
+  int dev = -1;
+  DTC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) { msg = "device ordinal out of range"; return DTC_ERR_CUDA; }
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  if (g_tables_loaded[dev]) return DTC_OK;
+  double c[181], sn[181];
+  degree_tables(c, sn);
+  DTC_CUDA(cudaMemcpyToSymbol(c_cosd, c, sizeof(c)));
+  DTC_CUDA(cudaMemcpyToSymbol(c_sind, sn, sizeof(sn)));
+  DTC_CUDA(cudaDeviceSynchronize());
+  g_tables_loaded[dev] = true;
+  return DTC_OK;
+}
+
 int rotation_search_device(const std::vector<const double*>& ees, std::vector<int64_t>& ang, std::vector<int>& jj,
                            std::vector<double>& crit, cudaStream_t s, int64_t& launches, std::string& msg) {
   const int ndom = (int)ees.size();
   if (ndom == 0) return DTC_OK;
-  double c[181], sn[181];
-  degree_tables(c, sn);
-  DTC_CUDA(cudaMemcpyToSymbolAsync(c_cosd, c, sizeof(c), 0, cudaMemcpyHostToDevice, s));
-  DTC_CUDA(cudaMemcpyToSymbolAsync(c_sind, sn, sizeof(sn), 0, cudaMemcpyHostToDevice, s));
+  if (int rc = ensure_degree_tables(msg)) return rc;
   std::vector<double> hee((size_t)36 * ndom);
   for (int d = 0; d < ndom; ++d) std::memcpy(&hee[(size_t)36 * d], ees[d], 36 * sizeof(double));
   double* dee = nullptr;
@@ -258,11 +290,8 @@ extern "C" dtc_status dtc_rotation_search_noalloc(const double* ee, int64_t n, i
     if (!g_noalloc_ptr[dev]) {
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, g_noalloc_part) != cudaSuccess || !p) return DTC_ERR_CUDA;
-      double c[181], sn[181];
-      degree_tables(c, sn);
-      if (cudaMemcpyToSymbol(c_cosd, c, sizeof(c)) != cudaSuccess ||
-          cudaMemcpyToSymbol(c_sind, sn, sizeof(sn)) != cudaSuccess)
-        return DTC_ERR_CUDA;
+      std::string msg;
+      if (ensure_degree_tables(msg) != DTC_OK) return DTC_ERR_CUDA;   // uploads and waits for them
       g_noalloc_ptr[dev] = static_cast<ArgMin*>(p);
     }
     part = g_noalloc_ptr[dev];

@@ -3,6 +3,9 @@
 #include <sched.h>
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <mutex>
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -25,6 +28,41 @@ inline int host_thread_count(int requested) {
     if (n > 0) return n;
   }
   return (int)std::max(1u, std::thread::hardware_concurrency());
+}
+
+// Runs f(i) for i in [0, n) on up to `threads` host threads (0: host_thread_count).  An
+// exception thrown by f on any thread stops the hand-out of further indices and is rethrown on
+// the calling thread once every started thread has joined; if a thread cannot be started, the
+// work runs on the threads that could (at least the calling one).
+template <class F>
+void parallel_for(int64_t n, int threads, F&& f) {
+  int nt = host_thread_count(threads);
+  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(n, 1));
+  std::atomic<int64_t> next(0);
+  std::mutex mu;
+  std::exception_ptr first;
+  auto work = [&]() {
+    try {
+      for (;;) {
+        const int64_t i = next.fetch_add(1);
+        if (i >= n) break;
+        f(i);
+      }
+    } catch (...) {
+      std::lock_guard<std::mutex> lock(mu);
+      if (!first) first = std::current_exception();
+      next.store(n);
+    }
+  };
+  std::vector<std::thread> pool;
+  try {
+    pool.reserve((size_t)nt);
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  } catch (...) {   // std::system_error (no thread) or std::bad_alloc: go on with fewer threads
+  }
+  work();
+  for (auto& th : pool) th.join();
+  if (first) std::rethrow_exception(first);
 }
 
 struct DomainTask {

@@ -10,6 +10,8 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+
+#include <quadmath.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -671,11 +673,38 @@ inline void unit_normal(double phi, double eta, double n[3]) {
   n[0] /= s; n[1] /= s; n[2] /= s;
 }
 
-// crit1 = sum (B^T E B)(1:4,5:6)^2 ; crit2 = sum over the 12 upper off-diagonal blocks
-inline void criteria(const double* EE, double alpha, double phi, double eta, double* c1, double* c2) {
-  double n[3], aa[9], BB[36];
-  unit_normal(phi, eta, n);
-  rot_alg(n, alpha, aa);
+// sin and cos of a candidate angle, rounded to nearest from quad precision (libquadmath).
+// The reference takes them from its platform's libm; the argmin of the deep refinement
+// levels is decided by their last bits, and glibc's double sin/cos differ from the nearest
+// double for a fraction of a percent of these arguments, so both this oracle and the GPU
+// code use the correctly rounded values (the GPU code computes them itself).
+struct SinCos { double s, c; };
+inline SinCos sincos_nearest(double x) {
+  const __float128 q = (__float128)x;
+  return {(double)sinq(q), (double)cosq(q)};
+}
+
+// criteria from the sines and cosines of (alpha, phi, eta); same expressions as rot_alg /
+// unit_normal with the trigonometric values supplied
+inline void criteria_sc(const double* EE, SinCos a, SinCos p, SinCos e, double* c1, double* c2) {
+  double n[3] = {p.c * e.s, p.s * e.s, e.c};
+  double s = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  n[0] /= s; n[1] /= s; n[2] /= s;
+  double aa[9], BB[36];
+  {
+    double ca = a.c, sa = a.s, omc = 1.0 - ca;
+    double n12 = n[0] * n[1], n13 = n[0] * n[2], n23 = n[1] * n[2];
+    auto A = [&](int i, int j) -> double& { return aa[(i - 1) + 3 * (j - 1)]; };
+    A(1, 1) = ca + n[0] * n[0] * omc;
+    A(2, 2) = ca + n[1] * n[1] * omc;
+    A(3, 3) = ca + n[2] * n[2] * omc;
+    A(1, 2) = n12 * omc - n[2] * sa;
+    A(2, 1) = n12 * omc + n[2] * sa;
+    A(1, 3) = n13 * omc + n[1] * sa;
+    A(3, 1) = n13 * omc - n[1] * sa;
+    A(2, 3) = n23 * omc - n[0] * sa;
+    A(3, 2) = n23 * omc + n[0] * sa;
+  }
   tra_r6(aa, BB);
   double t[13];
   const int ij[12][2] = {{1, 4}, {1, 5}, {1, 6}, {2, 4}, {2, 5}, {2, 6}, {3, 4}, {3, 5}, {3, 6}, {4, 5}, {4, 6}, {5, 6}};
@@ -685,16 +714,20 @@ inline void criteria(const double* EE, double alpha, double phi, double eta, dou
         t[9] * t[9] + t[10] * t[10] + t[11] * t[11] + t[12] * t[12];
 }
 
-// One criterion's sweep + x10 refinement; returns angles (integers in units of 10^-jj deg)
-// and jj.  MINLOC picks the first minimum in column-major order (alpha fastest).
+// One criterion's sweep + x10 refinement (mod_struct_calcmat.f90:762-1012 / :1206-1460);
+// returns angles (integers in units of 10^-jj deg) and jj.  MINLOC picks the first minimum
+// in column-major order (alpha fastest).  The angle of index i at a level is i * div with
+// div = (pi/180) * 0.1^jj formed by repeated multiplication, as the reference forms it.
 void search_one(const double* EE, int which, int64_t ang_out[3], int* jj_out, double* crit_out) {
+  SinCos deg[181];
+  for (int k = 0; k <= 180; ++k) deg[k] = sincos_nearest((double)k * kPiDiv180);
   double best = INFINITY;
   int64_t ba = 0, bp = 0, be = 0;
   for (int ie = 0; ie <= 90; ++ie)
     for (int ip = 0; ip <= 180; ++ip)
       for (int ia = 0; ia <= 180; ++ia) {
         double c1, c2;
-        criteria(EE, (double)ia * kPiDiv180, (double)ip * kPiDiv180, (double)ie * kPiDiv180, &c1, &c2);
+        criteria_sc(EE, deg[ia], deg[ip], deg[ie], &c1, &c2);
         double c = which == 1 ? c1 : c2;
         if (c < best) { best = c; ba = ia; bp = ip; be = ie; }
       }
@@ -708,13 +741,16 @@ void search_one(const double* EE, int which, int64_t ang_out[3], int* jj_out, do
     int64_t s[3] = {(ca - 1) * 10, (cp - 1) * 10, (ce - 1) * 10};
     int64_t e[3] = {(ca + 1) * 10, (cp + 1) * 10, (ce + 1) * 10};
     div = div * 0.1;
+    SinCos tab[3][21];
+    for (int d = 0; d < 3; ++d)
+      for (int64_t i = s[d]; i <= e[d]; ++i) tab[d][i - s[d]] = sincos_nearest((double)i * div);
     double wbest = INFINITY;
     int64_t na = 0, np = 0, nE = 0;
     for (int64_t ie = s[2]; ie <= e[2]; ++ie)
       for (int64_t ip = s[1]; ip <= e[1]; ++ip)
         for (int64_t ia = s[0]; ia <= e[0]; ++ia) {
           double c1, c2;
-          criteria(EE, (double)ia * div, (double)ip * div, (double)ie * div, &c1, &c2);
+          criteria_sc(EE, tab[0][ia - s[0]], tab[1][ip - s[1]], tab[2][ie - s[2]], &c1, &c2);
           double c = which == 1 ? c1 : c2;
           if (c < wbest) { wbest = c; na = ia; np = ip; nE = ie; }
         }
@@ -780,10 +816,12 @@ void rotation_search(const double* EE, orc_domain_out* out) {
       out->cr1_angle = alpha_out; std::memcpy(out->cr1_n, n_out, sizeof(n_out));
       std::memcpy(out->cr1_aa, aa, sizeof(aa)); std::memcpy(out->cr1_ee, EEr, sizeof(EEr));
       out->cr1_crit = crit; out->cr1_iters = jj;
+      std::memcpy(out->cr1_ang, ang, sizeof(ang));
     } else {                                                     // CR2 writes them after it (:1583-1597)
       out->cr2_angle = alpha; std::memcpy(out->cr2_n, n, sizeof(n));
       std::memcpy(out->cr2_aa, aa, sizeof(aa)); std::memcpy(out->cr2_ee, EEr, sizeof(EEr));
       out->cr2_crit = crit; out->cr2_iters = jj;
+      std::memcpy(out->cr2_ang, ang, sizeof(ang));
     }
   }
 }

@@ -77,6 +77,7 @@ typedef struct {
   double* bnode_vals;              /* 24 x (3*nb) prescribed values, column-major like bnode_vals(24,3nb) */
   double* displ;                   /* 24 x 3nn solutions incl. BC values (lc-major) */
   double* force;                   /* 24 x 3nn reaction forces AA_org*u (lc-major) */
+  int64_t cr1_ang[3], cr2_ang[3];  /* argmin indices (alpha, phi, eta) in units of 10^-jj degree */
 } orc_domain_out;
 
 /* Full path for one domain: mesh -> BC -> assembly -> 24 CG solves -> reactions ->

@@ -45,6 +45,7 @@ class OrcOut(C.Structure):
         ("nodes", C.POINTER(C.c_double)),
         ("bnode_ids", C.POINTER(C.c_int64)), ("bnode_vals", C.POINTER(C.c_double)),
         ("displ", C.POINTER(C.c_double)), ("force", C.POINTER(C.c_double)),
+        ("cr1_ang", C.c_int64 * 3), ("cr2_ang", C.c_int64 * 3),
     ]
 
 
@@ -170,6 +171,7 @@ def _result(dom, o, keep):
             "aa": np.array(getattr(o, k + "_aa")[:]).reshape(3, 3, order="F"),
             "ee": np.array(getattr(o, k + "_ee")[:]).reshape(6, 6, order="F"),
             "crit": getattr(o, k + "_crit"), "iters": getattr(o, k + "_iters"),
+            "ang": np.array(getattr(o, k + "_ang")[:], dtype=np.int64),
         }
     if keep:
         ne, nn, nb = o.ne, o.nn, o.nb

@@ -15,7 +15,7 @@ Fixtures written:
   vv_lin_eps1e-6.npy      mod_struct_calcmat.f90:1684-1770 init_loadcase_el_order_lin, vv(24,24)
   golden_meta.json        the source line ranges and the evaluation parameters
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference-checkout
 """
 import json
 import re
@@ -24,7 +24,9 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py /path/to/reference-checkout")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).resolve().parent
 
 
