@@ -197,6 +197,22 @@ dtc_status dtc_element_stiffness(int32_t elem_type, double E, double a, double n
 dtc_status dtc_energy_grad(dtc_handle* handle, const double* dloss_dc, float* const* grad_e,
                            int64_t n);
 
+/* dtc_solve_batch with the per-voxel moduli in device memory: E_voxel_dev[i] (n pointers in
+ * host memory; NULL for a domain without per-voxel moduli) points to L0*L1*L2 floats on the
+ * handle's device, x fastest; in[i].E_voxel is ignored for those domains.  The moduli are
+ * copied once through a pinned host buffer owned by the handle (the host mesh planning and
+ * multigrid build read them), then the call proceeds as dtc_solve_batch.  The copies are
+ * ordered after work already submitted to the legacy default stream.  No reference
+ * counterpart: the torch binding of the adjoint passes its tensors here. */
+dtc_status dtc_solve_batch_device_moduli(dtc_handle* handle, const dtc_domain_in* in, int64_t n,
+                                         dtc_domain_out* out, const float* const* E_voxel_dev);
+
+/* dtc_energy_grad writing into device memory: grad_e_dev[i] (n pointers in host memory) points
+ * to L0*L1*L2 floats on the handle's device; filled by device-to-device copies, complete when
+ * the call returns.  No reference counterpart. */
+dtc_status dtc_energy_grad_device(dtc_handle* handle, const double* dloss_dc, float* const* grad_e_dev,
+                                  int64_t n);
+
 /* Timing and work counters of the last dtc_solve_batch: device time of the solve in ms
  * (CUDA events on the solver stream, from the uploaded voxel factors to the last kernel,
  * summed over device passes; host meshing excluded), kernels launched, and the sum over

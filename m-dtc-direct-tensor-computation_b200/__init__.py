@@ -160,6 +160,24 @@ class Solver:
         self._check(self.lib.dtc_solve_batch(self.handle, ins, n, outs))
         return _results(outs, keep if want_fields else None)
 
+    def solve_device_moduli(self, domains, e_ptrs):
+        """solve() with each domain's per-voxel moduli in device memory: e_ptrs[i] is the device
+        address of L0*L1*L2 float32 values (x fastest), or 0 for none."""
+        n = len(domains)
+        ins = (capi.DomainIn * n)(*[d.struct for d in domains])
+        outs = (capi.DomainOut * n)()
+        ptrs = (C.c_void_p * n)(*[C.c_void_p(int(p)) if p else None for p in e_ptrs])
+        self._check(self.lib.dtc_solve_batch_device_moduli(self.handle, ins, n, outs, ptrs))
+        return _results(outs, None)
+
+    def energy_grad_device(self, dloss_dc, grad_ptrs):
+        """energy_grad() into device memory: grad_ptrs[i] is the device address of the L0*L1*L2
+        float32 gradient of domain i."""
+        dl = np.ascontiguousarray(np.asarray(dloss_dc, dtype=np.float64).reshape(-1, 6, 6).transpose(0, 2, 1))
+        n = dl.shape[0]
+        ptrs = (C.c_void_p * n)(*[C.c_void_p(int(p)) for p in grad_ptrs])
+        self._check(self.lib.dtc_energy_grad_device(self.handle, dl.ctypes.data_as(C.POINTER(C.c_double)), ptrs, n))
+
     def rotation_search(self, ee):
         """CR1/CR2 rotation search of given symmetric 6x6 tensors (n x 6 x 6): result dicts with
         the "cr1" and "cr2" entries of solve()."""

@@ -7,7 +7,8 @@
 
 Forward: one dtc_solve_batch with the per-voxel moduli E (keep_displacements = 1; batches
 larger than the device memory are solved in chunks whose displacements are checkpointed to
-the host).  Backward: dL/dE_v = a * sum_{a,b} G_ab u_a,v^T Khat u_b,v with
+the host).  A CUDA tensor E on the solver's device goes through the device-pointer entries:
+dtc_solve_batch_device_moduli reads it, dtc_energy_grad_device writes E.grad in place.  Backward: dL/dE_v = a * sum_{a,b} G_ab u_a,v^T Khat u_b,v with
 G = vv^-1 dL/dff, the derivative of the energy products u_a^T K u_b of the converged load
 cases -- the operator is self-adjoint, so the forward displacements are the adjoint solution.
 The reference has no gradient; this is an extension of its homogenisation
@@ -22,11 +23,22 @@ from . import Domain, Solver, synth
 class _EffectiveStiffnessFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, E, module):
-        e_np = E.detach().to(torch.float32).cpu().numpy()
-        doms = [Domain(p, E=module.E_ref, nu=module.nu, delta=module.delta, E_voxel=np.ascontiguousarray(e_np[i]),
-                       llimit=module.llimit)
-                for i, p in enumerate(module.phis)]
-        res = module.solver.solve(doms)
+        on_device = E.is_cuda and E.device.index == module.device
+        if on_device:
+            # the moduli stay on the device: the library copies them once through its own pinned
+            # buffer (dtc_solve_batch_device_moduli)
+            e_dev = E.detach().to(torch.float32).contiguous()
+            torch.cuda.current_stream(E.device).synchronize()
+            doms = [Domain(p, E=module.E_ref, nu=module.nu, delta=module.delta, llimit=module.llimit)
+                    for p in module.phis]
+            res = module.solver.solve_device_moduli(doms, [e_dev[i].data_ptr() for i in range(e_dev.shape[0])])
+        else:
+            e_np = E.detach().to(torch.float32).cpu().numpy()
+            doms = [Domain(p, E=module.E_ref, nu=module.nu, delta=module.delta,
+                           E_voxel=np.ascontiguousarray(e_np[i]), llimit=module.llimit)
+                    for i, p in enumerate(module.phis)]
+            res = module.solver.solve(doms)
+        ctx.on_device = on_device
         module._generation += 1
         ctx.module = module
         ctx.generation = module._generation
@@ -42,7 +54,12 @@ class _EffectiveStiffnessFn(torch.autograd.Function):
         if m._generation != ctx.generation:
             raise RuntimeError("EffectiveStiffness: backward must follow its own forward (the solver keeps the "
                                "displacements of its last forward only)")
-        dl = grad_c.detach().to(torch.float64).cpu().numpy()
+        dl = grad_c.detach().to(torch.float64).cpu().numpy()   # B x 36 values
+        if ctx.on_device:
+            g = torch.empty(ctx.shape, dtype=torch.float32, device=ctx.device)
+            torch.cuda.current_stream(ctx.device).synchronize()
+            m.solver.energy_grad_device(dl, [g[i].data_ptr() for i in range(ctx.shape[0])])
+            return g.to(dtype=ctx.dtype), None
         grads = [np.zeros(ctx.shape[1:], np.float32) for _ in range(ctx.shape[0])]
         m.solver.energy_grad(dl, grads)
         g = torch.from_numpy(np.stack(grads)).to(device=ctx.device, dtype=ctx.dtype)
@@ -58,6 +75,7 @@ class EffectiveStiffness(torch.nn.Module):
         super().__init__()
         self.phis = [np.asarray(p) for p in phis]
         self.delta, self.nu, self.E_ref, self.llimit = delta, nu, E_ref, llimit
+        self.device = device
         self.solver = Solver(precision=precision, rtol=rtol, max_it=max_it, rotation_search=False, device=device,
                              keep_displacements=True, inner_precond=inner_precond, estimator=estimator)
         self._generation = 0

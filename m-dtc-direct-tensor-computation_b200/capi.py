@@ -103,6 +103,9 @@ SIGNATURES = {
     "dtc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "dtc_element_stiffness": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "dtc_get_kernel_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStats), C.c_int32, C.POINTER(C.c_int32)]),
+    "dtc_solve_batch_device_moduli": (C.c_int, [C.c_void_p, C.POINTER(DomainIn), C.c_int64, C.POINTER(DomainOut),
+                                                C.POINTER(C.c_void_p)]),
+    "dtc_energy_grad_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.c_int64]),
     "dtc_rotation_search": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POINTER(DomainOut)]),
     "dtc_rotation_search_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p]),

@@ -22,6 +22,11 @@ struct dtc_handle {
   dtc::DeviceSolver solver;
   std::string err;
   dtc::SolverStats last;
+  float* staging = nullptr;   // pinned host copy of device-resident moduli (dtc_solve_batch_device_moduli)
+  size_t staging_n = 0;
+  ~dtc_handle() {
+    if (staging) cudaFreeHost(staging);
+  }
 };
 
 namespace {
@@ -339,6 +344,47 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
   return DTC_OK;
 }
 
+dtc_status dtc_solve_batch_device_moduli(dtc_handle* h, const dtc_domain_in* in, int64_t n, dtc_domain_out* out,
+                                         const float* const* E_voxel_dev) {
+  if (!h) return DTC_ERR_INVALID_ARGUMENT;
+  h->err.clear();
+  if (n < 0 || (n > 0 && (!in || !out || !E_voxel_dev))) { h->err = "in/out/E_voxel_dev must be non-NULL for n > 0"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (n == 0) return DTC_OK;
+  if (cudaSetDevice(h->opt.device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
+  size_t total = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (E_voxel_dev[i]) {
+      if (in[i].L[0] < 1 || in[i].L[1] < 1 || in[i].L[2] < 1) { h->err = "L must be >= 1"; return DTC_ERR_INVALID_ARGUMENT; }
+      total += (size_t)in[i].L[0] * in[i].L[1] * in[i].L[2];
+    }
+  if (total > h->staging_n) {
+    if (h->staging) cudaFreeHost(h->staging);
+    h->staging = nullptr;
+    h->staging_n = 0;
+    if (cudaMallocHost(&h->staging, sizeof(float) * total) != cudaSuccess) {
+      h->staging = nullptr;
+      h->err = "cudaMallocHost failed for the moduli staging buffer";
+      return DTC_ERR_OUT_OF_MEMORY;
+    }
+    h->staging_n = total;
+  }
+  std::vector<dtc_domain_in> loc(in, in + n);
+  size_t off = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!E_voxel_dev[i]) continue;
+    const size_t nv = (size_t)in[i].L[0] * in[i].L[1] * in[i].L[2];
+    if (cudaMemcpyAsync(h->staging + off, E_voxel_dev[i], sizeof(float) * nv, cudaMemcpyDeviceToHost, nullptr) !=
+        cudaSuccess) {
+      h->err = "copying the device moduli failed";
+      return DTC_ERR_CUDA;
+    }
+    loc[i].E_voxel = h->staging + off;
+    off += nv;
+  }
+  if (cudaStreamSynchronize(nullptr) != cudaSuccess) { h->err = "copying the device moduli failed"; return DTC_ERR_CUDA; }
+  return dtc_solve_batch(h, loc.data(), n, out);
+}
+
 dtc_status dtc_rotation_search(dtc_handle* h, const double* ee, int64_t n, dtc_domain_out* out) {
   if (!h) return DTC_ERR_INVALID_ARGUMENT;
   h->err.clear();
@@ -398,7 +444,15 @@ dtc_status dtc_energy_grad(dtc_handle* h, const double* dloss_dc, float* const* 
   h->err.clear();
   if (!h->opt.keep_displacements) { h->err = "energy_grad needs keep_displacements = 1"; return DTC_ERR_INVALID_ARGUMENT; }
   if (cudaSetDevice(h->opt.device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
-  return (dtc_status)h->solver.energy_grad(dloss_dc, grad_e, n, h->err);
+  return (dtc_status)h->solver.energy_grad(dloss_dc, grad_e, n, false, h->err);
+}
+
+dtc_status dtc_energy_grad_device(dtc_handle* h, const double* dloss_dc, float* const* grad_e_dev, int64_t n) {
+  if (!h || (n > 0 && (!dloss_dc || !grad_e_dev)) || n < 0) return DTC_ERR_INVALID_ARGUMENT;
+  h->err.clear();
+  if (!h->opt.keep_displacements) { h->err = "energy_grad needs keep_displacements = 1"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (cudaSetDevice(h->opt.device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
+  return (dtc_status)h->solver.energy_grad(dloss_dc, grad_e_dev, n, true, h->err);
 }
 
 dtc_status dtc_get_stats(const dtc_handle* h, double* ms_solve, int64_t* kernel_launches, double* dof_iterations) {

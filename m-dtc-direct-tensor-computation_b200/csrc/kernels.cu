@@ -870,9 +870,10 @@ int DeviceSolver::init(int device, std::string& msg) {
   return DTC_OK;
 }
 
-void launch_matvec_tc(const Tile* tiles, int64_t ntiles, const DomDev* doms, const float* svox,
-                      const uint8_t* flags, const float* u, float* y, double* acc_pw, const int* dom_active, int* err,
-                      cudaStream_t s);
+void launch_sweep_tc(int mode, const Tile* tiles, int64_t ntiles, const DomDev* doms, const float* svox,
+                     const uint8_t* flags, const float* binv, const float* b, const float* u, float* y, float scale,
+                     float omega, double* acc1, double* acc2, const int* dom_active, int* err, cudaStream_t s);
+int allow_sweep_tc(std::string& msg);
 int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg);
 int set_tc_spin_limit(long long spins, cudaStream_t s, std::string& msg);
 void build_tc20_operand(const double* k20, float* img);
@@ -1313,6 +1314,8 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
       launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
     k_mg_combine<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, om, nullptr, nullptr, act);
     ++launches;
+  } else if (fine && I.tensor_matvec) {
+    launch_sweep_tc(kTcRes, tsm, nsm, dl, sv, fl, bi, b, cur, rbuf, 1.0f, om, nullptr, nullptr, act, M.err, s);
   } else {
     k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   }
@@ -1338,7 +1341,9 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
       launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, dl, sv, fl, M.ke32, t, z, -1.0, nullptr, act, s);
     k_mg_combine<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, t, z, P.omega0, zz, zr, act);
     ++launches;
-  } else if (l == 0)
+  } else if (l == 0 && I.tensor_matvec)
+    launch_sweep_tc(kTcPost, tsm, nsm, dl, sv, fl, bi, b, t, z, 1.0f, P.omega0, zz, zr, act, M.err, s);
+  else if (l == 0)
     k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
   else if (twice) {
     // z holds the corrected iterate: t = z + w D^-1 (b - K z), then z = t + w D^-1 (b - K t)
@@ -1522,8 +1527,8 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
           I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
           q = I.begin(0);
           if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
-            launch_matvec_tc(ti, nti, dd, B<float>(I, bSvox), fl, (const float*)p, (float*)w, pw, act,
-                             B<int>(I, bErr), s);
+            launch_sweep_tc(kTcApply, ti, nti, dd, B<float>(I, bSvox), fl, nullptr, nullptr, (const float*)p,
+                            (float*)w, 1.0f, 0.0f, pw, nullptr, act, B<int>(I, bErr), s);
           else
             apply_k<T, NEN, false, true>(Wc, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
@@ -1617,7 +1622,8 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
           if (NEN == 8 && I.tensor_matvec)
-            launch_matvec_tc(Wc.ti, Wc.nti, dd, B<float>(I, bSvox), fl, p, w, pw, act, B<int>(I, bErr), s);
+            launch_sweep_tc(kTcApply, Wc.ti, Wc.nti, dd, B<float>(I, bSvox), fl, nullptr, nullptr, p, w, 1.0f, 0.0f,
+                            pw, nullptr, act, B<int>(I, bErr), s);
           else
             apply_k<float, NEN, false, true>(Wc, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
@@ -1852,8 +1858,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
     if (int e = upload_tc_operand(kh, s, msg)) return e;
-    if (I.tensor_matvec)
+    if (I.tensor_matvec) {
       if (int e = set_tc_spin_limit(opt.tc_wait_spins, s, msg)) return e;
+      if (int e = allow_sweep_tc(msg)) return e;
+    }
     if (NEN == 20) {
       std::vector<double> k20(3600);
       std::vector<float> k20f(3600);
@@ -2332,7 +2340,8 @@ void dloss_dff(const double* dc, const int64_t L[3], const double delta, double*
 
 }  // namespace
 
-int DeviceSolver::energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, std::string& msg) {
+int DeviceSolver::energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, bool grad_on_device,
+                              std::string& msg) {
   Impl& I = *impl_;
   DTC_CUDA(cudaSetDevice(I.device));
   cudaStream_t s = I.stream;
@@ -2424,6 +2433,17 @@ int DeviceSolver::energy_grad(const double* dloss_dc, float* const* grad_e, int6
       k_energy_grad<<<(unsigned)(vb.size() / 2), 128, 0, s>>>(blocks + nb.size(), B<DomDev>(I, bAdjDoms), sv, X,
                                                               B<double>(I, bAdjV), B<float>(I, bAdjGrad));
     if ((e = launch_check(msg))) return e;
+    if (grad_on_device) {
+      for (int d = 0; d < nd; ++d) {
+        const int64_t k = ch.index[d];
+        if (k < 0 || k >= n || !grad_e[k]) continue;
+        const DomDev& D = ch.doms[d];
+        DTC_CUDA(cudaMemcpyAsync(grad_e[k], B<float>(I, bAdjGrad) + D.vox_off,
+                                 sizeof(float) * (size_t)D.L[0] * D.L[1] * D.L[2], cudaMemcpyDeviceToDevice, s));
+      }
+      DTC_CUDA(cudaStreamSynchronize(s));
+      continue;
+    }
     std::vector<float> hg((size_t)ch.voxels);
     if (ch.voxels)
       DTC_CUDA(cudaMemcpyAsync(hg.data(), I.bufs[bAdjGrad], sizeof(float) * hg.size(), cudaMemcpyDeviceToHost, s));

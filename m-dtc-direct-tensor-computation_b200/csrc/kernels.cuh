@@ -31,6 +31,20 @@ __device__ __forceinline__ int64_t vec_index(int64_t node, int c, int lc) {
   return (node * 3 + c) * kNLC + lc;
 }
 
+// z = omega * D^-1 r with D^-1 the symmetric 3x3 node-block inverse (00, 11, 22, 01, 02, 12)
+__device__ __forceinline__ void block_jacobi(const float* __restrict__ binv, int64_t n, float omega, const float (&r)[3],
+                                             float (&z)[3]) {
+  const float* b = binv + n * 6;
+  const float b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2), b3 = __ldg(b + 3), b4 = __ldg(b + 4),
+              b5 = __ldg(b + 5);
+  z[0] = omega * (b0 * r[0] + b3 * r[1] + b4 * r[2]);
+  z[1] = omega * (b3 * r[0] + b1 * r[1] + b5 * r[2]);
+  z[2] = omega * (b4 * r[0] + b5 * r[1] + b2 * r[2]);
+}
+
+// Epilogues of the tensor-core HEX08 sweep (matvec_tc.cu, launch_sweep_tc)
+enum { kTcApply = 0, kTcRes = 1, kTcPost = 2 };
+
 template <typename T>
 __device__ __forceinline__ T block_sum_lc(T v, T* smem /* 4 warps x 8 */) {
   // threads with equal (threadIdx.x & 7) carry the same load case

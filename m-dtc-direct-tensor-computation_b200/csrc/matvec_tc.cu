@@ -1,20 +1,11 @@
 // matvec_tc.cu -- the voxel stiffness contraction on the 5th-generation tensor cores (sm_100a).
 //
-// w = K p on the interior nodes of one tile (8 x 4 x 4 owned nodes) for one group of 8 load
-// cases.  Every kept voxel v adjacent to an owned node contributes s_v * Khat * p_v, where
-// p_v holds the 24 DOFs of its 8 corners.  Per round the CTA stacks 16 voxels x 8 load cases
-// as the 128 rows of A (K = 24 voxel DOFs), multiplies by B = Khat (N = 24 output DOFs,
-// padded to 32) with tcgen05.mma kind::tf32 into a 128 x 32 FP32 accumulator in tensor
-// memory, reads it back with tcgen05.ld and adds s_v * D into shared-memory node
-// accumulators (only owned nodes are kept, so voxels on the tile rim are evaluated by every
-// tile they touch and no global atomics are needed).
-//
-// Precision: FP32 operands are split into tf32 hi + lo parts and the product is formed as
-// A_hi B_hi + A_hi B_lo + A_lo B_hi (nine K=8 MMAs per round), which recovers FP32-level
-// accuracy; accumulation is FP32 in TMEM.
-//
-// Waits: the one mbarrier wait per round is bounded; on time-out the kernel records an
-// error code, waits (bounded) for its own MMAs, frees its tensor memory and returns.
+// HEX08 (k_sweep_tc): the three fine-level sweeps of the FP32 inner solve -- the CG operator
+// application, the multigrid residual and the post-smoothing -- with the 24 x 24 voxel
+// contraction as tcgen05.mma kind::tf32, A (voxel DOFs x load cases) in tensor memory, B (the
+// unit voxel stiffness) in shared memory.  HEX20 (k_ebe_tc): the 60 x 60 element contraction
+// of the brick kernel, A and B in shared memory.  Both split FP32 operands into tf32 hi + lo
+// parts (three products) for FP32-level accuracy and bound every wait.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -115,17 +106,90 @@ int set_tc_spin_limit(long long spins, cudaStream_t s, std::string& msg) {
   return DTC_OK;
 }
 
+// -------------------------------------------------------------------------------------
+// HEX08 sweeps of the FP32 inner solve on the tensor cores.
+//
+// One CTA = one node tile (8 x 4 x 4 owned nodes) x one group of 8 load cases; it evaluates
+// every kept voxel adjacent to an owned node.  A round takes 16 of these voxels: thread
+// tid owns row tid of the MMA (voxel tid / 8 of the round, load case tid % 8), loads that
+// voxel's 24 corner DOFs of its load case straight from the nodal vector into registers,
+// splits them into tf32 hi + lo and stores the two halves into its own tensor-memory lane
+// (the A operand, columns 0-23 and 24-47).  One thread then issues
+//     D = A_hi B_hi + A_hi B_lo + A_lo B_hi      (B = Khat, split on the host; 3 K-chunks)
+// as nine tcgen05.mma kind::tf32 (M = 128, N = 32, K = 8) with A read from tensor memory and
+// B from shared memory, into one of two 32-column accumulators.  While those run, every
+// thread reads the previous round's accumulator row (tcgen05.ld: the voxel's 24 outputs),
+// scales it by the voxel's modulus factor and adds the outputs of owned nodes into shared
+// memory.  After the last round the owned active nodes get the sweep's own epilogue:
+//   kTcApply: y = scale * K u,                              acc1 += u . y  (CG: p . K p)
+//   kTcRes  : y = b - K u                                   (multigrid residual)
+//   kTcPost : y = u + omega D^-1 (b - K u),  acc1 += y . y, acc2 += y . b   (post-smoothing)
+// Precision: the split recovers FP32-level products (the tf32 rounding of the lo parts costs
+// at most 2^-21 relative); accumulation is FP32 in tensor memory, then FP64 for the scale.
+// Waits: every completion wait is bounded by g_tc_spin_limit polls; on time-out the CTA
+// records the error, waits (full bound) for the MMAs it committed, frees its tensor memory
+// and returns.
+namespace tc {
+constexpr int kSweepVox = 16;                        // voxels per round (x 8 load cases = 128 rows)
+constexpr uint32_t kColAHi = 0, kColALo = 24;        // A operand columns
+constexpr uint32_t kColD0 = 64, kColD1 = 96;         // the two accumulators
+constexpr uint32_t kSweepCols = 128;                 // tensor-memory columns per CTA
+constexpr int kSweepAccBytes = 128 * 3 * 8 * 4;      // owned node x comp x load case (floats)
+// dynamic shared memory per CTA: B (6 KB) + accumulators (12 KB), padded so that at most four
+// CTAs share an SM (4 x 128 columns = the SM's 512 tensor-memory columns)
+constexpr int kSweepSmem = 52 * 1024;
+
+__device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
+  uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// local corner lm (the mesher's HEX08 order) -> offsets
+__device__ __forceinline__ int corner_dx(int lm) { return (lm == 1 || lm == 2 || lm == 5 || lm == 6) ? 1 : 0; }
+__device__ __forceinline__ int corner_dy(int lm) { return (lm == 2 || lm == 3 || lm == 6 || lm == 7) ? 1 : 0; }
+__device__ __forceinline__ int corner_dz(int lm) { return lm >= 4 ? 1 : 0; }
+}  // namespace tc
+
 // Khat split into tf32 hi / lo, laid out as 6 canonical B chunks (hi k0..2, lo k0..2).
 __constant__ float c_bsplit[6 * tc::kN * tc::kKc];
 
+template <int MODE>
 __global__ void __launch_bounds__(128, 4)
-    k_matvec_tc(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms, const float* __restrict__ svox,
-                const uint8_t* __restrict__ flags, const float* __restrict__ u, float* __restrict__ y,
-                double* __restrict__ acc_pw, const int* __restrict__ dom_active, int* __restrict__ err) {
+    k_sweep_tc(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms, const float* __restrict__ svox,
+               const uint8_t* __restrict__ flags, const float* __restrict__ binv, const float* __restrict__ b,
+               const float* __restrict__ u, float* __restrict__ y, float scale, float omega,
+               double* __restrict__ acc1, double* __restrict__ acc2, const int* __restrict__ dom_active,
+               int* __restrict__ err) {
   using namespace tc;
-  __shared__ __align__(1024) unsigned char sA[2 * 3 * kAChunkBytes];   // 24 KB: hi chunks, lo chunks
-  __shared__ __align__(1024) unsigned char sB[6 * kBChunkBytes];       // 6 KB
-  __shared__ float acc[128 * 3 * 8];                                    // owned node x comp x lc
+  extern __shared__ __align__(1024) unsigned char dsm[];
+  unsigned char* sB = dsm;                                        // 6 KB, canonical K-major chunks
+  float* acc = reinterpret_cast<float*>(dsm + 6 * kBChunkBytes);   // 12 KB
   __shared__ int vlist[kMaxVox];
   __shared__ float vscale[kMaxVox];
   __shared__ int wcount[4];
@@ -142,7 +206,7 @@ __global__ void __launch_bounds__(128, 4)
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(kTmemCols));
+                 "r"(kSweepCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
@@ -153,7 +217,7 @@ __global__ void __launch_bounds__(128, 4)
   for (int i = tid; i < 6 * kN * kKc; i += 128) reinterpret_cast<float*>(sB)[i] = c_bsplit[i];
   for (int i = tid; i < 128 * 3 * 8; i += 128) acc[i] = 0.0f;
 
-  // kept voxels adjacent to the owned nodes, deterministic order
+  // kept voxels adjacent to the owned nodes, in x-fastest order
   const int L0 = D.L[0], L1 = D.L[1], L2 = D.L[2];
   int nv = 0;
   for (int base = 0; base < kMaxVox; base += 128) {
@@ -164,8 +228,7 @@ __global__ void __launch_bounds__(128, 4)
       const int ix = q % 9, iy = (q / 9) % 5, iz = q / 45;
       const int vx = t.x0 - 1 + ix, vy = t.y0 - 1 + iy, vz = t.z0 - 1 + iz;
       if (vx >= 0 && vy >= 0 && vz >= 0 && vx < L0 && vy < L1 && vz < L2) {
-        const int64_t o = vx + (int64_t)L0 * (vy + (int64_t)L1 * vz);
-        sv = __ldg(svox + D.vox_off + o);
+        sv = __ldg(svox + D.vox_off + vx + (int64_t)L0 * (vy + (int64_t)L1 * vz));
         if (sv != 0.0f) vidx = vx + L0 * (vy + L1 * vz);
       }
     }
@@ -182,127 +245,188 @@ __global__ void __launch_bounds__(128, 4)
     nv += wcount[0] + wcount[1] + wcount[2] + wcount[3];
     __syncthreads();
   }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B visible to the tensor cores
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  const uint32_t sA_addr = smem_u32(sA), sB_addr = smem_u32(sB);
-  const int lcl = tid & 7, lc = g * 8 + lcl;
-  const int rounds = (nv + kVoxPerRound - 1) / kVoxPerRound;
-  const int lo_x = 1, hi_x = L0 - 1, hi_y = L1 - 1, hi_z = L2 - 1;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t sB_addr = smem_u32(sB);
+  const int lcl = tid & 7, lc = g * kLcGroup + lcl;
+  const int rounds = (nv + kSweepVox - 1) / kSweepVox;
+  const long long lim = g_tc_spin_limit;
+  const int64_t nx = D.n[0], nxy = (int64_t)D.n[0] * D.n[1];
+  const int hi_x = D.n[0] - 2, hi_y = D.n[1] - 2, hi_z = D.n[2] - 2;
 
-  int rd = 0;
-  for (; rd < rounds; ++rd) {
-    const int vs = rd * kVoxPerRound + (tid >> 3);
-    int vx = 0, vy = 0, vz = 0;
-    float a[kK];
-    if (vs < nv) {
-      const int vi = vlist[vs];
-      vx = vi % L0; vy = (vi / L0) % L1; vz = vi / (L0 * L1);
+  int committed = 0;
+  for (int rd = 0; rd <= rounds; ++rd) {
+    // (1) this round's A row: the voxel's 24 corner DOFs of this thread's load case
+    uint32_t av[48];
+    if (rd < rounds) {
+      const int vs = rd * kSweepVox + (tid >> 3);
+      float a[24];
+      if (vs < nv) {
+        const int vi = vlist[vs];
+        const int vx = vi % L0, vy = (vi / L0) % L1, vz = vi / (L0 * L1);
+        const int64_t n0 = D.node_off + vx + nx * vy + nxy * vz;
 #pragma unroll
-      for (int lm = 0; lm < 8; ++lm) {
-        const int ox = (lm == 1 || lm == 2 || lm == 5 || lm == 6), oy = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
-                  oz = lm >= 4;
-        const int64_t nb = vec_index(node_index(D, vx + ox, vy + oy, vz + oz), 0, lc);
+        for (int lm = 0; lm < 8; ++lm) {
+          const int64_t nb = vec_index(n0 + corner_dx(lm) + nx * corner_dy(lm) + nxy * corner_dz(lm), 0, lc);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) a[3 * lm + c] = __ldg(u + nb + c * kNLC);
+          for (int c = 0; c < 3; ++c) a[3 * lm + c] = __ldg(u + nb + c * kNLC);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 24; ++k) a[k] = 0.0f;
       }
-    } else {
 #pragma unroll
-      for (int k = 0; k < kK; ++k) a[k] = 0.0f;
+      for (int k = 0; k < 24; ++k) {
+        const uint32_t hb = __float_as_uint(a[k]) & 0xFFFFE000u;   // tf32 hi: exact, low 13 bits clear
+        av[k] = hb;
+        av[24 + k] = __float_as_uint(a[k] - __uint_as_float(hb));
+      }
     }
-    // A hi / lo chunks in canonical layout
-#pragma unroll
-    for (int k = 0; k < kK; ++k) {
-      const float hi = to_tf32(a[k]);
-      const float lo = to_tf32(a[k] - hi);
-      const int kc = k >> 3, kk = k & 7;
-      *reinterpret_cast<float*>(sA + kc * kAChunkBytes + canon_offset(tid, kk)) = hi;
-      *reinterpret_cast<float*>(sA + (3 + kc) * kAChunkBytes + canon_offset(tid, kk)) = lo;
+    // (2) the MMAs of the previous round have finished: A is free, its accumulator is ready
+    if (rd >= 1 && !mbar_wait(smem_u32(&mbar), (uint32_t)((rd - 1) & 1), lim)) atomicOr(&fail, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // (3) store A, then one thread issues this round's MMAs
+    if (rd < rounds) {
+      tmem_st16(lane_addr + kColAHi, av);
+      tmem_st16(lane_addr + kColAHi + 16, av + 16);
+      tmem_st16(lane_addr + kColAHi + 32, av + 32);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int kc = 0; kc < 3; ++kc) {
-        const uint64_t ahi = smem_desc(sA_addr + kc * kAChunkBytes), alo = smem_desc(sA_addr + (3 + kc) * kAChunkBytes);
-        const uint64_t bhi = smem_desc(sB_addr + kc * kBChunkBytes), blo = smem_desc(sB_addr + (3 + kc) * kBChunkBytes);
-        mma_tf32(tmem, ahi, bhi, kc > 0 ? 1u : 0u);
-        mma_tf32(tmem, ahi, blo, 1u);
-        mma_tf32(tmem, alo, bhi, 1u);
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&mbar))
-                   : "memory");
-    }
-    if (!mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1), g_tc_spin_limit)) atomicOr(&fail, 1);
-    __syncthreads();
     if (fail) break;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (vs < nv) {
-      const float s = vscale[vs];
+    if (rd < rounds) {
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + ((rd & 1) ? kColD1 : kColD0);
 #pragma unroll
-      for (int lm = 0; lm < 8; ++lm) {
-        const int ox = (lm == 1 || lm == 2 || lm == 5 || lm == 6), oy = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
-                  oz = lm >= 4;
-        const int nx = vx + ox, ny = vy + oy, nz = vz + oz;
-        const int lx = nx - t.x0, ly = ny - t.y0, lz = nz - t.z0;
-        const bool own = lx >= 0 && lx < kTileX && ly >= 0 && ly < kTileY && lz >= 0 && lz < kTileZ && nx >= lo_x &&
-                         nx <= hi_x && ny >= 1 && ny <= hi_y && nz >= 1 && nz <= hi_z;
-        if (own) {
-          const int nl = lx + kTileX * (ly + kTileY * lz);
+        for (int kc = 0; kc < 3; ++kc) {
+          const uint64_t bhi = smem_desc(sB_addr + kc * kBChunkBytes), blo = smem_desc(sB_addr + (3 + kc) * kBChunkBytes);
+          mma_ts(d, tmem + kColAHi + 8 * kc, bhi, kc > 0 ? 1u : 0u);
+          mma_ts(d, tmem + kColAHi + 8 * kc, blo, 1u);
+          mma_ts(d, tmem + kColALo + 8 * kc, bhi, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+      }
+      ++committed;
+    }
+    // (4) the previous round's outputs into the owned nodes, while this round's MMAs run
+    if (rd >= 1) {
+      uint32_t r[32];
+      tmem_ld32(lane_addr + (((rd - 1) & 1) ? kColD1 : kColD0), r);
+      const int vs = (rd - 1) * kSweepVox + (tid >> 3);
+      if (vs < nv) {
+        const int vi = vlist[vs];
+        const int vx = vi % L0, vy = (vi / L0) % L1, vz = vi / (L0 * L1);
+        const float s = vscale[vs];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) atomicAdd(&acc[(nl * 3 + c) * 8 + lcl], s * __uint_as_float(r[3 * lm + c]));
+        for (int lm = 0; lm < 8; ++lm) {
+          const int ox = vx + corner_dx(lm), oy = vy + corner_dy(lm), oz = vz + corner_dz(lm);
+          const int lx = ox - t.x0, ly = oy - t.y0, lz = oz - t.z0;
+          const bool own = lx >= 0 && lx < kTileX && ly >= 0 && ly < kTileY && lz >= 0 && lz < kTileZ && ox >= 1 &&
+                           ox <= hi_x && oy >= 1 && oy <= hi_y && oz >= 1 && oz <= hi_z;
+          if (own) {
+            const int nl = lx + kTileX * (ly + kTileY * lz);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) atomicAdd(&acc[(nl * 3 + c) * 8 + lcl], s * __uint_as_float(r[3 * lm + c]));
+          }
         }
       }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
   }
   if (fail) {
     if (tid == 0) atomicExch(err, 1);
-    mbar_wait(smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this iteration's MMAs
+    // bounded with the full limit: wait for the last committed MMAs before freeing their memory
+    if (committed > 0) mbar_wait(smem_u32(&mbar), (uint32_t)((committed - 1) & 1));
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kSweepCols));
   }
   if (fail) return;
-  // owned interior nodes: w = scale * acc, dot with p
-  double dot = 0.0;
-  const int nsub = tid >> 3;  // 16 node slots per pass
-  for (int nl = nsub; nl < 128; nl += 16) {
+  // owned active interior nodes: the sweep's epilogue
+  double d1 = 0.0, d2 = 0.0;
+  for (int nl = tid >> 3; nl < 128; nl += 16) {
     const int lx = nl % kTileX, ly = (nl / kTileX) % kTileY, lz = nl / (kTileX * kTileY);
     const int x = t.x0 + lx, yv = t.y0 + ly, z = t.z0 + lz;
     if (x > hi_x || yv > hi_y || z > hi_z) continue;
     const int64_t node = node_index(D, x, yv, z);
-    if (!(flags[node] & kNodeActive)) continue;  // void node: w stays 0
-    float v[3];
+    if (!(flags[node] & kNodeActive)) continue;  // void node: not written
+    const int64_t k0 = vec_index(node, 0, lc);
+    float ku[3], v[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) v[c] = (float)(D.scale * (double)acc[(nl * 3 + c) * 8 + lcl]);
-    const int64_t b = vec_index(node, 0, lc);
+    for (int c = 0; c < 3; ++c) ku[c] = (float)(D.scale * (double)acc[(nl * 3 + c) * 8 + lcl]);
+    if (MODE == kTcApply) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      y[b + c * kNLC] = v[c];
-      dot += (double)__ldg(u + b + c * kNLC) * (double)v[c];
+      for (int c = 0; c < 3; ++c) {
+        v[c] = scale * ku[c];
+        d1 += (double)__ldg(u + k0 + c * kNLC) * (double)v[c];
+      }
+    } else {
+      float bc[3], res[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        bc[c] = __ldg(b + k0 + c * kNLC);
+        res[c] = bc[c] - ku[c];
+      }
+      if (MODE == kTcRes) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = res[c];
+      } else {
+        float dz[3];
+        block_jacobi(binv, node, omega, res, dz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          v[c] = __ldg(u + k0 + c * kNLC) + dz[c];
+          d1 += (double)v[c] * (double)v[c];
+          d2 += (double)v[c] * (double)bc[c];
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) y[k0 + c * kNLC] = v[c];
+  }
+  if (MODE == kTcApply || MODE == kTcPost) {
+    const int64_t col = (int64_t)t.dom * kNLC + lc;
+    const double s1 = block_sum_lc<double>(d1, red);
+    if (threadIdx.x < 8) atomicAdd(acc1 + col, s1);
+    if (MODE == kTcPost) {
+      __syncthreads();
+      const double s2 = block_sum_lc<double>(d2, red);
+      if (threadIdx.x < 8) atomicAdd(acc2 + col, s2);
     }
   }
-  const double s = block_sum_lc<double>(dot, red);
-  if (threadIdx.x < 8) atomicAdd(acc_pw + (int64_t)t.dom * kNLC + lc, s);
+}
+
+int allow_sweep_tc(std::string& msg) {
+  DTC_CUDA(cudaFuncSetAttribute(k_sweep_tc<kTcApply>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSweepSmem));
+  DTC_CUDA(cudaFuncSetAttribute(k_sweep_tc<kTcRes>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSweepSmem));
+  DTC_CUDA(cudaFuncSetAttribute(k_sweep_tc<kTcPost>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSweepSmem));
+  return DTC_OK;
+}
+
+void launch_sweep_tc(int mode, const Tile* tiles, int64_t ntiles, const DomDev* doms, const float* svox,
+                     const uint8_t* flags, const float* binv, const float* b, const float* u, float* y, float scale,
+                     float omega, double* acc1, double* acc2, const int* dom_active, int* err, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  const unsigned grid = (unsigned)(3 * ntiles);
+  if (mode == kTcApply)
+    k_sweep_tc<kTcApply><<<grid, 128, tc::kSweepSmem, s>>>(tiles, doms, svox, flags, binv, b, u, y, scale, omega,
+                                                            acc1, acc2, dom_active, err);
+  else if (mode == kTcRes)
+    k_sweep_tc<kTcRes><<<grid, 128, tc::kSweepSmem, s>>>(tiles, doms, svox, flags, binv, b, u, y, scale, omega, acc1,
+                                                          acc2, dom_active, err);
+  else
+    k_sweep_tc<kTcPost><<<grid, 128, tc::kSweepSmem, s>>>(tiles, doms, svox, flags, binv, b, u, y, scale, omega,
+                                                           acc1, acc2, dom_active, err);
 }
 
 // Host: build the split Khat in the canonical B layout and upload it.
@@ -332,14 +456,6 @@ int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg) {
   DTC_CUDA(cudaMemcpyToSymbolAsync(c_bsplit, img, sizeof(img), 0, cudaMemcpyHostToDevice, s));
   return DTC_OK;
 }
-
-void launch_matvec_tc(const Tile* tiles, int64_t ntiles, const DomDev* doms, const float* svox,
-                      const uint8_t* flags, const float* u, float* y, double* acc_pw, const int* dom_active, int* err,
-                      cudaStream_t s) {
-  if (ntiles <= 0) return;
-  k_matvec_tc<<<(unsigned)(3 * ntiles), 128, 0, s>>>(tiles, doms, svox, flags, u, y, acc_pw, dom_active, err);
-}
-
 
 // -------------------------------------------------------------------------------------
 // HEX20: the 60x60 element contraction of the brick kernel (ebe.cuh) on the tensor cores.

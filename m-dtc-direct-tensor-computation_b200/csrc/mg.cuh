@@ -35,17 +35,6 @@ constexpr int kMgMaxCoarse = 4;                  // voxels per edge on the coars
 constexpr int kMgDenseN = 81;                    // 3 * 3^3 interior DOFs at most
 enum { kMgRes = 0, kMgPost = 1 };
 
-// z = omega * D^-1 r with D^-1 the symmetric 3x3 block inverse (00, 11, 22, 01, 02, 12)
-__device__ __forceinline__ void block_jacobi(const float* __restrict__ binv, int64_t n, float omega, const float (&r)[3],
-                                             float (&z)[3]) {
-  const float* b = binv + n * 6;
-  const float b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2), b3 = __ldg(b + 3), b4 = __ldg(b + 4),
-              b5 = __ldg(b + 5);
-  z[0] = omega * (b0 * r[0] + b3 * r[1] + b4 * r[2]);
-  z[1] = omega * (b3 * r[0] + b1 * r[1] + b5 * r[2]);
-  z[2] = omega * (b4 * r[0] + b5 * r[1] + b2 * r[2]);
-}
-
 __device__ __forceinline__ void load_plane_f(float (&pl)[3][3][3], const float* __restrict__ u, const DomDev& D, int x,
                                              int y, int z, int lc) {
 #pragma unroll

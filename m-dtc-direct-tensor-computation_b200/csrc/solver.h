@@ -119,7 +119,9 @@ class DeviceSolver {
   int solve(std::vector<DomainTask>& tasks, const dtc_options& opt, double nu, HostBatchPtr batch,
             std::string& msg);
   // Adjoint: dL/dE_voxel for the domains of the last solve (kept displacements).
-  int energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, std::string& msg);
+  // grad_on_device: grad_e[i] are device pointers on this solver's device (filled by device
+  // copies, no host round trip); else host pointers.
+  int energy_grad(const double* dloss_dc, float* const* grad_e, int64_t n, bool grad_on_device, std::string& msg);
   const SolverStats& stats() const { return stats_; }
   void set_keep(int mode) { keep_ = mode; }
   // Forget what earlier solves kept for the adjoint (start of a batch).

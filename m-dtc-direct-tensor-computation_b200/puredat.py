@@ -238,5 +238,102 @@ def write_scalar_tree(head_path, volume, spacing, origin=(0, 0, 0), shift=(0.0, 
     return Tree(head)
 
 
+# The result record of one domain: the 24 leaves of the "Averaged Material Properties" branch
+# (f-src_main/dtc.f90:738-777; f-src_main/struct_process.f90:704-741), in order, with their
+# type (4 = int8, 5 = real8) and values per domain for the linear macro element (24 load cases).
+RESULT_LEAVES = [
+    ("Domain number", 4, 1), ("Number of Elements", 4, 1), ("Number of Nodes", 4, 1), ("Collected logs", 4, 24),
+    ("Start Time", 5, 1), ("Duration", 5, 1), ("Domain forces", 5, 576), ("Effective numerical stiffness", 5, 576),
+    ("Symmetry deviation - effective numerical stiffness", 5, 1), ("Averaged stresses", 5, 144),
+    ("Averaged strains", 5, 144), ("Effective stiffness", 5, 36), ("Symmetry deviation - effective stiffness", 5, 1),
+    ("Averaged Effective stiffness", 5, 36), ("Symmetry deviation - Averaged effective stiffness", 5, 1),
+    ("Rotation Angle CR_1", 5, 1), ("Rotation Vector CR_1", 5, 3), ("Final coordinate system CR_1", 5, 9),
+    ("Optimized Effective stiffness CR_1", 5, 36), ("Rotation Angle CR_2", 5, 1), ("Rotation Vector CR_2", 5, 3),
+    ("Final coordinate system CR_2", 5, 9), ("Optimized Effective stiffness CR_2", 5, 36),
+    ("Effective density", 5, 1)]
+
+
+def _record_values(r, start_time, duration):
+    """The 24 leaf values of one result dict (Solver.solve), matrices flattened column-major
+    as the reference's reshape writes them."""
+    f = lambda m: np.asarray(m, dtype=float).reshape(-1, order="F")   # noqa: E731
+    cr = [r.get("cr1", {}), r.get("cr2", {})]
+    out = [[r["domain_number"]], [r["ne"]], [r["nn"]], np.asarray(r["iters"], dtype=np.int64),
+           [start_time], [duration], f(r["ff"]), f(r["kmacro"]), [r["sym_k"]],
+           np.zeros(144), np.zeros(144), f(r["c"]), [r["sym_c"]], f(r["ee"]), [r["sym_ee"]]]
+    for k in cr:
+        out += [[k.get("angle", 0.0)], np.asarray(k.get("n", np.zeros(3)), dtype=float),
+                f(k.get("aa", np.zeros((3, 3)))), f(k.get("ee", np.zeros((6, 6))))]
+    out.append([r["density"]])
+    return out
+
+
+def write_result_tree(head_path, results, *, name=None, start_time=0.0, duration=0.0, decomposition=None):
+    """Write the results of a batch (Solver.solve dicts, in domain order) as a PureDat tree with
+    the reference's result branch "Averaged Material Properties": its 24 leaves, each holding
+    the values of every domain back to back (domain i at offset i * values-per-domain, as the
+    reference's workers write them at their comm_nn offsets, f-src_main/struct_process.f90:
+    1230-1245), int8 leaves 1-4 in `<name>.int8.st`, real8 leaves 5-24 in `<name>.real8.st`.
+    decomposition: optional dict of the 'Global domain decomposition' leaves (x_D, x_D_phy,
+    delta, nn_D, ...) written as a branch before the results, like the reference's tree.
+    Leaf "Collected logs" holds each load case's CG iteration count (the reference logs its
+    24 stage marks there), "Averaged stresses/strains" hold zeros (the reference never computes
+    them), "Start Time"/"Duration" the given batch values."""
+    head = Path(head_path)
+    prefix = str(head)[: -len(".head")]
+    pos = {t: 1 for t in TYPES}
+    data = {t: [] for t in TYPES}
+
+    def add(desc, ty, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.dtype(TYPES[ty][1])).ravel()
+        lf = Leaf(desc, arr.size, ty, pos[ty], pos[ty] + arr.size - 1)
+        pos[ty] += arr.size
+        data[ty].append(arr)
+        return lf
+
+    branches = []
+    if decomposition:
+        dleaves = [add(k, 4 if np.asarray(v).dtype.kind in "iu" else 5, np.atleast_1d(v))
+                   for k, v in decomposition.items()]
+        branches.append(Branch("Global domain decomposition", leaves=dleaves))
+    recs = [_record_values(r, start_time, duration) for r in results]
+    leaves = []
+    for j, (desc, ty, per) in enumerate(RESULT_LEAVES):
+        vals = [np.asarray(rec[j]).ravel() for rec in recs]
+        if any(v.size != per for v in vals):
+            raise ValueError(f"leaf {desc!r}: expected {per} values per domain")
+        leaves.append(add(desc, ty, np.concatenate(vals) if vals else np.zeros(0)))
+    branches.append(Branch("Averaged Material Properties", leaves=leaves))
+    root = Branch(name or head.stem, branches=branches, streams=[pos[t] - 1 for t in (1, 2, 3, 4, 5, 6, 7)],
+                  log_sep=" ")
+    for t, arrs in data.items():
+        if arrs:
+            with open(f"{prefix}.{TYPES[t][0]}.st", "wb") as fh:
+                for a in arrs:
+                    fh.write(a.tobytes())
+    write_head(head, root)
+    return Tree(head)
+
+
+def read_result_tree(head_path):
+    """Per-domain records of a tree written by write_result_tree (or a reference result tree
+    laid out the same way): a list of dicts leaf description -> values of that domain."""
+    t = Tree(head_path)
+    res = None
+    def walk(b):
+        nonlocal res
+        if b.desc == "Averaged Material Properties":
+            res = b
+        for sb in b.branches:
+            walk(sb)
+    walk(t.root)
+    if res is None:
+        raise KeyError("no 'Averaged Material Properties' branch")
+    per = {d: n for d, _, n in RESULT_LEAVES}
+    n = res.leaves[0].dat_no // per[res.leaves[0].desc]
+    vals = {lf.desc: np.array(t.leaf_map(lf)).reshape(n, -1) for lf in res.leaves}
+    return [{d: v[i] for d, v in vals.items()} for i in range(n)]
+
+
 __all__ = ["Leaf", "Branch", "Tree", "read_head", "head_text", "write_head", "puredat_domains", "write_scalar_tree",
-           "TYPES"]
+           "write_result_tree", "read_result_tree", "RESULT_LEAVES", "TYPES"]

@@ -150,3 +150,29 @@ def test_autograd_function(dtc):
     assert torch.allclose(E.grad, torch.from_numpy(np.stack(g)))
     assert float(E.grad.abs().max()) > 0
     model.close()
+
+
+def test_autograd_function_device_tensors(dtc):
+    """E as a CUDA tensor: moduli in and gradient out through the device-pointer entries
+    (dtc_solve_batch_device_moduli, dtc_energy_grad_device); same C and gradient as the host path."""
+    torch = pytest.importorskip("torch")
+    from importlib import import_module
+    ag = import_module(dtc.__name__ + ".autograd")
+    syn = dtc.synth
+    grays = [syn.bone_volume((8, 8, 8), 0.4, syn.seed_for(4, 30 + i)) for i in range(3)]
+    E0 = np.stack([syn.modulus_of_gray(g) for g in grays])
+    target = torch.eye(6, dtype=torch.float64) * 5000.0
+    out = {}
+    for where in ("cpu", "cuda"):
+        E = torch.tensor(E0, requires_grad=True, device=where)
+        model = ag.EffectiveStiffness(grays, precision="fp64", rtol=1e-12)
+        C = model(E)
+        assert C.device.type == where
+        loss = ((C - target.to(where)) ** 2).sum()
+        loss.backward()
+        assert E.grad.device.type == where
+        out[where] = (C.detach().cpu().numpy(), E.grad.detach().cpu().numpy())
+        model.close()
+    assert np.abs(out["cuda"][0] - out["cpu"][0]).max() <= 1e-9 * np.abs(out["cpu"][0]).max()
+    assert np.abs(out["cuda"][1] - out["cpu"][1]).max() <= 1e-6 * np.abs(out["cpu"][1]).max()
+    assert np.abs(out["cuda"][1]).max() > 0

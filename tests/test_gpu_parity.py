@@ -54,7 +54,7 @@ def test_fp64_matches_oracle(dtc, batch):
 
 
 @pytest.mark.parametrize("matvec,precond", [("simt", "block"), ("tensor", "block"), ("simt", "jacobi"),
-                                            ("simt", "mg")])
+                                            ("simt", "mg"), ("tensor", "mg"), ("tensor", "jacobi")])
 def test_mixed_matches_oracle(dtc, batch, matvec, precond):
     pairs, refs = batch
     with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, mixed_matvec=matvec,
