@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--estimator", default="energy", choices=["energy", "reaction"])
     p.add_argument("--precond", default="mg", choices=["mg", "block", "jacobi"],
                    help="preconditioner of the FP32 inner solve of the mixed arm")
+    p.add_argument("--matvec", default="simt", choices=["simt", "tensor"],
+                   help="HEX08 fine-level sweeps of the mixed arm: SIMT FP32 or tcgen05 (3xTF32)")
     p.add_argument("--max-it", type=int, default=20000)
     p.add_argument("--check", type=int, default=16, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
@@ -316,6 +318,7 @@ def run_config(args, dtc):
                 res[:] = sv.solve(doms)
                 return sv.stats()["ms_solve"]
             dev, wall = _timed(step, steps, warm)
+            rot = sv.kernel_stats().get("rotation_search_f64", {})
         sample = [i for i in range(0, n, max(1, n // 12))]
         with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device=local) as ref:
             truth = ref.solve([doms[i] for i in sample])
@@ -325,6 +328,10 @@ def run_config(args, dtc):
                      "domains_per_s_device": n / (dev / 1e3), "domains_per_s_wall": n / wall, "ms_device": dev,
                      "ms_wall": 1e3 * wall, "domains_solved": ok,
                      "max_rel_err_vs_fp64_1e-10": _err([res[i] for i in sample], truth),
+                     "rotation_ms": rot.get("ms_total"), "rotation_us_per_domain":
+                         1e3 * rot["ms_total"] / n if rot else None,
+                     "rotation_fp64_tflops": (rot["flops_per_launch"] * rot["launches"] / (rot["ms_total"] / 1e3)
+                                              / 1e12 if rot and rot["ms_total"] > 0 else None),
                      "voxels": int(sum(int(L) ** 3 for L in Ls))})
     elif args.config == "c4":
         # adjoint: 64 HEX08 domains of 48^3, loss ||C - C_target||_F^2, gradient vs one forward solve
@@ -403,7 +410,7 @@ def main():
             doms = [dtc.Domain(g, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA,
                                E_voxel=syn.modulus_of_gray(g)) for g in grays]
         with dtc.Solver(precision="mixed", rtol=rt, max_it=args.max_it, rotation_search=False, device=local,
-                        estimator=args.estimator, inner_precond=args.precond) as sv:
+                        estimator=args.estimator, inner_precond=args.precond, mixed_matvec=args.matvec) as sv:
             sv.solve(doms)
             n0 = sv.stats()["kernel_launches"]
             sv.solve(doms)
@@ -424,7 +431,8 @@ def main():
         return max(float(np.abs(r["c"] - t).max() / np.abs(t).max()) for r, t in zip(res, truth))
 
     ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8, 3e-9, 1e-9]
-    arms = {"mixed": dict(precision="mixed", estimator=args.estimator, inner_precond=args.precond),
+    arms = {"mixed": dict(precision="mixed", estimator=args.estimator, inner_precond=args.precond,
+                          mixed_matvec=args.matvec),
             "fp64": dict(precision="fp64", estimator="reaction")}
     rtol_of, err_of = {}, {}
     for arm, kw in arms.items():
@@ -440,7 +448,7 @@ def main():
     # every rank times the same configuration: the tightest rtol any rank calibrated
     rtol_of["mixed"], rtol_of["fp64"] = reduce_over_ranks([rtol_of["mixed"], rtol_of["fp64"]], "min")
     mixed = dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
-                       device=local, estimator=args.estimator, inner_precond=args.precond)
+                       device=local, estimator=args.estimator, inner_precond=args.precond, mixed_matvec=args.matvec)
 
     def barrier():
         torch.cuda.synchronize()
@@ -482,7 +490,7 @@ def main():
     # dominant kernel: one extra, untimed-for-the-metric step with CUDA-event timing per launch
     with dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
                     device=local, profile_kernels=True, estimator=args.estimator,
-                    inner_precond=args.precond) as prof:
+                    inner_precond=args.precond, mixed_matvec=args.matvec) as prof:
         prof.solve(doms)
         ks = prof.kernel_stats()
     host = {k: ks.pop(k) for k in list(ks) if k.startswith("host_")}   # host phases, wall ms
@@ -501,6 +509,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": workload(args),
                 "rtol": rtol_of["mixed"], "estimator": args.estimator, "inner_precond": args.precond,
+                "matvec": args.matvec,
                 "max_rel_err_vs_fp64_1e-10": timed_err, "accuracy_target": TARGET, "accuracy_sample": nchk,
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),

@@ -93,10 +93,11 @@ typedef struct dtc_options {
                               CUDA graph; 1: kernels are launched one by one */
   int32_t tc_wait_spins;   /* tensor-core kernels: polls of a round's completion barrier before
                               the kernel gives up and the call returns DTC_ERR_INTERNAL
-                              (0 -> 2^26).  Only for testing that error path: a small value
-                              makes the wait run out; the drain before tensor memory is freed
-                              keeps the full bound */
-  int32_t reserved[1];
+                              (0 -> 2^26; < 0 -> no poll: every such wait gives up at once).
+                              Only for testing that error path; the drain before tensor memory
+                              is freed keeps the full bound */
+  int32_t device_mesher;   /* 1: mesh the domains on the device (the reference numbering, bit
+                              for bit the host planner's result); 0: on host threads */
 } dtc_options;
 
 typedef struct dtc_domain_in {
@@ -182,6 +183,12 @@ dtc_status dtc_solve_batch(dtc_handle* handle, const dtc_domain_in* in, int64_t 
  * node numbering and constrained-node list bit-identical to gen_quadmesh_from_phi and
  * generate_boundaries).  Needs no device. */
 dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out);
+
+/* dtc_mesh_domain for n domains of one element type, computed on the handle's device
+ * (gen_quadmesh_from_phi and generate_boundaries as device kernels: 26-connected regions by a
+ * lock-free union-find, the bounding-box keep test, the compaction quirks, first-appearance
+ * node numbering by prefix sums).  out[i] is filled exactly as dtc_mesh_domain fills it. */
+dtc_status dtc_mesh_batch(dtc_handle* handle, const dtc_domain_in* in, int64_t n, dtc_mesh_out* out);
 
 /* Host-only: element stiffness matrix of one voxel element, column-major (3*elem_type)^2,
  * node order of the mesher.  Mirrors Hexe08 / Hexe20 (f-src/mod_linfe.f90:161-776,

@@ -104,7 +104,7 @@ class Solver:
     def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=0.0, max_refine=12,
                  rotation_search=True, device=0, host_threads=0, keep_displacements=False,
                  profile_kernels=False, mixed_matvec="simt", inner_precond="block", estimator="reaction",
-                 chunk_domains=0, graphs=True, tc_wait_spins=0):
+                 chunk_domains=0, graphs=True, tc_wait_spins=0, device_mesher=False):
         self.lib = capi.load()
         o = capi.Options()
         self.lib.dtc_default_options(C.byref(o))
@@ -119,6 +119,7 @@ class Solver:
         o.chunk_domains = int(chunk_domains)
         o.graph_chunks = 0 if graphs else 1
         o.tc_wait_spins = int(tc_wait_spins)
+        o.device_mesher = int(bool(device_mesher))
         self.options = o
         h = C.c_void_p()
         rc = self.lib.dtc_create(C.byref(h), C.byref(o))
@@ -178,6 +179,16 @@ class Solver:
         ptrs = (C.c_void_p * n)(*[C.c_void_p(int(p)) for p in grad_ptrs])
         self._check(self.lib.dtc_energy_grad_device(self.handle, dl.ctypes.data_as(C.POINTER(C.c_double)), ptrs, n))
 
+    def mesh_batch(self, domains):
+        """mesh_domain() for many domains of one element type, computed on the device
+        (dtc_mesh_batch)."""
+        n = len(domains)
+        ins = (capi.DomainIn * n)(*[d.struct for d in domains])
+        made = [_mesh_out(d) for d in domains]
+        outs = (capi.MeshOut * n)(*[m[0] for m in made])
+        self._check(self.lib.dtc_mesh_batch(self.handle, ins, n, outs))
+        return [_mesh_result(d, outs[i], made[i][1]) for i, d in enumerate(domains)]
+
     def rotation_search(self, ee):
         """CR1/CR2 rotation search of given symmetric 6x6 tensors (n x 6 x 6): result dicts with
         the "cr1" and "cr2" entries of solve()."""
@@ -226,9 +237,7 @@ def element_stiffness(elem_type, E, a, nu):
     return ke
 
 
-def mesh_domain(domain):
-    """Reference mesh + boundary conditions of one domain (host only, no GPU needed)."""
-    lib = capi.load()
+def _mesh_out(domain):
     L = domain.L
     nen = domain.elem_type
     m = 1 if nen == HEX08 else 2
@@ -244,10 +253,23 @@ def mesh_domain(domain):
     o.nodes = nodes.ctypes.data_as(C.POINTER(C.c_double))
     o.bnode_ids = bids.ctypes.data_as(C.POINTER(C.c_int64))
     o.bnode_vals = bvals.ctypes.data_as(C.POINTER(C.c_double))
-    rc = lib.dtc_mesh_domain(C.byref(domain.struct), C.byref(o))
-    if rc != capi.DTC_OK:
-        raise DTCError(rc, "dtc_mesh_domain failed")
+    return o, (elems, nodes, bids, bvals)
+
+
+def _mesh_result(domain, o, keep):
+    elems, nodes, bids, bvals = keep
+    nen = domain.elem_type
     ne, nn, nb = o.ne, o.nn, o.nb
     return {"status": o.status, "ne": ne, "nn": nn, "nb": nb, "last_elem_partial": bool(o.last_elem_partial),
             "elems": elems[: nen * ne].reshape(ne, nen), "nodes": nodes[: 3 * nn].reshape(nn, 3),
             "bnode_ids": bids[:nb], "bnode_vals": bvals[: 24 * 3 * nb].reshape(24, 3 * nb, order="F")}
+
+
+def mesh_domain(domain):
+    """Reference mesh + boundary conditions of one domain (host only, no GPU needed)."""
+    lib = capi.load()
+    o, keep = _mesh_out(domain)
+    rc = lib.dtc_mesh_domain(C.byref(domain.struct), C.byref(o))
+    if rc != capi.DTC_OK:
+        raise DTCError(rc, "dtc_mesh_domain failed")
+    return _mesh_result(domain, o, keep)

@@ -30,7 +30,7 @@ class Options(C.Structure):
         ("keep_displacements", C.c_int32), ("profile_kernels", C.c_int32),
         ("mixed_matvec", C.c_int32), ("inner_precond", C.c_int32),
         ("tensor_estimator", C.c_int32), ("chunk_domains", C.c_int32), ("graph_chunks", C.c_int32),
-        ("tc_wait_spins", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("tc_wait_spins", C.c_int32), ("device_mesher", C.c_int32),
     ]
 
 
@@ -99,6 +99,7 @@ SIGNATURES = {
     "dtc_destroy": (C.c_int, [C.c_void_p]),
     "dtc_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(DomainIn), C.c_int64, C.POINTER(DomainOut)]),
     "dtc_mesh_domain": (C.c_int, [C.POINTER(DomainIn), C.POINTER(MeshOut)]),
+    "dtc_mesh_batch": (C.c_int, [C.c_void_p, C.POINTER(DomainIn), C.c_int64, C.POINTER(MeshOut)]),
     "dtc_energy_grad": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.POINTER(C.c_float)), C.c_int64]),
     "dtc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "dtc_element_stiffness": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),

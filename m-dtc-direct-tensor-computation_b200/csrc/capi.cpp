@@ -24,8 +24,20 @@ struct dtc_handle {
   dtc::SolverStats last;
   float* staging = nullptr;   // pinned host copy of device-resident moduli (dtc_solve_batch_device_moduli)
   size_t staging_n = 0;
+  cudaStream_t mesh_stream = nullptr;   // the device mesher's stream (created on first use)
   ~dtc_handle() {
     if (staging) cudaFreeHost(staging);
+    if (mesh_stream) cudaStreamDestroy(mesh_stream);
+  }
+  // meshes in[0..n) on the device into plans; callable from any host thread
+  int mesh_on_device(const dtc_domain_in* in, int64_t n, dtc::MeshPlan* plans, bool numbering, std::string& msg) {
+    if (cudaSetDevice(opt.device) != cudaSuccess) { msg = "cudaSetDevice failed"; return DTC_ERR_CUDA; }
+    if (!mesh_stream && cudaStreamCreateWithFlags(&mesh_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      mesh_stream = nullptr;
+      msg = "cudaStreamCreate failed";
+      return DTC_ERR_CUDA;
+    }
+    return dtc::mesh_batch_device(in, n, plans, numbering, mesh_stream, msg);
   }
 };
 
@@ -96,7 +108,8 @@ int64_t device_bytes_per_node() { return 72 * (4 * 8 + 4 * 4) + 64; }
 
 namespace dtc {
 int rotation_search_device(const std::vector<const double*>& ees, std::vector<int64_t>& ang, std::vector<int>& jj,
-                           std::vector<double>& crit, cudaStream_t s, int64_t& launches, std::string& msg);
+                           std::vector<double>& crit, cudaStream_t s, int64_t& launches, std::string& msg,
+                           double* ms = nullptr);
 }
 
 extern "C" {
@@ -130,7 +143,7 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
     return DTC_ERR_INVALID_ARGUMENT;
   if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 1 ||
       o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0 || o.graph_chunks < 0 ||
-      o.graph_chunks > 1 || o.tc_wait_spins < 0)
+      o.graph_chunks > 1 || o.device_mesher < 0 || o.device_mesher > 1)
     return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
@@ -151,12 +164,12 @@ const char* dtc_last_error(const dtc_handle* handle) {
   return handle->err.c_str();
 }
 
-dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out) {
-  if (!in || !out) return DTC_ERR_INVALID_ARGUMENT;
-  std::string msg;
-  if (validate_domain(*in, msg)) return DTC_ERR_INVALID_ARGUMENT;
-  MeshPlan mp;
-  if (plan_mesh(*in, true, mp) != DTC_OK) return DTC_ERR_INVALID_ARGUMENT;
+}  // extern "C"
+
+namespace {
+
+// dtc_mesh_out of one planned domain (reference numbering, coordinates, boundary values)
+dtc_status fill_mesh_out(const dtc_domain_in* in, const MeshPlan& mp, dtc_mesh_out* out) {
   out->ne = mp.ne; out->nn = mp.nn; out->nb = mp.nb;
   out->status = mp.status;
   out->last_elem_partial = mp.last_partial ? 1 : 0;
@@ -191,6 +204,42 @@ dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out) {
       ++b;
     }
   }
+  return DTC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+dtc_status dtc_mesh_domain(const dtc_domain_in* in, dtc_mesh_out* out) {
+  if (!in || !out) return DTC_ERR_INVALID_ARGUMENT;
+  std::string msg;
+  if (validate_domain(*in, msg)) return DTC_ERR_INVALID_ARGUMENT;
+  MeshPlan mp;
+  if (plan_mesh(*in, true, mp) != DTC_OK) return DTC_ERR_INVALID_ARGUMENT;
+  return fill_mesh_out(in, mp, out);
+}
+
+dtc_status dtc_mesh_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dtc_mesh_out* out) {
+  if (!h) return DTC_ERR_INVALID_ARGUMENT;
+  h->err.clear();
+  if (n < 0 || (n > 0 && (!in || !out))) { h->err = "in/out must be non-NULL for n > 0"; return DTC_ERR_INVALID_ARGUMENT; }
+  if (n == 0) return DTC_OK;
+  bool numbering = false;
+  for (int64_t i = 0; i < n; ++i) {
+    std::string msg;
+    if (validate_domain(in[i], msg)) { h->err = "domain " + std::to_string(i) + ": " + msg; return DTC_ERR_INVALID_ARGUMENT; }
+    if (in[i].elem_type != in[0].elem_type) { h->err = "all domains of one call must share elem_type"; return DTC_ERR_INVALID_ARGUMENT; }
+    numbering = numbering || out[i].elems || out[i].nodes || out[i].bnode_ids || out[i].bnode_vals;
+  }
+  std::vector<MeshPlan> plans((size_t)n);
+  int rc = h->mesh_on_device(in, n, plans.data(), numbering, h->err);
+  if (rc != DTC_OK) return (dtc_status)rc;
+  for (int64_t i = 0; i < n; ++i)
+    if (dtc_status st = fill_mesh_out(&in[i], plans[i], &out[i])) {
+      h->err = "domain " + std::to_string(i) + ": output capacity too small";
+      return st;
+    }
   return DTC_OK;
 }
 
@@ -248,7 +297,12 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
   };
   auto host_stage_body = [&](size_t c, Stage& st) {
     const int64_t a = cuts[c], b = cuts[c + 1];
-    plan_all(in + a, b - a, plans.data() + a, want_fields, h->opt.host_threads);
+    if (h->opt.device_mesher) {
+      st.rc = h->mesh_on_device(in + a, b - a, plans.data() + a, want_fields, st.msg);
+      if (st.rc != DTC_OK) return;
+    } else {
+      plan_all(in + a, b - a, plans.data() + a, want_fields, h->opt.host_threads);
+    }
     for (int64_t i = a; i < b; ++i) {
       dtc_domain_out* o = &out[i];
       double* keep_d = o->displ;
@@ -334,8 +388,18 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     std::vector<int> jj;
     std::vector<double> crit;
     cudaStream_t s = nullptr;
-    int rc = rotation_search_device(ees, ang, jj, crit, s, h->last.kernel_launches, h->err);
+    double ms = 0.0;
+    int rc = rotation_search_device(ees, ang, jj, crit, s, h->last.kernel_launches, h->err, &ms);
     if (rc != DTC_OK) return (dtc_status)rc;
+    // per candidate about 400 FP64 flops: 2 981 371 sweep points and up to 2 x 16 x 9261 refinements
+    KernelClass& kr = h->last.kc[kcRotation];
+    kr.name = "rotation_search_f64";
+    kr.launches = 2;
+    kr.ms = ms;
+    double evals = 2981371.0 * (double)ees.size();
+    for (int q : jj) evals += 9261.0 * q;
+    kr.flops = 400.0 * evals;
+    h->last.ms_rotation = ms;
     for (size_t d = 0; d < ees.size(); ++d) {
       finish_rotation(ees[d], 1, &ang[6 * d], jj[2 * d], crit[2 * d], rot_out[d]);
       finish_rotation(ees[d], 2, &ang[6 * d + 3], jj[2 * d + 1], crit[2 * d + 1], rot_out[d]);

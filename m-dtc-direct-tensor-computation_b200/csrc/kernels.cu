@@ -1837,7 +1837,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
                                              "direction_f32", "direction_f64", "colstate", "reaction_f64",
                                              "project_f64", "mg_jacobi_f32", "mg_residual_f32",
                                              "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
-                                             "host_pack", "host_multigrid_build"};
+                                             "rotation_search_f64", "host_pack", "host_multigrid_build"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;

@@ -69,8 +69,10 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
 }
 
 // Waits until the mbarrier phase of the given parity has completed: one immediate test, then
-// up to limit - 1 potentially suspending polls.  Returns false when the limit runs out.
+// up to limit - 1 potentially suspending polls.  Returns false when the limit runs out (at
+// once for limit <= 0).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = kSpinLimit) {
+  if (limit <= 0) return false;
   uint32_t done;
   asm volatile(
       "{\n\t.reg .pred P1;\n\t"
@@ -100,7 +102,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
 __device__ long long g_tc_spin_limit = tc::kSpinLimit;
 
 int set_tc_spin_limit(long long spins, cudaStream_t s, std::string& msg) {
-  const long long v = spins > 0 ? spins : tc::kSpinLimit;
+  const long long v = spins > 0 ? spins : spins == 0 ? tc::kSpinLimit : 0;
   DTC_CUDA(cudaMemcpyToSymbolAsync(g_tc_spin_limit, &v, sizeof(v), 0, cudaMemcpyHostToDevice, s));
   DTC_CUDA(cudaStreamSynchronize(s));   // v lives on this stack frame
   return DTC_OK;

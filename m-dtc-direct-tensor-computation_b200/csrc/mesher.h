@@ -1,6 +1,7 @@
 // mesher.h -- host planner: the reference mesh of one domain, in structured form.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/dtc.h"
@@ -33,6 +34,12 @@ int64_t gray_value(const dtc_domain_in& in, int64_t v);
 
 // Returns DTC_OK or DTC_ERR_INVALID_ARGUMENT; per-domain outcome in mp.status.
 int plan_mesh(const dtc_domain_in& in, bool numbering, MeshPlan& mp);
+
+// The same for n domains of one element type on the current CUDA device (mesher_dev.cu):
+// plans[i] equals plan_mesh's result bit for bit.  stream: a cudaStream_t; the call returns
+// when its work on that stream is done.
+int mesh_batch_device(const dtc_domain_in* in, int64_t n, MeshPlan* plans, bool numbering, void* stream,
+                      std::string& msg);
 
 // Grid geometry helpers: the node grid has (L+1) points per edge for HEX08 and (2L+1) for
 // HEX20; coordinates are (g + xa_n - 1)*delta or (g/2 + xa_n - 1)*delta.

@@ -217,8 +217,11 @@ int ensure_degree_tables(std::string& msg) {
   return DTC_OK;
 }
 
+// Sweep and refinement of every tensor on the device; ms (optional) receives their CUDA-event
+// time on stream s.
 int rotation_search_device(const std::vector<const double*>& ees, std::vector<int64_t>& ang, std::vector<int>& jj,
-                           std::vector<double>& crit, cudaStream_t s, int64_t& launches, std::string& msg) {
+                           std::vector<double>& crit, cudaStream_t s, int64_t& launches, std::string& msg,
+                           double* ms) {
   const int ndom = (int)ees.size();
   if (ndom == 0) return DTC_OK;
   if (int rc = ensure_degree_tables(msg)) return rc;
@@ -245,16 +248,30 @@ int rotation_search_device(const std::vector<const double*>& ees, std::vector<in
   if ((e = cudaMalloc(&dcrit, sizeof(double) * 2 * ndom))) return fail(e, "cudaMalloc");
   if ((e = cudaMemcpyAsync(dee, hee.data(), sizeof(double) * 36 * ndom, cudaMemcpyHostToDevice, s)))
     return fail(e, "cudaMemcpyAsync");
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (ms && (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess)) ms = nullptr;
+  if (ms) cudaEventRecord(ev[0], s);
   k_rot_sweep<<<dim3(kSweepBlocks, ndom), kRotThreads, 0, s>>>(dee, dpart);
   k_rot_refine<<<dim3(ndom, 2), kRotThreads, 0, s>>>(dee, dpart, std::acos(-1.0) / 180.0, dang, djj, dcrit);
+  if (ms) cudaEventRecord(ev[1], s);
   launches += 2;
-  if ((e = cudaGetLastError())) return fail(e, "rotation kernels");
+  if ((e = cudaGetLastError())) {
+    for (cudaEvent_t q : ev) if (q) cudaEventDestroy(q);
+    return fail(e, "rotation kernels");
+  }
   ang.resize(6 * ndom); jj.resize(2 * ndom); crit.resize(2 * ndom);
   if ((e = cudaMemcpyAsync(ang.data(), dang, sizeof(int64_t) * 6 * ndom, cudaMemcpyDeviceToHost, s)) ||
       (e = cudaMemcpyAsync(jj.data(), djj, sizeof(int) * 2 * ndom, cudaMemcpyDeviceToHost, s)) ||
       (e = cudaMemcpyAsync(crit.data(), dcrit, sizeof(double) * 2 * ndom, cudaMemcpyDeviceToHost, s)) ||
-      (e = cudaStreamSynchronize(s)))
+      (e = cudaStreamSynchronize(s))) {
+    for (cudaEvent_t q : ev) if (q) cudaEventDestroy(q);
     return fail(e, "rotation results");
+  }
+  if (ms) {
+    float t = 0.f;
+    *ms = cudaEventElapsedTime(&t, ev[0], ev[1]) == cudaSuccess ? (double)t : 0.0;
+  }
+  for (cudaEvent_t q : ev) if (q) cudaEventDestroy(q);
   cleanup();
   return DTC_OK;
 }
