@@ -77,7 +77,10 @@ typedef struct dtc_options {
   int32_t profile_kernels; /* 1: time every solver kernel with CUDA events on its stream
                               (dtc_get_kernel_stats); adds event records, off for production */
   int32_t mixed_matvec;    /* stiffness contraction of the FP32 inner solve: 0 = SIMT FP32,
-                              1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy) */
+                              1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy),
+                              2 = autotuned: HEX08 multigrid solves time both sweep kernels on
+                              the batch's own tiles and keep the faster, cached per device and
+                              size class (dtc_get_kernel_stats lists the timings) */
   int32_t inner_precond;   /* preconditioner of the FP32 inner solve: 0 = Jacobi (as PETSc's
                               PCJACOBI), 1 = node-block Jacobi (3x3 diagonal blocks),
                               2 = multigrid V-cycle on halved voxel grids (HEX20 domains are

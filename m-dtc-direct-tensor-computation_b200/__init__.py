@@ -113,7 +113,7 @@ class Solver:
         o.rotation_search, o.device, o.host_threads = int(bool(rotation_search)), int(device), int(host_threads)
         o.keep_displacements = int(bool(keep_displacements))
         o.profile_kernels = int(bool(profile_kernels))
-        o.mixed_matvec = {"simt": 0, "tensor": 1}[mixed_matvec]
+        o.mixed_matvec = {"simt": 0, "tensor": 1, "auto": 2}[mixed_matvec]
         o.inner_precond = {"jacobi": 0, "block": 1, "mg": 2}[inner_precond]
         o.tensor_estimator = {"reaction": 0, "energy": 1}[estimator]
         o.chunk_domains = int(chunk_domains)

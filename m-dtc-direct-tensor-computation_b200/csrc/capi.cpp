@@ -141,7 +141,7 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
   }
   if (!(o.rtol > 0 && o.rtol < 1) || o.max_it < 1 || (o.precision != DTC_PREC_FP64 && o.precision != DTC_PREC_MIXED))
     return DTC_ERR_INVALID_ARGUMENT;
-  if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 1 ||
+  if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 2 ||
       o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0 || o.graph_chunks < 0 ||
       o.graph_chunks > 1 || o.device_mesher < 0 || o.device_mesher > 1)
     return DTC_ERR_INVALID_ARGUMENT;

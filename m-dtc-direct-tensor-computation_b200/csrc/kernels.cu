@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -1666,6 +1669,100 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
 // the solvable tasks, and the multigrid plan of a mixed multigrid solve.  Built by
 // DeviceSolver::prepare, which touches no device state (it may run on a host thread while the
 // solver executes an earlier pass), and consumed by DeviceSolver::solve.
+// -------------------------------------------------------------------------------------
+// Autotuner of the fine-level HEX08 sweeps (mixed_matvec = 2): the SIMT slab sweep and the
+// tcgen05 sweep run the post-smoothing step of the batch's first V-cycle on its own tiles,
+// one warm-up and three timed launches each (CUDA events on the solver stream); the faster
+// one serves the whole solve (CG operator, residual and post-smoothing sweeps share the
+// contraction).  Choices are cached per device and size class -- the median domain edge
+// (16, 24, 32, 48, 64 voxels ...) and the kept-voxel fraction (below 0.15, 0.30, above) --
+// so later batches of the same class skip the timing.
+struct TuneKey {
+  int device, lclass, fclass;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, lclass, fclass) < std::tie(o.device, o.lclass, o.fclass);
+  }
+};
+struct TuneResult {
+  int pick;            // 0 = SIMT, 1 = tensor cores
+  float ms[2];         // the timed launches of each candidate
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneResult> g_tune_choice;
+constexpr int kTuneReps = 3;
+
+// the decision in the solve's kernel statistics (also on a cache hit: the timings that decided)
+void record_tuning(SolverStats& st, const TuneResult& r) {
+  st.kc[kcTuneSimt].launches += kTuneReps;
+  st.kc[kcTuneSimt].ms += r.ms[0];
+  st.kc[kcTuneTc].launches += kTuneReps;
+  st.kc[kcTuneTc].ms += r.ms[1];
+}
+
+int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const MgDev& M,
+                   const std::vector<DomDev>& doms, const std::vector<float>& svox, std::string& msg) {
+  cudaStream_t s = I.stream;
+  std::vector<int> Ls;
+  for (const DomDev& D : doms) Ls.push_back(std::max(D.L[0], std::max(D.L[1], D.L[2])));
+  std::nth_element(Ls.begin(), Ls.begin() + Ls.size() / 2, Ls.end());
+  const int lmed = Ls.empty() ? 0 : Ls[Ls.size() / 2];
+  int64_t kept = 0;
+  for (float v : svox) kept += v != 0.0f;
+  const double frac = svox.empty() ? 0.0 : (double)kept / (double)svox.size();
+  const TuneKey key{I.device, (int)std::lround(4.0 * std::log2(std::max(lmed, 1))), frac < 0.15 ? 0 : frac < 0.30 ? 1 : 2};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_choice.find(key);
+    if (it != g_tune_choice.end()) {
+      I.tensor_matvec = it->second.pick == 1;
+      record_tuning(st, it->second);
+      return DTC_OK;
+    }
+  }
+  const int64_t nsm = M.P->sm_n[0];
+  const Tile* tsm = M.tiles + M.P->sm_off[0];
+  if (nsm <= 0) return DTC_OK;
+  const float* b = B<float>(I, bR32);
+  double* zz = B<double>(I, bZz);
+  double* zr = B<double>(I, bZr);
+  cudaEvent_t ev[2];
+  DTC_CUDA(cudaEventCreate(&ev[0]));
+  DTC_CUDA(cudaEventCreate(&ev[1]));
+  float ms[2] = {0.f, 0.f};
+  const int reps = kTuneReps;
+  for (int cand = 0; cand < 2; ++cand) {
+    auto launch = [&]() {
+      if (cand == 0)
+        k_mg_matvec<kMgPost, true><<<(unsigned)(3 * nsm), kThreads, 0, s>>>(tsm, M.doms0, M.svox0, M.binv0, b, M.t0,
+                                                                           M.z0, M.P->omega0, zz, zr, nullptr);
+      else
+        launch_sweep_tc(kTcPost, tsm, nsm, M.doms0, M.svox0, M.flags0, M.binv0, b, M.t0, M.z0, 1.0f, M.P->omega0, zz,
+                        zr, nullptr, M.err, s);
+    };
+    launch();
+    cudaEventRecord(ev[0], s);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(ev[1], s);
+    const cudaError_t ec = cudaEventSynchronize(ev[1]);
+    if (ec != cudaSuccess) {
+      cudaEventDestroy(ev[0]);
+      cudaEventDestroy(ev[1]);
+      msg = std::string("autotune: ") + cudaGetErrorString(ec);
+      return DTC_ERR_CUDA;
+    }
+    cudaEventElapsedTime(&ms[cand], ev[0], ev[1]);
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (int e = launch_check(msg)) return e;
+  const TuneResult r{ms[1] < ms[0] ? 1 : 0, {ms[0], ms[1]}};
+  I.tensor_matvec = r.pick == 1;
+  record_tuning(st, r);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_choice[key] = r;
+  return DTC_OK;
+}
+
 struct HostBatch {
   int nen = 0;
   std::vector<int64_t> tidx;   // tasks solved in this pass
@@ -1837,11 +1934,13 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
                                              "direction_f32", "direction_f64", "colstate", "reaction_f64",
                                              "project_f64", "mg_jacobi_f32", "mg_residual_f32",
                                              "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
-                                             "rotation_search_f64", "host_pack", "host_multigrid_build"};
+                                             "rotation_search_f64", "autotune_simt_sweep", "autotune_tc_sweep",
+                                             "host_pack", "host_multigrid_build"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
   I.tensor_matvec = opt.mixed_matvec == 1;
+  const bool tune = opt.mixed_matvec == 2;
   I.graphs = opt.graph_chunks == 0;
   I.pending.clear();
   I.h_active.clear();
@@ -1858,7 +1957,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
     if (int e = upload_tc_operand(kh, s, msg)) return e;
-    if (I.tensor_matvec) {
+    if (I.tensor_matvec || tune) {
       if (int e = set_tc_spin_limit(opt.tc_wait_spins, s, msg)) return e;
       if (int e = allow_sweep_tc(msg)) return e;
     }
@@ -2085,6 +2184,14 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.ke32 = W.ke32;
       mgd.ke20tc = W.ke20tc;
       mgd.err = W.err;
+      if (tune && NEN == 8) {
+        if ((e = autotune_sweep(I, stats_, W, mgd, doms, svox, msg))) return e;
+        // the timed launches wrote the fine multigrid vectors and the dot accumulators
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bZr], 0, sizeof(double) * ncol, s));
+      }
     }
     // inner FP32 solves aim straight at the outer target when FP32 can reach it
     const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);

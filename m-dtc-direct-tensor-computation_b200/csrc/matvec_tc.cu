@@ -260,27 +260,31 @@ __global__ void __launch_bounds__(128, 4)
   const int64_t nx = D.n[0], nxy = (int64_t)D.n[0] * D.n[1];
   const int hi_x = D.n[0] - 2, hi_y = D.n[1] - 2, hi_z = D.n[2] - 2;
 
+  // the voxel's 24 corner DOFs of this thread's load case for round rd (zero rows past the list)
+  auto gather = [&](int rd, float (&a)[24]) {
+    const int vs = rd * kSweepVox + (tid >> 3);
+    if (vs < nv) {
+      const int vi = vlist[vs];
+      const int vx = vi % L0, vy = (vi / L0) % L1, vz = vi / (L0 * L1);
+      const int64_t n0 = D.node_off + vx + nx * vy + nxy * vz;
+#pragma unroll
+      for (int lm = 0; lm < 8; ++lm) {
+        const int64_t nb = vec_index(n0 + corner_dx(lm) + nx * corner_dy(lm) + nxy * corner_dz(lm), 0, lc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[3 * lm + c] = __ldg(u + nb + c * kNLC);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 24; ++k) a[k] = 0.0f;
+    }
+  };
+  float a[24];
+  if (rounds > 0) gather(0, a);
   int committed = 0;
   for (int rd = 0; rd <= rounds; ++rd) {
-    // (1) this round's A row: the voxel's 24 corner DOFs of this thread's load case
+    // (1) this round's A row, split into tf32 hi + lo (its loads were issued an iteration ago)
     uint32_t av[48];
     if (rd < rounds) {
-      const int vs = rd * kSweepVox + (tid >> 3);
-      float a[24];
-      if (vs < nv) {
-        const int vi = vlist[vs];
-        const int vx = vi % L0, vy = (vi / L0) % L1, vz = vi / (L0 * L1);
-        const int64_t n0 = D.node_off + vx + nx * vy + nxy * vz;
-#pragma unroll
-        for (int lm = 0; lm < 8; ++lm) {
-          const int64_t nb = vec_index(n0 + corner_dx(lm) + nx * corner_dy(lm) + nxy * corner_dz(lm), 0, lc);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) a[3 * lm + c] = __ldg(u + nb + c * kNLC);
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 24; ++k) a[k] = 0.0f;
-      }
 #pragma unroll
       for (int k = 0; k < 24; ++k) {
         const uint32_t hb = __float_as_uint(a[k]) & 0xFFFFE000u;   // tf32 hi: exact, low 13 bits clear
@@ -318,7 +322,9 @@ __global__ void __launch_bounds__(128, 4)
       }
       ++committed;
     }
-    // (4) the previous round's outputs into the owned nodes, while this round's MMAs run
+    // (4) the next round's loads, in flight while (5) runs
+    if (rd + 1 < rounds) gather(rd + 1, a);
+    // (5) the previous round's outputs into the owned nodes, while this round's MMAs run
     if (rd >= 1) {
       uint32_t r[32];
       tmem_ld32(lane_addr + (((rd - 1) & 1) ? kColD1 : kColD0), r);

@@ -84,7 +84,8 @@ struct KernelClass {
 
 enum KClassId { kcMatvec32, kcMatvec64, kcUpdate32, kcUpdate64, kcDirection32, kcDirection64, kcColstate,
                 kcReaction, kcProject, kcMgJacobi, kcMgResidual, kcMgPost, kcMgTransfer, kcMgCoarse,
-                kcRotation, kcHostPack, kcHostMgBuild, kcNumClasses };   // the last two: host phases (wall ms)
+                kcRotation, kcTuneSimt, kcTuneTc, kcHostPack, kcHostMgBuild,
+                kcNumClasses };   // the last two: host phases (wall ms)
 
 struct SolverStats {
   double ms_solve = 0;   // device time of the solve (CUDA events, inputs resident)

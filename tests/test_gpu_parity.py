@@ -299,3 +299,23 @@ def test_pipelined_passes_match_one_pass(dtc, precision, precond, rtol):
             if precision == "fp64":
                 assert np.abs(a["iters"] - b["iters"]).max() <= 2   # atomic reduction order, as vs the oracle
     assert out[True][7]["status"] != 0
+
+
+def test_autotuned_sweeps(dtc, batch):
+    """mixed_matvec = auto: both sweep kernels are timed on the batch's tiles, the faster one
+    solves; a second handle of the same size class reuses the cached decision (same timings)."""
+    pairs, refs = batch
+    doms = [p[0] for p in pairs]
+    stats = []
+    for _ in range(2):
+        with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, inner_precond="mg",
+                        mixed_matvec="auto") as s:
+            res = s.solve(doms)
+            stats.append(s.kernel_stats())
+        for r, ref in zip(res, refs):
+            assert r["status"] == 0
+            assert rel(r["c"], ref["c"]) <= TOL_MIXED
+    for st in stats:
+        assert st["autotune_simt_sweep"]["launches"] == st["autotune_tc_sweep"]["launches"] == 3
+        assert st["autotune_simt_sweep"]["ms_total"] > 0 and st["autotune_tc_sweep"]["ms_total"] > 0
+    assert stats[0]["autotune_tc_sweep"]["ms_total"] == stats[1]["autotune_tc_sweep"]["ms_total"]
