@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(128, 4)
       const int vx = t.x0 - 1 + ix, vy = t.y0 - 1 + iy, vz = t.z0 - 1 + iz;
       if (vx >= 0 && vy >= 0 && vz >= 0 && vx < L0 && vy < L1 && vz < L2) {
         sv = __ldg(svox + D.vox_off + vx + (int64_t)L0 * (vy + (int64_t)L1 * vz));
-        if (sv != 0.0f) vidx = vx + L0 * (vy + L1 * vz);
+        if (sv != 0.0f) vidx = vx | (vy << 10) | (vz << 20);   // packed: no divisions in the rounds
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, vidx >= 0);
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(128, 4)
     const int vs = rd * kSweepVox + (tid >> 3);
     if (vs < nv) {
       const int vi = vlist[vs];
-      const int vx = vi % L0, vy = (vi / L0) % L1, vz = vi / (L0 * L1);
+      const int vx = vi & 1023, vy = (vi >> 10) & 1023, vz = vi >> 20;
       const int64_t n0 = D.node_off + vx + nx * vy + nxy * vz;
 #pragma unroll
       for (int lm = 0; lm < 8; ++lm) {
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(128, 4)
       const int vs = (rd - 1) * kSweepVox + (tid >> 3);
       if (vs < nv) {
         const int vi = vlist[vs];
-        const int vx = vi % L0, vy = (vi / L0) % L1, vz = vi / (L0 * L1);
+        const int vx = vi & 1023, vy = (vi >> 10) & 1023, vz = vi >> 20;
         const float s = vscale[vs];
 #pragma unroll
         for (int lm = 0; lm < 8; ++lm) {

@@ -132,7 +132,8 @@ def test_result_tree_of_a_solve(dtc, tmp_path):
                        delta=syn.DELTA, domain_number=7 + i) for i, b in enumerate((0.4, 0.55))]
     with dtc.Solver(precision="fp64", rtol=1e-8, rotation_search=True) as s:
         res = s.solve(doms)
-    dtc.puredat.write_result_tree(tmp_path / "r.head", res, duration=s.stats()["ms_solve"] / 1e3)
+        ms = s.stats()["ms_solve"]
+    dtc.puredat.write_result_tree(tmp_path / "r.head", res, duration=ms / 1e3)
     back = dtc.puredat.read_result_tree(tmp_path / "r.head")
     for r, b in zip(res, back):
         assert b["Domain number"][0] == r["domain_number"]
