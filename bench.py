@@ -50,8 +50,9 @@ def parse():
     p.add_argument("--estimator", default="energy", choices=["energy", "reaction"])
     p.add_argument("--precond", default="mg", choices=["mg", "block", "jacobi"],
                    help="preconditioner of the FP32 inner solve of the mixed arm")
-    p.add_argument("--matvec", default="simt", choices=["simt", "tensor"],
-                   help="HEX08 fine-level sweeps of the mixed arm: SIMT FP32 or tcgen05 (3xTF32)")
+    p.add_argument("--matvec", default="auto", choices=["simt", "tensor", "auto"],
+                   help="HEX08 fine-level sweeps of the mixed arm: SIMT FP32, tcgen05 (3xTF32), or auto "
+                        "(the library times both on the batch and keeps the faster)")
     p.add_argument("--max-it", type=int, default=20000)
     p.add_argument("--check", type=int, default=16, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
@@ -358,11 +359,41 @@ def run_config(args, dtc):
                 if k >= warm:
                     fwd.append(t1 - t0)
                     bwd.append(t2 - t1)
+        # the same step end to end through the torch binding: E a CUDA tensor with requires_grad,
+        # C = model(E), loss, backward (moduli in and gradients out through device pointers)
+        import importlib
+        ag = importlib.import_module(dtc.__name__ + ".autograd")
+        model = ag.EffectiveStiffness(grays, precision="mixed", rtol=1e-6, inner_precond="mg", estimator="energy",
+                                      device=local)
+        Et = torch.tensor(np.stack(E), device=torch.device("cuda", local), requires_grad=True)
+        Tt = torch.tensor(target, device=torch.device("cuda", local))
+        tf, tb = [], []
+        for k in range(warm + steps):
+            Et.grad = None
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            C = model(Et)
+            loss = ((C - Tt) ** 2).sum()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            loss.backward()
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            if k >= warm:
+                tf.append(t1 - t0)
+                tb.append(t2 - t1)
+        gmax_t = float(Et.grad.abs().max())
+        model.close()
         line.update({"workload": f"adjoint: {n} HEX08 domains of 48^3, BV/TV 0.25, per-voxel E, "
                                  "loss ||C - C_target||_F^2, mixed+MG forward at rtol 1e-6",
                      "forward_s": float(np.mean(fwd)), "adjoint_s": float(np.mean(bwd)),
                      "adjoint_over_forward": float(np.mean(bwd) / np.mean(fwd)),
-                     "grad_abs_max": float(max(np.abs(g).max() for g in grads))})
+                     "grad_abs_max": float(max(np.abs(g).max() for g in grads)),
+                     "torch_e2e": {"forward_s": float(np.mean(tf)), "backward_s": float(np.mean(tb)),
+                                   "backward_over_forward": float(np.mean(tb) / np.mean(tf)),
+                                   "grad_abs_max": gmax_t,
+                                   "path": "EffectiveStiffness on a CUDA tensor: dtc_solve_batch_device_moduli, "
+                                           "dtc_energy_grad_device (no numpy round trip)"}})
     print(json.dumps(line), flush=True)
 
 
@@ -494,6 +525,12 @@ def main():
         prof.solve(doms)
         ks = prof.kernel_stats()
     host = {k: ks.pop(k) for k in list(ks) if k.startswith("host_")}   # host phases, wall ms
+    tune = {k: ks.pop(k) for k in list(ks) if k.startswith("autotune_")}
+    autotune = None
+    if tune:
+        us = {k[len("autotune_"):]: 1e3 * v["ms_total"] / max(v["launches"], 1) for k, v in tune.items()}
+        autotune = {"post_smoothing_sweep_us": us,
+                    "pick": "tensor" if us.get("tc_sweep", 1e30) < us.get("simt_sweep", 1e30) else "simt"}
     top = max((k for k in ks if ks[k]["bytes_per_launch"] > 0), key=lambda k: ks[k]["ms_total"])
     kt = ks[top]
     t_launch = kt["ms_total"] / kt["launches"] / 1e3
@@ -509,7 +546,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": workload(args),
                 "rtol": rtol_of["mixed"], "estimator": args.estimator, "inner_precond": args.precond,
-                "matvec": args.matvec,
+                "matvec": args.matvec, "autotune": autotune,
                 "max_rel_err_vs_fp64_1e-10": timed_err, "accuracy_target": TARGET, "accuracy_sample": nchk,
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),

@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(128, 4)
   float* acc = reinterpret_cast<float*>(dsm + 6 * kBChunkBytes);   // 12 KB
   __shared__ int vlist[kMaxVox];
   __shared__ float vscale[kMaxVox];
+  __shared__ int vown[kMaxVox];   // owned corners (8 bits) | (local node of corner 0 + 64) << 8
   __shared__ int wcount[4];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -243,6 +244,17 @@ __global__ void __launch_bounds__(128, 4)
       const int pos = off + __popc(m & ((1u << lane) - 1));
       vlist[pos] = vidx;
       vscale[pos] = sv;
+      const int vx = vidx & 1023, vy = (vidx >> 10) & 1023, vz = vidx >> 20;
+      int own = 0;
+#pragma unroll
+      for (int lm = 0; lm < 8; ++lm) {
+        const int ox = vx + corner_dx(lm), oy = vy + corner_dy(lm), oz = vz + corner_dz(lm);
+        const int lx = ox - t.x0, ly = oy - t.y0, lz = oz - t.z0;
+        if (lx >= 0 && lx < kTileX && ly >= 0 && ly < kTileY && lz >= 0 && lz < kTileZ && ox >= 1 &&
+            ox <= D.n[0] - 2 && oy >= 1 && oy <= D.n[1] - 2 && oz >= 1 && oz <= D.n[2] - 2)
+          own |= 1 << lm;
+      }
+      vown[pos] = own | ((vx - t.x0 + kTileX * ((vy - t.y0) + kTileY * (vz - t.z0)) + 64) << 8);
     }
     nv += wcount[0] + wcount[1] + wcount[2] + wcount[3];
     __syncthreads();
@@ -330,17 +342,13 @@ __global__ void __launch_bounds__(128, 4)
       tmem_ld32(lane_addr + (((rd - 1) & 1) ? kColD1 : kColD0), r);
       const int vs = (rd - 1) * kSweepVox + (tid >> 3);
       if (vs < nv) {
-        const int vi = vlist[vs];
-        const int vx = vi & 1023, vy = (vi >> 10) & 1023, vz = vi >> 20;
+        const int own = vown[vs];
+        const int nl0 = (own >> 8) - 64;
         const float s = vscale[vs];
 #pragma unroll
         for (int lm = 0; lm < 8; ++lm) {
-          const int ox = vx + corner_dx(lm), oy = vy + corner_dy(lm), oz = vz + corner_dz(lm);
-          const int lx = ox - t.x0, ly = oy - t.y0, lz = oz - t.z0;
-          const bool own = lx >= 0 && lx < kTileX && ly >= 0 && ly < kTileY && lz >= 0 && lz < kTileZ && ox >= 1 &&
-                           ox <= hi_x && oy >= 1 && oy <= hi_y && oz >= 1 && oz <= hi_z;
-          if (own) {
-            const int nl = lx + kTileX * (ly + kTileY * lz);
+          if (own & (1 << lm)) {
+            const int nl = nl0 + corner_dx(lm) + kTileX * (corner_dy(lm) + kTileY * corner_dz(lm));
 #pragma unroll
             for (int c = 0; c < 3; ++c) atomicAdd(&acc[(nl * 3 + c) * 8 + lcl], s * __uint_as_float(r[3 * lm + c]));
           }
