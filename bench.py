@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--matvec", default="auto", choices=["simt", "tensor", "auto"],
                    help="HEX08 fine-level sweeps of the mixed arm: SIMT FP32, tcgen05 (3xTF32), or auto "
                         "(the library times both on the batch and keeps the faster)")
+    p.add_argument("--device-mesher", action="store_true",
+                   help="mixed arm: mesh the domains on the device (dtc_options.device_mesher)")
     p.add_argument("--max-it", type=int, default=20000)
     p.add_argument("--check", type=int, default=16, help="domains re-solved in FP64 at 1e-10 for the accuracy gate")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
@@ -479,7 +481,8 @@ def main():
     # every rank times the same configuration: the tightest rtol any rank calibrated
     rtol_of["mixed"], rtol_of["fp64"] = reduce_over_ranks([rtol_of["mixed"], rtol_of["fp64"]], "min")
     mixed = dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
-                       device=local, estimator=args.estimator, inner_precond=args.precond, mixed_matvec=args.matvec)
+                       device=local, estimator=args.estimator, inner_precond=args.precond, mixed_matvec=args.matvec,
+                       device_mesher=args.device_mesher)
 
     def barrier():
         torch.cuda.synchronize()
@@ -564,7 +567,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": workload(args),
                 "rtol": rtol_of["mixed"], "estimator": args.estimator, "inner_precond": args.precond,
-                "matvec": args.matvec, "autotune": autotune,
+                "matvec": args.matvec, "autotune": autotune, "device_mesher": args.device_mesher,
                 "max_rel_err_vs_fp64_1e-10": timed_err, "accuracy_target": TARGET, "accuracy_sample": nchk,
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),
