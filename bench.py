@@ -284,7 +284,8 @@ def run_config(args, dtc):
             truth = ref.solve(sample)
         out = {}
         ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8]
-        for arm, kw in (("mixed", dict(precision="mixed", estimator="energy", inner_precond="mg")),
+        for arm, kw in (("mixed", dict(precision="mixed", estimator="energy", inner_precond="mg",
+                                       mixed_matvec=args.matvec)),
                         ("fp64", dict(precision="fp64"))):
             # loosest rtol whose tensors stay within TARGET/2 of FP64 at 1e-10 on the sample
             for rt in ladder:
@@ -298,8 +299,12 @@ def run_config(args, dtc):
                     sv.solve(doms)
                     return sv.stats()["ms_solve"]
                 dev, wall = _timed(step, steps, warm)
+                tune = {k: round(1e3 * v["ms_total"] / max(v["launches"], 1), 1)
+                        for k, v in sv.kernel_stats().items() if k.startswith("autotune_")}
             out[arm] = {"domains_per_s": n / (dev / 1e3), "ms_per_step": dev, "rtol": rt, "max_rel_err": err,
                         "e2e_domains_per_s": n / wall}
+            if tune:
+                out[arm]["autotune_us_per_fine_application"] = tune
         line.update({"workload": f"{n} HEX20 domains of 24^3, BV/TV 0.25, per-voxel E", "mixed": out["mixed"],
                      "fp64_plain": out["fp64"],
                      "speedup_mixed_over_fp64": out["mixed"]["domains_per_s"] / out["fp64"]["domains_per_s"]})

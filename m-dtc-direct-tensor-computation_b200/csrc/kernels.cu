@@ -1678,9 +1678,9 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
 // (16, 24, 32, 48, 64 voxels ...) and the kept-voxel fraction (below 0.15, 0.30, above) --
 // so later batches of the same class skip the timing.
 struct TuneKey {
-  int device, lclass, fclass;
+  int device, nen, lclass, fclass;
   bool operator<(const TuneKey& o) const {
-    return std::tie(device, lclass, fclass) < std::tie(o.device, o.lclass, o.fclass);
+    return std::tie(device, nen, lclass, fclass) < std::tie(o.device, o.nen, o.lclass, o.fclass);
   }
 };
 struct TuneResult {
@@ -1699,8 +1699,11 @@ void record_tuning(SolverStats& st, const TuneResult& r) {
   st.kc[kcTuneTc].ms += r.ms[1];
 }
 
+// HEX20 fine levels: the SIMT brick kernel and the tcgen05 brick kernel apply K to the fine
+// multigrid vector on the interior bricks (the operator of the residual and post-smoothing
+// steps and of the CG application).
 int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const MgDev& M,
-                   const std::vector<DomDev>& doms, const std::vector<float>& svox, std::string& msg) {
+                   const std::vector<DomDev>& doms, const std::vector<float>& svox, int nen, std::string& msg) {
   cudaStream_t s = I.stream;
   std::vector<int> Ls;
   for (const DomDev& D : doms) Ls.push_back(std::max(D.L[0], std::max(D.L[1], D.L[2])));
@@ -1709,7 +1712,8 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const 
   int64_t kept = 0;
   for (float v : svox) kept += v != 0.0f;
   const double frac = svox.empty() ? 0.0 : (double)kept / (double)svox.size();
-  const TuneKey key{I.device, (int)std::lround(4.0 * std::log2(std::max(lmed, 1))), frac < 0.15 ? 0 : frac < 0.30 ? 1 : 2};
+  const TuneKey key{I.device, nen, (int)std::lround(4.0 * std::log2(std::max(lmed, 1))),
+                    frac < 0.15 ? 0 : frac < 0.30 ? 1 : 2};
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune_choice.find(key);
@@ -1721,7 +1725,7 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const 
   }
   const int64_t nsm = M.P->sm_n[0];
   const Tile* tsm = M.tiles + M.P->sm_off[0];
-  if (nsm <= 0) return DTC_OK;
+  if (nsm <= 0 || (nen == 20 && (M.nbricks0 <= 0 || !W.ke20tc))) return DTC_OK;
   const float* b = B<float>(I, bR32);
   double* zz = B<double>(I, bZz);
   double* zr = B<double>(I, bZr);
@@ -1732,12 +1736,20 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const 
   const int reps = kTuneReps;
   for (int cand = 0; cand < 2; ++cand) {
     auto launch = [&]() {
-      if (cand == 0)
+      if (nen == 20) {
+        if (cand == 0)
+          launch_ebe<float, 20, false, false>(M.bricks0, M.nbricks0, M.doms0, M.svox0, M.flags0, M.ke32, M.t0, M.z0,
+                                              -1.0, nullptr, nullptr, s);
+        else
+          launch_ebe_tc(M.bricks0, M.nbricks0, M.doms0, M.svox0, M.flags0, W.ke20tc, M.t0, M.z0, -1.0, nullptr,
+                        nullptr, M.err, s);
+      } else if (cand == 0) {
         k_mg_matvec<kMgPost, true><<<(unsigned)(3 * nsm), kThreads, 0, s>>>(tsm, M.doms0, M.svox0, M.binv0, b, M.t0,
                                                                            M.z0, M.P->omega0, zz, zr, nullptr);
-      else
+      } else {
         launch_sweep_tc(kTcPost, tsm, nsm, M.doms0, M.svox0, M.flags0, M.binv0, b, M.t0, M.z0, 1.0f, M.P->omega0, zz,
                         zr, nullptr, M.err, s);
+      }
     };
     launch();
     cudaEventRecord(ev[0], s);
@@ -1972,7 +1984,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       DTC_CUDA(cudaMemcpyAsync(I.bufs[bKe20], k20.data(), sizeof(double) * 3600, cudaMemcpyHostToDevice, s));
       DTC_CUDA(cudaMemcpyAsync(B<double>(I, bKe20) + 3600, k20f.data(), sizeof(float) * 3600, cudaMemcpyHostToDevice,
                                s));
-      if (I.tensor_matvec) {   // HEX20 FP32 applications on the tensor cores
+      if (I.tensor_matvec || tune) {   // HEX20 FP32 applications on the tensor cores
         std::vector<float> img(tc20_operand_bytes() / sizeof(float));
         build_tc20_operand(k20.data(), img.data());
         if (int e = ensure(I, bKe20tc, tc20_operand_bytes(), msg)) return e;
@@ -2072,8 +2084,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   const Tile* ti = B<Tile>(I, bTilesI);
   const Tile* ta = B<Tile>(I, bTilesA);
   const double* ke64 = NEN == 20 ? B<double>(I, bKe20) : nullptr;
-  const float* ke20tc = (NEN == 20 && I.tensor_matvec) ? B<float>(I, bKe20tc) : nullptr;
-  const Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba,
+  const float* ke20tc = (NEN == 20 && (I.tensor_matvec || tune)) ? B<float>(I, bKe20tc) : nullptr;
+  Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba,
                B<int64_t>(I, bNodesI), (int64_t)nodes_i.size(), ke64,
                ke64 ? reinterpret_cast<const float*>(ke64 + 3600) : nullptr, ke20tc, B<int>(I, bErr)};
   const DomDev* dd = B<DomDev>(I, bDoms);
@@ -2184,8 +2196,9 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.ke32 = W.ke32;
       mgd.ke20tc = W.ke20tc;
       mgd.err = W.err;
-      if (tune && NEN == 8) {
-        if ((e = autotune_sweep(I, stats_, W, mgd, doms, svox, msg))) return e;
+      if (tune) {
+        if ((e = autotune_sweep(I, stats_, W, mgd, doms, svox, NEN, msg))) return e;
+        if (!I.tensor_matvec) W.ke20tc = mgd.ke20tc = nullptr;   // HEX20: the brick kernel won
         // the timed launches wrote the fine multigrid vectors and the dot accumulators
         DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
         DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));

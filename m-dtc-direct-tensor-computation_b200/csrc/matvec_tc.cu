@@ -475,44 +475,49 @@ int upload_tc_operand(const double* khat, cudaStream_t s, std::string& msg) {
 
 // -------------------------------------------------------------------------------------
 // HEX20: the 60x60 element contraction of the brick kernel (ebe.cuh) on the tensor cores.
-// One CTA = one brick of 4x4x2 voxels (owned nodes 8x8x4 on the doubled grid) x 4 load cases.
-// Per round the 128 rows of A are 32 kept voxels x 4 load cases (row = voxel * 4 + load case),
-// K = the 60 voxel DOFs (padded to 64), B = the unit element matrix (N = 60 outputs, padded to
-// 64), D = A B^T in a 128 x 64 FP32 tensor-memory accumulator; 3xTF32 split as above.  The
-// epilogue adds s_v * D into shared accumulators of the owned nodes, which are written once.
 namespace tc20 {
 constexpr int kRows = 128, kVoxPerRound = 32, kLcg = 4;
 constexpr int kK = 64, kN = 64, kKc = 8, kChunks = kK / kKc;
-constexpr int kAChunkBytes = kRows * kKc * 4;   // 4 KB
 constexpr int kBChunkBytes = kN * kKc * 4;      // 2 KB
 constexpr int kBx = 4, kBy = 4, kBz = 2;        // brick (voxels)
 constexpr int kOx = 2 * kBx, kOy = 2 * kBy, kOz = 2 * kBz;
+constexpr int kIx = kOx + 3, kIy = kOy + 3, kIz = kOz + 3;   // staged input nodes (1-voxel halo below)
 constexpr int kMaxVox = (kBx + 1) * (kBy + 1) * (kBz + 1);
-constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kColAHi = 0, kColALo = 64, kColD0 = 128, kColD1 = 192;
+constexpr uint32_t kTmemCols = 256;
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kN >> 3) << 17) |
                             ((uint32_t)(kRows >> 4) << 24);
-// shared memory: A hi/lo, B hi/lo, owned accumulators
-constexpr size_t kSmemA = 2 * kChunks * kAChunkBytes;            // 64 KB
-constexpr size_t kSmemB = 2 * kChunks * kBChunkBytes;            // 32 KB
-constexpr size_t kSmemAcc = (size_t)kOx * kOy * kOz * 3 * kLcg * 4;   // 12 KB
-constexpr size_t kSmem = kSmemA + kSmemB + kSmemAcc + 1024;      // + alignment slack
+// shared memory: B hi/lo (canonical chunks), staged inputs, owned accumulators
+constexpr size_t kSmemB = 2 * kChunks * kBChunkBytes;                    // 32 KB
+constexpr size_t kSmemIn = (size_t)kIx * kIy * kIz * 3 * kLcg * 4;       // 39.7 KB
+constexpr size_t kSmemAcc = (size_t)kOx * kOy * kOz * 3 * kLcg * 4;      // 12 KB
+constexpr size_t kSmem = kSmemB + kSmemIn + kSmemAcc + 1024;             // + alignment slack
 
 __device__ constexpr int8_t kRing[20][3] = {
     {0, 0, 0}, {1, 0, 0}, {2, 0, 0}, {2, 1, 0}, {2, 2, 0}, {1, 2, 0}, {0, 2, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 1},
     {2, 2, 1}, {0, 2, 1}, {0, 0, 2}, {1, 0, 2}, {2, 0, 2}, {2, 1, 2}, {2, 2, 2}, {1, 2, 2}, {0, 2, 2}, {0, 1, 2}};
 
-__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
   uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       :
-      : "r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+      : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 }  // namespace tc20
 
 // y = scale * K u on the owned interior nodes of one brick (HEX20, FP32); DOT: acc += u . y.
+// One CTA = one brick of 4 x 4 x 2 voxels (owned nodes 8 x 8 x 4 on the doubled grid) x 4 load
+// cases.  The brick's input nodes (with a 1-voxel halo below) are staged in shared memory once;
+// per round the 128 rows of A are 32 kept voxels x 4 load cases: each thread reads its voxel's
+// 60 DOFs of its load case from the staged nodes, splits them into tf32 hi + lo and stores them
+// in its own tensor-memory lane (columns 0-63 hi, 64-127 lo; K padded to 64).  One thread issues
+// D = A_hi B_hi + A_hi B_lo + A_lo B_hi (B = the unit element matrix, split on the host, N = 60
+// padded to 64) as 24 tcgen05.mma (M 128, N 64, K 8) into one of two 64-column accumulators;
+// meanwhile every thread scales the previous round's row by the voxel's modulus factor and adds
+// the outputs of owned nodes into shared accumulators, which are written once at the end.
 // bsplit: the element matrix split into tf32 hi / lo in the canonical B layout (2 x 8 chunks).
 template <bool DOT>
 __global__ void __launch_bounds__(128, 2)
@@ -523,16 +528,17 @@ __global__ void __launch_bounds__(128, 2)
   using namespace tc20;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* sA = base;
-  unsigned char* sB = base + kSmemA;
-  float* sacc = reinterpret_cast<float*>(base + kSmemA + kSmemB);
-  __shared__ int vlist[kMaxVox];
+  unsigned char* sB = base;
+  float* sin = reinterpret_cast<float*>(base + kSmemB);
+  float* sacc = reinterpret_cast<float*>(base + kSmemB + kSmemIn);
+  __shared__ int vlist[kMaxVox];      // staged-grid origin of the voxel (its node 0), packed
   __shared__ float vscale[kMaxVox];
+  __shared__ int vown[kMaxVox];       // owned ring nodes (20 bits)
   __shared__ int wcount[4];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
   __shared__ int fail;
-  __shared__ double red[32];
+  __shared__ double red[kLcg];
 
   const Tile t = bricks[blockIdx.x / (kNLC / kLcg)];
   if (dom_active && !dom_active[t.dom]) return;
@@ -550,23 +556,46 @@ __global__ void __launch_bounds__(128, 2)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(&mbar)));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
+  if (tid < kLcg) red[tid] = 0.0;
   for (int i = tid; i < (int)(kSmemB / 16); i += 128)
     reinterpret_cast<float4*>(sB)[i] = __ldg(reinterpret_cast<const float4*>(bsplit) + i);
   for (int i = tid; i < kOx * kOy * kOz * 3 * kLcg; i += 128) sacc[i] = 0.0f;
+  // staged input nodes: fine coordinates 2 (x0 - 1) .. 2 (x0 + 4), and likewise in y, z
+  const int ix0 = 2 * (t.x0 - 1), iy0 = 2 * (t.y0 - 1), iz0 = 2 * (t.z0 - 1);
+  for (int i = tid; i < kIx * kIy * kIz * 3 * kLcg; i += 128) {
+    const int l = i % kLcg, c = (i / kLcg) % 3, nl = i / (3 * kLcg);
+    const int gx = ix0 + nl % kIx, gy = iy0 + (nl / kIx) % kIy, gz = iz0 + nl / (kIx * kIy);
+    float v = 0.0f;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < D.n[0] && gy < D.n[1] && gz < D.n[2])
+      v = __ldg(u + vec_index(node_index(D, gx, gy, gz), c, g * kLcg + l));
+    sin[i] = v;
+  }
 
-  // kept voxels touching the owned nodes (brick plus a 1-voxel halo below), deterministic order
+  // kept voxels touching the owned nodes (brick plus a 1-voxel halo below), x-fastest order,
+  // with the staged-grid index of their node 0 and the mask of their owned ring nodes
   const int L0 = D.L[0], L1 = D.L[1], L2 = D.L[2];
+  const int hx = D.n[0] - 2, hy = D.n[1] - 2, hz = D.n[2] - 2;
   int nv = 0;
   {
     const int q = tid;
-    int code = -1;
+    int code = -1, own = 0;
     float sv = 0.0f;
     if (q < kMaxVox) {
       const int qx = q % (kBx + 1), qy = (q / (kBx + 1)) % (kBy + 1), qz = q / ((kBx + 1) * (kBy + 1));
       const int vx = t.x0 - 1 + qx, vy = t.y0 - 1 + qy, vz = t.z0 - 1 + qz;
       if (vx >= 0 && vy >= 0 && vz >= 0 && vx < L0 && vy < L1 && vz < L2) {
         sv = __ldg(svox + D.vox_off + vx + (int64_t)L0 * (vy + (int64_t)L1 * vz));
-        if (sv != 0.0f) code = q;
+        if (sv != 0.0f) {
+          code = (2 * qx) + kIx * ((2 * qy) + kIy * (2 * qz));
+#pragma unroll
+          for (int a = 0; a < 20; ++a) {
+            const int ox = 2 * vx + kRing[a][0], oy = 2 * vy + kRing[a][1], oz = 2 * vz + kRing[a][2];
+            const int lx = ox - 2 * t.x0, ly = oy - 2 * t.y0, lz = oz - 2 * t.z0;
+            if (lx >= 0 && lx < kOx && ly >= 0 && ly < kOy && lz >= 0 && lz < kOz && ox >= 1 && ox <= hx &&
+                oy >= 1 && oy <= hy && oz >= 1 && oz <= hz)
+              own |= 1 << a;
+          }
+        }
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, code >= 0);
@@ -578,113 +607,106 @@ __global__ void __launch_bounds__(128, 2)
       const int pos = off + __popc(m & ((1u << lane) - 1));
       vlist[pos] = code;
       vscale[pos] = sv;
+      vown[pos] = own;
     }
     nv = wcount[0] + wcount[1] + wcount[2] + wcount[3];
   }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // B visible to the tensor cores
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  const uint32_t sA_addr = tc::smem_u32(sA), sB_addr = tc::smem_u32(sB);
-  const int l = tid & (kLcg - 1), lc = g * kLcg + l;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t sB_addr = tc::smem_u32(sB);
+  const int l = tid & (kLcg - 1);
   const int rounds = (nv + kVoxPerRound - 1) / kVoxPerRound;
-  const int ix0 = 2 * t.x0, iy0 = 2 * t.y0, iz0 = 2 * t.z0;   // first owned fine coordinate
-  const int hx = D.n[0] - 2, hy = D.n[1] - 2, hz = D.n[2] - 2;
+  const long long lim = g_tc_spin_limit;
+  // staged-grid offset of ring node a relative to the voxel's node 0
+  auto ring_off = [](int a) { return kRing[a][0] + kIx * (kRing[a][1] + kIy * kRing[a][2]); };
 
-  int rd = 0;
-  for (; rd < rounds; ++rd) {
-    const int vs = rd * kVoxPerRound + (tid >> 2);
-    int fx = 0, fy = 0, fz = 0;
-    const bool have = vs < nv;
-    if (have) {
-      const int q = vlist[vs];
-      const int qx = q % (kBx + 1), qy = (q / (kBx + 1)) % (kBy + 1), qz = q / ((kBx + 1) * (kBy + 1));
-      fx = 2 * (t.x0 - 1 + qx); fy = 2 * (t.y0 - 1 + qy); fz = 2 * (t.z0 - 1 + qz);
-    }
-    // A row: the 60 DOFs of this voxel for this load case, hi / lo, K padded with zeros
+  int committed = 0;
+  for (int rd = 0; rd <= rounds; ++rd) {
+    // (1) the MMAs of the previous round have finished: A is free, its accumulator is ready
+    if (rd >= 1 && !tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)((rd - 1) & 1), lim)) atomicOr(&fail, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // (2) this round's A row: the voxel's 60 DOFs of this thread's load case, hi then lo
+    if (rd < rounds) {
+      const int vs = rd * kVoxPerRound + (tid >> 2);
+      const int o = vs < nv ? vlist[vs] : -1;
 #pragma unroll
-    for (int a = 0; a < 20; ++a) {
-      float v[3] = {0.f, 0.f, 0.f};
-      if (have) {
-        const int64_t nb = vec_index(node_index(D, fx + kRing[a][0], fy + kRing[a][1], fz + kRing[a][2]), 0, lc);
+      for (int ch = 0; ch < 4; ++ch) {   // K chunks of 16 columns (the last holds 12 DOFs)
+        uint32_t hv[16], lv[16];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = __ldg(u + nb + c * kNLC);
+        for (int j = 0; j < 16; ++j) {
+          const int k = 16 * ch + j;
+          float v = 0.0f;
+          if (k < 60 && o >= 0) v = sin[((o + ring_off(k / 3)) * 3 + k % 3) * kLcg + l];
+          const uint32_t hb = __float_as_uint(v) & 0xFFFFE000u;
+          hv[j] = hb;
+          lv[j] = __float_as_uint(v - __uint_as_float(hb));
+        }
+        tc::tmem_st16(lane_addr + kColAHi + 16 * ch, hv);
+        tc::tmem_st16(lane_addr + kColALo + 16 * ch, lv);
       }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int k = 3 * a + c, kc = k >> 3, kk = k & 7;
-        const float hi = tc::to_tf32(v[c]);
-        *reinterpret_cast<float*>(sA + kc * kAChunkBytes + tc::canon_offset(tid, kk)) = hi;
-        *reinterpret_cast<float*>(sA + (kChunks + kc) * kAChunkBytes + tc::canon_offset(tid, kk)) = tc::to_tf32(v[c] - hi);
-      }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     }
-#pragma unroll
-    for (int k = 60; k < kK; ++k) {
-      const int kc = k >> 3, kk = k & 7;
-      *reinterpret_cast<float*>(sA + kc * kAChunkBytes + tc::canon_offset(tid, kk)) = 0.0f;
-      *reinterpret_cast<float*>(sA + (kChunks + kc) * kAChunkBytes + tc::canon_offset(tid, kk)) = 0.0f;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int kc = 0; kc < kChunks; ++kc) {
-        const uint64_t ahi = tc::smem_desc(sA_addr + kc * kAChunkBytes);
-        const uint64_t alo = tc::smem_desc(sA_addr + (kChunks + kc) * kAChunkBytes);
-        const uint64_t bhi = tc::smem_desc(sB_addr + kc * kBChunkBytes);
-        const uint64_t blo = tc::smem_desc(sB_addr + (kChunks + kc) * kBChunkBytes);
-        tc20::mma(tmem, ahi, bhi, kc > 0 ? 1u : 0u);
-        tc20::mma(tmem, ahi, blo, 1u);
-        tc20::mma(tmem, alo, bhi, 1u);
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       tc::smem_u32(&mbar))
-                   : "memory");
-    }
-    if (!tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)(rd & 1), g_tc_spin_limit)) atomicOr(&fail, 1);
-    __syncthreads();
     if (fail) break;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // the tensor-memory loads are collective (.sync.aligned): every thread issues them, then
-    // only rows that hold a voxel scatter
-    const float s = have ? vscale[vs] : 0.0f;
+    if (rd < rounds) {
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + ((rd & 1) ? kColD1 : kColD0);
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      uint32_t r[32];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
-            "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-            "=r"(r[30]), "=r"(r[31])
-          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(half * 32)));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int kc = 0; kc < kChunks; ++kc) {
+          const uint64_t bhi = tc::smem_desc(sB_addr + kc * kBChunkBytes);
+          const uint64_t blo = tc::smem_desc(sB_addr + (kChunks + kc) * kBChunkBytes);
+          tc20::mma_ts(d, tmem + kColAHi + 8 * kc, bhi, kc > 0 ? 1u : 0u);
+          tc20::mma_ts(d, tmem + kColAHi + 8 * kc, blo, 1u);
+          tc20::mma_ts(d, tmem + kColALo + 8 * kc, bhi, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         tc::smem_u32(&mbar))
+                     : "memory");
+      }
+      ++committed;
+    }
+    // (3) the previous round's outputs into the owned nodes, while this round's MMAs run
+    if (rd >= 1) {
+      const int vs = (rd - 1) * kVoxPerRound + (tid >> 2);
+      const bool have = vs < nv;
+      const int own = have ? vown[vs] : 0;
+      const float s = have ? vscale[vs] : 0.0f;
+      // owned-node index of the voxel's node 0: staged origin minus the owned grid's offset (2, 2, 2)
+      int on0 = 0;
       if (have) {
+        const int o = vlist[vs];
+        const int ox = o % kIx, oy = (o / kIx) % kIy, oz = o / (kIx * kIy);
+        on0 = (ox - 2) + kOx * ((oy - 2) + kOy * (oz - 2));
+      }
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t r[32];
+        tc::tmem_ld32(lane_addr + ((((rd - 1) & 1) ? kColD1 : kColD0) + 32 * half), r);
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-          const int n = half * 32 + j;
+          const int n = 32 * half + j;
           if (n >= 60) continue;
           const int a = n / 3, c = n % 3;
-          const int ox = fx + kRing[a][0], oy = fy + kRing[a][1], oz = fz + kRing[a][2];
-          const int lx = ox - ix0, ly = oy - iy0, lz = oz - iz0;
-          const bool own = lx >= 0 && lx < kOx && ly >= 0 && ly < kOy && lz >= 0 && lz < kOz && ox >= 1 &&
-                           ox <= hx && oy >= 1 && oy <= hy && oz >= 1 && oz <= hz;
-          if (own) atomicAdd(&sacc[((lx + kOx * (ly + kOy * lz)) * 3 + c) * kLcg + l], s * __uint_as_float(r[j]));
+          if (own & (1 << a)) {
+            const int on = on0 + kRing[a][0] + kOx * (kRing[a][1] + kOy * kRing[a][2]);
+            atomicAdd(&sacc[(on * 3 + c) * kLcg + l], s * __uint_as_float(r[j]));
+          }
         }
       }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
   }
   if (fail) {
     if (tid == 0) atomicExch(err, 1);
-    tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)(rd & 1));  // bounded: drain this iteration's MMAs
+    // bounded with the full limit: wait for the last committed MMAs before freeing their memory
+    if (committed > 0) tc::mbar_wait(tc::smem_u32(&mbar), (uint32_t)((committed - 1) & 1));
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -696,21 +718,20 @@ __global__ void __launch_bounds__(128, 2)
   for (int i = tid; i < kOx * kOy * kOz * kLcg; i += 128) {
     const int on = i / kLcg;   // i % kLcg == l: the stride 128 is a multiple of kLcg
     const int lx = on % kOx, ly = (on / kOx) % kOy, lz = on / (kOx * kOy);
-    const int gx = ix0 + lx, gy = iy0 + ly, gz = iz0 + lz;
+    const int gx = 2 * t.x0 + lx, gy = 2 * t.y0 + ly, gz = 2 * t.z0 + lz;
     if (gx < 1 || gy < 1 || gz < 1 || gx > hx || gy > hy || gz > hz) continue;
     const int64_t node = node_index(D, gx, gy, gz);
     if (!(flags[node] & kNodeActive)) continue;
-    const int64_t b = vec_index(node, 0, lc);
+    const int64_t b = vec_index(node, 0, g * kLcg + l);
+    const int nin = (lx + 2) + kIx * ((ly + 2) + kIy * (lz + 2));
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float v = (float)(scale * D.scale * (double)sacc[(on * 3 + c) * kLcg + l]);
       y[b + c * kNLC] = v;
-      if (DOT) dot += (double)__ldg(u + b + c * kNLC) * (double)v;
+      if (DOT) dot += (double)sin[(nin * 3 + c) * kLcg + l] * (double)v;
     }
   }
   if (DOT) {
-    if (tid < kLcg) red[tid] = 0.0;
-    __syncthreads();
     atomicAdd(&red[l], dot);
     __syncthreads();
     if (tid < kLcg) atomicAdd(acc_pw + (int64_t)t.dom * kNLC + g * kLcg + tid, red[tid]);
