@@ -89,14 +89,16 @@ __global__ void __launch_bounds__(128) k_ebe(const Tile* __restrict__ tiles, con
   if (tid == 0) nv_sh = 0;
   if (tid < LCG) red[tid] = 0.0;
   for (int i = tid; i < ND * ND; i += NT) ske[i] = __ldg(ke + i);
-  // stage the input nodes of the brick and its 1-voxel halo
-  for (int i = tid; i < S::IX * S::IY * S::IZ * 3 * LCG; i += NT) {
-    const int l = i % LCG, c = (i / LCG) % 3, nl = i / (3 * LCG);
+  // stage the input nodes of the brick and its 1-voxel halo: the LCG load cases of one
+  // (node, component) are 16 contiguous bytes in the vector and in the stage (one vector load)
+  static_assert(sizeof(T) * LCG == 16, "one 16-byte load per (node, component)");
+  for (int i = tid; i < S::IX * S::IY * S::IZ * 3; i += NT) {
+    const int c = i % 3, nl = i / 3;
     const int gx = ix0 + nl % S::IX, gy = iy0 + (nl / S::IX) % S::IY, gz = iz0 + nl / (S::IX * S::IY);
-    T v = T(0);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (gx >= 0 && gy >= 0 && gz >= 0 && gx < D.n[0] && gy < D.n[1] && gz < D.n[2])
-      v = __ldg(u + vec_index(node_index(D, gx, gy, gz), c, g * LCG + l));
-    sin[i] = v;
+      v = __ldg(reinterpret_cast<const float4*>(u + vec_index(node_index(D, gx, gy, gz), c, g * LCG)));
+    reinterpret_cast<float4*>(sin)[i] = v;
   }
   for (int i = tid; i < S::OX * S::OY * S::OZ * 3 * LCG; i += NT) sacc[i] = T(0);
   __syncthreads();

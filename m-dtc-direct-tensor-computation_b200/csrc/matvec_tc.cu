@@ -562,13 +562,14 @@ __global__ void __launch_bounds__(128, 2)
   for (int i = tid; i < kOx * kOy * kOz * 3 * kLcg; i += 128) sacc[i] = 0.0f;
   // staged input nodes: fine coordinates 2 (x0 - 1) .. 2 (x0 + 4), and likewise in y, z
   const int ix0 = 2 * (t.x0 - 1), iy0 = 2 * (t.y0 - 1), iz0 = 2 * (t.z0 - 1);
-  for (int i = tid; i < kIx * kIy * kIz * 3 * kLcg; i += 128) {
-    const int l = i % kLcg, c = (i / kLcg) % 3, nl = i / (3 * kLcg);
+  // (the 4 load cases of one (node, component) are 16 contiguous bytes: one vector load)
+  for (int i = tid; i < kIx * kIy * kIz * 3; i += 128) {
+    const int c = i % 3, nl = i / 3;
     const int gx = ix0 + nl % kIx, gy = iy0 + (nl / kIx) % kIy, gz = iz0 + nl / (kIx * kIy);
-    float v = 0.0f;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (gx >= 0 && gy >= 0 && gz >= 0 && gx < D.n[0] && gy < D.n[1] && gz < D.n[2])
-      v = __ldg(u + vec_index(node_index(D, gx, gy, gz), c, g * kLcg + l));
-    sin[i] = v;
+      v = __ldg(reinterpret_cast<const float4*>(u + vec_index(node_index(D, gx, gy, gz), c, g * kLcg)));
+    reinterpret_cast<float4*>(sin)[i] = v;
   }
 
   // kept voxels touching the owned nodes (brick plus a 1-voxel halo below), x-fastest order,
