@@ -88,10 +88,15 @@ __global__ void __launch_bounds__(128) k_ebe(const Tile* __restrict__ tiles, con
   const int ix0 = M * (t.x0 - 1), iy0 = M * (t.y0 - 1), iz0 = M * (t.z0 - 1);
   if (tid == 0) nv_sh = 0;
   if (tid < LCG) red[tid] = 0.0;
-  for (int i = tid; i < ND * ND; i += NT) ske[i] = __ldg(ke + i);
+  // element matrix and input nodes: 16-byte loads, several in flight per thread
+  static_assert((sizeof(T) * ND * ND) % 16 == 0, "the element matrix is copied in 16-byte pieces");
+#pragma unroll 4
+  for (int i = tid; i < (int)(sizeof(T) * ND * ND / 16); i += NT)
+    reinterpret_cast<float4*>(ske)[i] = __ldg(reinterpret_cast<const float4*>(ke) + i);
   // stage the input nodes of the brick and its 1-voxel halo: the LCG load cases of one
   // (node, component) are 16 contiguous bytes in the vector and in the stage (one vector load)
   static_assert(sizeof(T) * LCG == 16, "one 16-byte load per (node, component)");
+#pragma unroll 4
   for (int i = tid; i < S::IX * S::IY * S::IZ * 3; i += NT) {
     const int c = i % 3, nl = i / 3;
     const int gx = ix0 + nl % S::IX, gy = iy0 + (nl / S::IX) % S::IY, gz = iz0 + nl / (S::IX * S::IY);

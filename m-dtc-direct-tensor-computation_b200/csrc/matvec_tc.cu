@@ -557,12 +557,14 @@ __global__ void __launch_bounds__(128, 2)
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   if (tid < kLcg) red[tid] = 0.0;
+#pragma unroll 4
   for (int i = tid; i < (int)(kSmemB / 16); i += 128)
     reinterpret_cast<float4*>(sB)[i] = __ldg(reinterpret_cast<const float4*>(bsplit) + i);
   for (int i = tid; i < kOx * kOy * kOz * 3 * kLcg; i += 128) sacc[i] = 0.0f;
   // staged input nodes: fine coordinates 2 (x0 - 1) .. 2 (x0 + 4), and likewise in y, z
   const int ix0 = 2 * (t.x0 - 1), iy0 = 2 * (t.y0 - 1), iz0 = 2 * (t.z0 - 1);
   // (the 4 load cases of one (node, component) are 16 contiguous bytes: one vector load)
+#pragma unroll 4
   for (int i = tid; i < kIx * kIy * kIz * 3; i += 128) {
     const int c = i % 3, nl = i / 3;
     const int gx = ix0 + nl % kIx, gy = iy0 + (nl / kIx) % kIy, gz = iz0 + nl / (kIx * kIy);
