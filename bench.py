@@ -576,6 +576,12 @@ def main():
                 "max_rel_err_vs_fp64_1e-10": timed_err, "accuracy_target": TARGET, "accuracy_sample": nchk,
                 "fp64_plain": fp64,
                 "dof_iterations_per_s": st["dof_iterations"] / (step_ms / 1e3),
+                # whole-solver roofline on the streaming model of an FP32 CG iteration: 40 bytes per
+                # unconstrained DOF, load case and inner iteration (operator in/out 8 B, CG update 32 B)
+                "solver_roofline": {"bytes_per_dof_rhs_iteration": 40,
+                                    "achieved_gbs": 40 * st["dof_iterations"] / (step_ms / 1e3) / 1e9,
+                                    "peak": peak, "unit": "GB/s",
+                                    "frac": 40 * st["dof_iterations"] / (step_ms / 1e3) / 1e9 / peak},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": src,
                              "traffic_source": (f"ncu dram bytes / algorithmic bytes = {ratio} on the 16x32^3 case "

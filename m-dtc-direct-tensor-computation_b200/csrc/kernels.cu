@@ -129,6 +129,87 @@ __device__ __forceinline__ void load_voxels(float (&sp)[2][2], const float* __re
     }
 }
 
+// FP32 slab on packed two-lane FMAs (sm_100 FFMA2).  A voxel of the row feeds two output rows
+// r of the thread's nodes: the corner at plane x (l0, node x) and the corner at plane x+1 (l1,
+// node x+1); one packed FMA applies both rows' entries of a column to one broadcast input value
+// (lane x: node x, lane y: node x+1), halving the FMA instructions of the scalar slab.  The table
+// holds the two rows' entries side by side, per voxel slot (b, c) of the row.
+__constant__ float2 c_khat32r2[4 * 3 * 24];   // [2b + c][r][col] = (Khat[3 l0 + r, col], Khat[3 l1 + r, col])
+
+template <bool FIRST>
+__device__ __forceinline__ void slab_rp(const float (&P0)[3][3][3], const float (&P1)[3][3][3], const float (&sv)[2][2],
+                                        float (&cur)[3], float (&nxt)[3]) {
+  if (FIRST) {
+    slab<float, true>(P0, P1, sv, cur, nxt);
+    return;
+  }
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float s = sv[b][c];
+      if (s != 0.0f) {
+        float2 acc[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) acc[r] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int mz = 0; mz < 2; ++mz)
+#pragma unroll
+          for (int my = 0; my < 2; ++my)
+#pragma unroll
+            for (int mx = 0; mx < 2; ++mx) {
+              const int lm = corner_local(mx, my, mz);
+#pragma unroll
+              for (int cj = 0; cj < 3; ++cj) {
+                const float v = mx ? P1[b + my][c + mz][cj] : P0[b + my][c + mz][cj];
+                const float2 vv = make_float2(v, v);
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                  acc[r] = __ffma2_rn(c_khat32r2[((2 * b + c) * 3 + r) * 24 + 3 * lm + cj], vv, acc[r]);
+              }
+            }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          cur[r] = fmaf(s, acc[r].x, cur[r]);
+          nxt[r] = fmaf(s, acc[r].y, nxt[r]);
+        }
+      }
+    }
+}
+
+// Two-plane register window of the slab sweeps: load the first two planes, advance by one
+// plane, apply the slab between them, read the centre value of plane x.  PACKED: the FP32
+// slab on packed FMAs (slab_rp); otherwise scalar FMAs (FP64, and the FP32 reference form).
+template <typename T, bool PACKED = false> struct Win {
+  T P0[3][3][3], P1[3][3][3];
+  template <bool GUARD>
+  __device__ __forceinline__ void start(const T* __restrict__ u, const DomDev& D, int x, int y, int z, int lc) {
+    load_plane<T, GUARD>(P0, u, D, x, y, z, lc);
+    load_plane<T, GUARD>(P1, u, D, x + 1, y, z, lc);
+  }
+  template <bool GUARD>
+  __device__ __forceinline__ void advance(const T* __restrict__ u, const DomDev& D, int x, int y, int z, int lc) {
+#pragma unroll
+    for (int py = 0; py < 3; ++py)
+#pragma unroll
+      for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
+    load_plane<T, GUARD>(P1, u, D, x, y, z, lc);
+  }
+  template <bool FIRST>
+  __device__ __forceinline__ void apply(const float (&sv)[2][2], T (&cur)[3], T (&nxt)[3]) const {
+    slab<T, FIRST>(P0, P1, sv, cur, nxt);
+  }
+  __device__ __forceinline__ T centre(int c) const { return P0[1][1][c]; }
+};
+template <> struct Win<float, true> : Win<float, false> {
+  template <bool FIRST>
+  __device__ __forceinline__ void apply(const float (&sv)[2][2], float (&cur)[3], float (&nxt)[3]) const {
+    slab_rp<FIRST>(P0, P1, sv, cur, nxt);
+  }
+};
+
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
 // node of the grid (reaction forces).
@@ -150,37 +231,30 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_matvec(con
   const int xhi = ALL ? D.n[0] - 1 : D.n[0] - 2, yhi = ALL ? D.n[1] - 1 : D.n[1] - 2, zhi = ALL ? D.n[2] - 1 : D.n[2] - 2;
   double dot = 0.0;
   if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi) {
-    T P0[3][3][3], P1[3][3][3];
+    Win<T, sizeof(T) == 4> W;
     float sv[2][2];
     T cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
-    load_plane<T, ALL>(P0, u, D, t.x0 - 1, yy, zz, lc);
-    load_plane<T, ALL>(P1, u, D, t.x0, yy, zz, lc);
+    W.template start<ALL>(u, D, t.x0 - 1, yy, zz, lc);
     load_voxels<ALL>(sv, svox, D, t.x0 - 1, yy, zz);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
-    slab<T, true>(P0, P1, sv, cur, nxt);
+    W.template apply<true>(sv, cur, nxt);
 #pragma unroll 1
     for (int i = 0; i < kTileX; ++i) {
       const int x = t.x0 + i;
       if (x > xhi) break;
-#pragma unroll
-      for (int py = 0; py < 3; ++py)
-#pragma unroll
-        for (int pz = 0; pz < 3; ++pz)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
-      load_plane<T, ALL>(P1, u, D, x + 1, yy, zz, lc);
+      W.template advance<ALL>(u, D, x + 1, yy, zz, lc);
       load_voxels<ALL>(sv, svox, D, x, yy, zz);
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
       for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = T(0); }
-      slab<T, false>(P0, P1, sv, cur, nxt);
+      W.template apply<false>(sv, cur, nxt);
       if (anyp | anyc) {
         const int64_t b = vec_index(node_index(D, x, yy, zz), 0, lc);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const T v = (T)(scale * D.scale * (double)cur[c]);
           y[b + c * kNLC] = v;
-          if (DOT) dot += (double)P0[1][1][c] * (double)v;
+          if (DOT) dot += (double)W.centre(c) * (double)v;
         }
       }
       anyp = anyc;
@@ -1967,6 +2041,15 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     macro_modes(1e-6, uu);   // the hard-coded boundary eps (mod_write_deck.f90:61)
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat64, kh, sizeof(kh), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
+    float2 khr[4 * 3 * 24];
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 2; ++c) {
+        const int l0 = corner_local(0, 1 - b, 1 - c), l1 = corner_local(1, 1 - b, 1 - c);
+        for (int r = 0; r < 3; ++r)
+          for (int col = 0; col < 24; ++col)
+            khr[((2 * b + c) * 3 + r) * 24 + col] = make_float2(kh32[col * 24 + 3 * l0 + r], kh32[col * 24 + 3 * l1 + r]);
+      }
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32r2, khr, sizeof(khr), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
     if (int e = upload_tc_operand(kh, s, msg)) return e;
     if (I.tensor_matvec || tune) {

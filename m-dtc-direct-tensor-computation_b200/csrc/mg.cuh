@@ -35,18 +35,6 @@ constexpr int kMgMaxCoarse = 4;                  // voxels per edge on the coars
 constexpr int kMgDenseN = 81;                    // 3 * 3^3 interior DOFs at most
 enum { kMgRes = 0, kMgPost = 1 };
 
-__device__ __forceinline__ void load_plane_f(float (&pl)[3][3][3], const float* __restrict__ u, const DomDev& D, int x,
-                                             int y, int z, int lc) {
-#pragma unroll
-  for (int py = 0; py < 3; ++py)
-#pragma unroll
-    for (int pz = 0; pz < 3; ++pz) {
-      const int64_t base = vec_index(node_index(D, x, y + py - 1, z + pz - 1), 0, lc);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) pl[py][pz][c] = __ldg(u + base + c * kNLC);
-    }
-}
-
 __device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __restrict__ svox, const DomDev& D, int vx,
                                               int y, int z) {
 #pragma unroll
@@ -75,30 +63,23 @@ __global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restric
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   double szz = 0.0, szr = 0.0;
   if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
-    float P0[3][3][3], P1[3][3][3];
+    Win<float, true> W;
     float sv[2][2];
     float cur[3] = {0.f, 0.f, 0.f}, nxt[3] = {0.f, 0.f, 0.f};
-    load_plane_f(P0, u, D, t.x0 - 1, yy, zz, lc);
-    load_plane_f(P1, u, D, t.x0, yy, zz, lc);
+    W.start<false>(u, D, t.x0 - 1, yy, zz, lc);
     load_voxels_f(sv, svox, D, t.x0 - 1, yy, zz);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
-    slab<float, true>(P0, P1, sv, cur, nxt);
+    W.apply<true>(sv, cur, nxt);
 #pragma unroll 1
     for (int i = 0; i < kTileX; ++i) {
       const int x = t.x0 + i;
       if (x > D.n[0] - 2) break;
-#pragma unroll
-      for (int py = 0; py < 3; ++py)
-#pragma unroll
-        for (int pz = 0; pz < 3; ++pz)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
-      load_plane_f(P1, u, D, x + 1, yy, zz, lc);
+      W.advance<false>(u, D, x + 1, yy, zz, lc);
       load_voxels_f(sv, svox, D, x, yy, zz);
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
       for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = 0.f; }
-      slab<float, false>(P0, P1, sv, cur, nxt);
+      W.apply<false>(sv, cur, nxt);
       if (anyp | anyc) {
         const int64_t n = node_index(D, x, yy, zz);
         const int64_t k0 = vec_index(n, 0, lc);
@@ -115,7 +96,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restric
           float dz[3];
           block_jacobi(binv, n, omega, res, dz);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) v[c] = P0[1][1][c] + dz[c];
+          for (int c = 0; c < 3; ++c) v[c] = W.centre(c) + dz[c];
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
