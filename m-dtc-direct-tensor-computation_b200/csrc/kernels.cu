@@ -903,7 +903,7 @@ enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, b
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
            bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF,
-           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bNumBufs };
+           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bMgNodes, bMgNodesC, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -1041,6 +1041,8 @@ struct MgPlan {
   std::vector<int64_t> sm_off, sm_n, in_off, in_n, all_off, all_n;
   std::vector<int> lists;
   std::vector<int64_t> list_off, list_n;
+  std::vector<int64_t> nodes_l;                     // levels >= 1: active interior nodes, (domain << kListShift) | node
+  std::vector<int64_t> nl_off, nl_n;
   std::vector<float> svox;                          // voxels of levels >= 1
   std::vector<float> minv;                          // ndom * 81 * 81
   int64_t nodes = 0;                                // nodes of levels >= 1
@@ -1207,6 +1209,7 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
     DomDev C;
     std::vector<float> sv;
     std::vector<Tile> t_in, t_sm, t_all;
+    std::vector<int32_t> n_in;   // active interior nodes (index inside the level's grid)
   };
   std::vector<std::vector<Level>> lev(ndom);
   P.minv.assign((size_t)ndom * kMgDenseN * kMgDenseN, 0.f);
@@ -1264,6 +1267,12 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
           for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
             if (any(x0, y0, z0, 0, nx - 1, ny - 1, nz - 1))
               Lv.t_all.push_back(Tile{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+      for (int z = 1; z < nz - 1; ++z)
+        for (int y = 1; y < ny - 1; ++y)
+          for (int x = 1; x < nx - 1; ++x) {
+            const int32_t k = x + nx * (y + ny * z);
+            if (act[k]) Lv.n_in.push_back(k);
+          }
       Lv.C = C;
       Lv.sv = nv;
       cur.swap(nv);
@@ -1278,7 +1287,8 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
   P.doms.assign((size_t)nl * ndom, DomDev{});
   P.sm_off.assign(nl, 0); P.sm_n.assign(nl, 0); P.in_off.assign(nl, 0); P.in_n.assign(nl, 0);
   P.all_off.assign(nl, 0); P.all_n.assign(nl, 0); P.list_off.assign(nl, 0); P.list_n.assign(nl, 0);
-  P.tiles.clear(); P.lists.clear(); P.svox.clear(); P.nodes = 0;
+  P.nl_off.assign(nl, 0); P.nl_n.assign(nl, 0);
+  P.tiles.clear(); P.lists.clear(); P.svox.clear(); P.nodes_l.clear(); P.nodes = 0;
   for (int d = 0; d < ndom; ++d) P.doms[d] = doms0[d];
   P.sm_off[0] = 0;
   for (const Tile& t : fine_i) if (nlev[t.dom] > 1) P.tiles.push_back(t);
@@ -1302,6 +1312,12 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
     append(&Level::t_sm, P.sm_off[l], P.sm_n[l]);
     append(&Level::t_in, P.in_off[l], P.in_n[l]);
     append(&Level::t_all, P.all_off[l], P.all_n[l]);
+    P.nl_off[l] = (int64_t)P.nodes_l.size();
+    for (int d = 0; d < ndom; ++d)
+      if (nlev[d] > l)
+        for (const int32_t k : lev[d][l].n_in)
+          P.nodes_l.push_back(((int64_t)d << kListShift) | (lev[d][l].C.node_off + k));
+    P.nl_n[l] = (int64_t)P.nodes_l.size() - P.nl_off[l];
   }
   for (int l = 0; l < nl; ++l) {
     P.list_off[l] = (int64_t)P.lists.size();
@@ -1321,11 +1337,14 @@ struct MgDev {
   const float *svox0, *svox, *binv0, *binv, *minv;
   const uint8_t *flags0, *flags;
   const int* lists;
+  const int64_t* nodes;  // levels >= 1: active interior nodes (segments nl_off / nl_n of the plan)
   float *b, *t, *z;      // levels >= 1
   float *t0, *z0;        // fine level
   int nen0;              // element of the fine level; HEX20 applies K with the brick kernel
   const Tile* bricks0;   // fine-level interior bricks (HEX20)
   int64_t nbricks0;
+  const int64_t* nodes0; // fine-level active interior nodes, (domain << kListShift) | node
+  int64_t nnodes0;
   const float* ke32;     // HEX20 unit element matrix (FP32)
   const float* ke20tc;   // its tensor-core operand, or null (brick SIMT kernel)
   int* err;
@@ -1368,7 +1387,11 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   int q = -1;
   if (!(fine && t_ready)) {
     q = fine ? I.begin(0) : -1;
-    k_mg_jacobi<<<g, kThreads, 0, s>>>(tsm, dl, fl, bi, b, fine ? P.omega0 : P.omega, t, act);
+    const int64_t items = (int64_t)kQuads * (fine ? M.nnodes0 : P.nl_n[l]);
+    if (items > 0)
+      k_mg_jacobi_flat<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(fine ? M.nodes0 : M.nodes + P.nl_off[l], items,
+                                                                         M.doms + (size_t)(l + 1) * M.ndom, bi, b,
+                                                                         fine ? P.omega0 : P.omega, t, act);
     if (fine) I.end(kcMgJacobi, q, 2 * vb + vb / 12, 0);   // b in, t out, 6 floats of D^-1 per node
     ++launches;
   }
@@ -1399,16 +1422,24 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
   q = fine ? I.begin(0) : -1;
-  if (P.in_n[l + 1] > 0)
-    k_mg_restrict<<<(unsigned)(3 * P.in_n[l + 1]), kThreads, 0, s>>>(M.tiles + P.in_off[l + 1], dc, M.flags, dl,
-                                                                    rbuf, M.b, act);
+  {
+    const int64_t items = (int64_t)kQuads * P.nl_n[l + 1];
+    if (items > 0)
+      k_mg_restrict_flat<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(M.nodes + P.nl_off[l + 1], items, dc, dl,
+                                                                           rbuf, M.b, act);
+  }
   if (fine) I.end(kcMgTransfer, q, vb * (1.0 + 1.0 / 8.0), 0);
   launches += 2;
   if (!fine) I.end(kcMgCoarse, q0, 0, 0);
   mg_vcycle(I, M, l + 1, r0, zz, zr, act, launches);
   const int q1 = fine ? -1 : I.begin(0);
   q = fine ? I.begin(0) : -1;
-  k_mg_prolong<<<g, kThreads, 0, s>>>(tsm, dl, fl, dc, M.z, cur, act);
+  {
+    const int64_t items = (int64_t)kQuads * (fine ? M.nnodes0 : P.nl_n[l]);
+    if (items > 0)
+      k_mg_prolong_flat<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(fine ? M.nodes0 : M.nodes + P.nl_off[l],
+                                                                          items, dl, dc, M.z, cur, act);
+  }
   if (fine) I.end(kcMgTransfer, q, vb * (2.0 + 1.0 / 8.0), 0);
   q = fine ? I.begin(0) : -1;
   if (l == 0 && M.nen0 == 20) {
@@ -1518,7 +1549,7 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   cudaStream_t s = I.stream;
   static const MgPlan kNoLevels;
   const MgPlan& P = M ? *M->P : kNoLevels;
-  const int nseg = 3 + 3 * P.nlev;
+  const int nseg = 3 + 4 * P.nlev;
   int e;
   if ((e = ensure(I, bCompactCnt, sizeof(int) * nseg, msg))) return e;
   if ((e = ensure(I, bTilesIc, sizeof(Tile) * std::max<int64_t>(W.nti, 1), msg))) return e;
@@ -1526,6 +1557,7 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   if ((e = ensure(I, bBricksIc, sizeof(Tile) * std::max<int64_t>(W.nbi, 1), msg))) return e;
   if ((e = ensure(I, bMgTilesC, sizeof(Tile) * std::max<size_t>(P.tiles.size(), 1), msg))) return e;
   if ((e = ensure(I, bMgListC, sizeof(int) * std::max<size_t>(P.lists.size(), 1), msg))) return e;
+  if ((e = ensure(I, bMgNodesC, sizeof(int64_t) * std::max<size_t>(P.nodes_l.size(), 1), msg))) return e;
   int* cnt = B<int>(I, bCompactCnt);
   DTC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * nseg, s));
   Tile* tc = B<Tile>(I, bTilesIc);
@@ -1533,13 +1565,15 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   Tile* bc = B<Tile>(I, bBricksIc);
   Tile* mt = B<Tile>(I, bMgTilesC);
   int* ml = B<int>(I, bMgListC);
+  int64_t* mn = B<int64_t>(I, bMgNodesC);
   launch_compact(W.ti, W.nti, act, tc, cnt + 0, s);
   launch_compact(W.nodes, W.nnodes, act, nc, cnt + 1, s);
   launch_compact(W.bi, W.nbi, act, bc, cnt + 2, s);
   for (int l = 0; l < P.nlev; ++l) {
-    launch_compact(M->tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 3 + 3 * l, s);
-    launch_compact(M->tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 4 + 3 * l, s);
-    launch_compact(M->lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 5 + 3 * l, s);
+    launch_compact(M->tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 3 + 4 * l, s);
+    launch_compact(M->tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 4 + 4 * l, s);
+    launch_compact(M->lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 5 + 4 * l, s);
+    launch_compact(M->nodes + P.nl_off[l], P.nl_n[l], act, mn + P.nl_off[l], cnt + 6 + 4 * l, s);
   }
   launches += nseg;
   if ((e = launch_check(msg))) return e;
@@ -1551,12 +1585,15 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   Wc.bi = bc; Wc.nbi = h[2];
   if (M) {
     Mc->bricks0 = bc; Mc->nbricks0 = h[2];
+    Mc->nodes0 = nc; Mc->nnodes0 = h[1];
     Mc->tiles = mt;
     Mc->lists = ml;
+    Mc->nodes = mn;
     for (int l = 0; l < P.nlev; ++l) {
-      Pc->sm_n[l] = h[3 + 3 * l];
-      Pc->in_n[l] = h[4 + 3 * l];
-      Pc->list_n[l] = h[5 + 3 * l];
+      Pc->sm_n[l] = h[3 + 4 * l];
+      Pc->in_n[l] = h[4 + 4 * l];
+      Pc->list_n[l] = h[5 + 4 * l];
+      Pc->nl_n[l] = h[6 + 4 * l];
     }
   }
   return DTC_OK;
@@ -1654,6 +1691,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   Pc.nlev = M.P->nlev; Pc.omega = M.P->omega; Pc.omega0 = M.P->omega0;
   Pc.sm_off = M.P->sm_off; Pc.sm_n = M.P->sm_n; Pc.in_off = M.P->in_off; Pc.in_n = M.P->in_n;
   Pc.list_off = M.P->list_off; Pc.list_n = M.P->list_n;
+  Pc.nl_off = M.P->nl_off; Pc.nl_n = M.P->nl_n;
   MgDev Mc = M;
   Mc.P = &Pc;
   int64_t listed = ndom;   // domains the current lists were compacted to
@@ -2225,7 +2263,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
           (e = ensure(I, bMgB, sizeof(float) * 72 * cn, msg)) || (e = ensure(I, bMgT, sizeof(float) * 72 * cn, msg)) ||
           (e = ensure(I, bMgZ, sizeof(float) * 72 * cn, msg)) ||
           (e = ensure(I, bMgMinv, sizeof(float) * mgp.minv.size(), msg)) ||
-          (e = ensure(I, bMgList, sizeof(int) * std::max<size_t>(mgp.lists.size(), 1), msg)))
+          (e = ensure(I, bMgList, sizeof(int) * std::max<size_t>(mgp.lists.size(), 1), msg)) ||
+          (e = ensure(I, bMgNodes, sizeof(int64_t) * std::max<size_t>(mgp.nodes_l.size(), 1), msg)))
         return e;
       DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgDoms], mgp.doms.data(), sizeof(DomDev) * mgp.doms.size(),
                                cudaMemcpyHostToDevice, s));
@@ -2239,6 +2278,9 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
                                cudaMemcpyHostToDevice, s));
       if (!mgp.lists.empty())
         DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgList], mgp.lists.data(), sizeof(int) * mgp.lists.size(),
+                                 cudaMemcpyHostToDevice, s));
+      if (!mgp.nodes_l.empty())
+        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgNodes], mgp.nodes_l.data(), sizeof(int64_t) * mgp.nodes_l.size(),
                                  cudaMemcpyHostToDevice, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bMgFlags], 0, cn, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bMgBinv32], 0, sizeof(float) * 6 * cn, s));
@@ -2268,6 +2310,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.flags0 = fl;
       mgd.flags = B<uint8_t>(I, bMgFlags);
       mgd.lists = B<int>(I, bMgList);
+      mgd.nodes = B<int64_t>(I, bMgNodes);
       mgd.b = B<float>(I, bMgB);
       mgd.t = B<float>(I, bMgT);
       mgd.z = B<float>(I, bMgZ);
@@ -2276,6 +2319,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgd.nen0 = NEN;
       mgd.bricks0 = W.bi;
       mgd.nbricks0 = W.nbi;
+      mgd.nodes0 = W.nodes;
+      mgd.nnodes0 = W.nnodes;
       mgd.ke32 = W.ke32;
       mgd.ke20tc = W.ke20tc;
       mgd.err = W.err;

@@ -20,11 +20,11 @@
 // correction, so the V-cycle is a fixed SPD operator.
 //
 // One V-cycle per CG iteration, per level l that is not a domain's coarsest:
-//   t_l = omega D_l^-1 b_l                        k_mg_jacobi (fine level: k_update_flat)
+//   t_l = omega D_l^-1 b_l                        k_mg_jacobi_flat (fine level: k_update_flat)
 //   r_l = b_l - K_l t_l                           k_mg_matvec<kMgRes>
-//   b_{l+1} = P^T r_l                             k_mg_restrict
+//   b_{l+1} = P^T r_l                             k_mg_restrict_flat
 //   (level l+1: recurse, or z_{l+1} = K^-1 b)     ...  / k_mg_coarse
-//   t_l += P z_{l+1}                              k_mg_prolong
+//   t_l += P z_{l+1}                              k_mg_prolong_flat
 //   z_l = t_l + omega D_l^-1 (b_l - K_l t_l)      k_mg_matvec<kMgPost> (+ z.z, z.b on level 0)
 // Levels >= 2 apply the smoothing step twice before and twice after the coarse correction.
 #pragma once
@@ -34,6 +34,9 @@ namespace dtc {
 constexpr int kMgMaxCoarse = 4;                  // voxels per edge on the coarsest level
 constexpr int kMgDenseN = 81;                    // 3 * 3^3 interior DOFs at most
 enum { kMgRes = 0, kMgPost = 1 };
+// node-list entries: (domain << kListShift) | node
+constexpr int kListShift = 40;
+constexpr int64_t kListNodeMask = (int64_t(1) << kListShift) - 1;
 
 __device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __restrict__ svox, const DomDev& D, int vx,
                                               int y, int z) {
@@ -186,114 +189,146 @@ __global__ void __launch_bounds__(kThreads) k_mg_combine(const Tile* __restrict_
   }
 }
 
-// b_c = P^T r_f on the active interior nodes of the coarse level (full weighting:
-// weight 1 at the coincident fine node, 1/2 per axis offset by one).
-__global__ void __launch_bounds__(kThreads) k_mg_restrict(const Tile* __restrict__ tiles,
-                                                          const DomDev* __restrict__ doms_c,
-                                                          const uint8_t* __restrict__ flags_c,
-                                                          const DomDev* __restrict__ doms_f,
-                                                          const float* __restrict__ r_f, float* __restrict__ b_c,
-                                                          const int* __restrict__ dom_active) {
-  const Tile t = tiles[blockIdx.x / 3];
-  if (dom_active && !dom_active[t.dom]) return;
-  const DomDev C = doms_c[t.dom];
-  const DomDev F = doms_f[t.dom];
-  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
-  const int row = threadIdx.x >> 3;
-  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
-  if (yy < 1 || yy > C.n[1] - 2 || zz < 1 || zz > C.n[2] - 2) return;
-  for (int i = 0; i < kTileX; ++i) {
-    const int x = t.x0 + i;
-    if (x > C.n[0] - 2) break;
-    const int64_t nc = node_index(C, x, yy, zz);
-    if (!(flags_c[nc] & kNodeActive)) continue;
-    float s[3] = {0.f, 0.f, 0.f};
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int fz = 2 * zz + dz;
-      if (fz > F.n[2] - 1) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int fy = 2 * yy + dy;
-        if (fy > F.n[1] - 1) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int fx = 2 * x + dx;
-          if (fx > F.n[0] - 1) continue;
-          const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
-          const int64_t k = vec_index(node_index(F, fx, fy, fz), 0, lc);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) s[c] = fmaf(wgt, __ldg(r_f + k + c * kNLC), s[c]);
-        }
-      }
-    }
-    const int64_t k0 = vec_index(nc, 0, lc);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) b_c[k0 + c * kNLC] = s[c];
-  }
+// -------------------------------------------------------------------------------------
+// Grid transfers over node lists: one thread per (active interior node, 4 load cases) with
+// 16-byte loads and stores, all threads independent.  (A tile walk, one thread per node row and
+// load case, visits a tile's nodes one after the other including its inactive ones, and ran at
+// 27-38 % of the HBM bandwidth; these lists carry only the active nodes.)
+constexpr int kQuads = kNLC / 4;
+
+__device__ __forceinline__ float4 ldq(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void fmaq(float w, float4 v, float4& s) {
+  s.x = fmaf(w, v.x, s.x);
+  s.y = fmaf(w, v.y, s.y);
+  s.z = fmaf(w, v.z, s.z);
+  s.w = fmaf(w, v.w, s.w);
 }
 
-// t_f += P z_c on the active interior nodes of the fine level (trilinear).
-__global__ void __launch_bounds__(kThreads) k_mg_prolong(const Tile* __restrict__ tiles,
+// t_f += P z_c (trilinear) over a fine level's node list; domains without a coarser level
+// (their coarse record is empty) are skipped.
+__global__ void __launch_bounds__(256) k_mg_prolong_flat(const int64_t* __restrict__ list, int64_t nitems,
                                                          const DomDev* __restrict__ doms_f,
-                                                         const uint8_t* __restrict__ flags_f,
                                                          const DomDev* __restrict__ doms_c,
                                                          const float* __restrict__ z_c, float* __restrict__ t_f,
                                                          const int* __restrict__ dom_active) {
-  const Tile t = tiles[blockIdx.x / 3];
-  if (dom_active && !dom_active[t.dom]) return;
-  const DomDev F = doms_f[t.dom];
-  const DomDev C = doms_c[t.dom];
-  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
-  const int row = threadIdx.x >> 3;
-  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
-  if (yy < 1 || yy > F.n[1] - 2 || zz < 1 || zz > F.n[2] - 2) return;
-  const int cy0 = yy >> 1, cy1 = (yy + 1) >> 1, cz0 = zz >> 1, cz1 = (zz + 1) >> 1;
-  for (int i = 0; i < kTileX; ++i) {
-    const int x = t.x0 + i;
-    if (x > F.n[0] - 2) break;
-    const int64_t nf = node_index(F, x, yy, zz);
-    if (!(flags_f[nf] & kNodeActive)) continue;
-    const int cx0 = x >> 1, cx1 = (x + 1) >> 1;
-    float s[3] = {0.f, 0.f, 0.f};
-    // odd coordinates average the two coarse neighbours, even ones take the coincident node
-    // (cx0 == cx1 then, and each of the duplicate corners carries half of it)
-    for (int kz = 0; kz < 2; ++kz)
-      for (int ky = 0; ky < 2; ++ky)
-        for (int kx = 0; kx < 2; ++kx) {
-          const int64_t k = vec_index(node_index(C, kx ? cx1 : cx0, ky ? cy1 : cy0, kz ? cz1 : cz0), 0, lc);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nitems) return;
+  const int64_t e = __ldg(list + i / kQuads);
+  const int dom = (int)(e >> kListShift);
+  if (dom_active && !dom_active[dom]) return;
+  const DomDev C = doms_c[dom];
+  if (C.n[0] == 0) return;
+  const DomDev F = doms_f[dom];
+  const int64_t nf = e & kListNodeMask;
+  const int loc = (int)(nf - F.node_off);
+  const int x = loc % F.n[0], yz = loc / F.n[0];
+  const int y = yz % F.n[1], z = yz / F.n[1];
+  const int lc0 = 4 * (int)(i % kQuads);
+  const int cx0 = x >> 1, cx1 = (x + 1) >> 1, cy0 = y >> 1, cy1 = (y + 1) >> 1, cz0 = z >> 1, cz1 = (z + 1) >> 1;
+  float4 s[3];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) s[c] = fmaf(0.125f, __ldg(z_c + k + c * kNLC), s[c]);
-        }
-    const int64_t k0 = vec_index(nf, 0, lc);
+  for (int c = 0; c < 3; ++c) s[c] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) t_f[k0 + c * kNLC] += s[c];
+  for (int kz = 0; kz < 2; ++kz)
+#pragma unroll
+    for (int ky = 0; ky < 2; ++ky)
+#pragma unroll
+      for (int kx = 0; kx < 2; ++kx) {
+        const int64_t k = vec_index(node_index(C, kx ? cx1 : cx0, ky ? cy1 : cy0, kz ? cz1 : cz0), 0, lc0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fmaq(0.125f, ldq(z_c + k + c * kNLC), s[c]);
+      }
+  const int64_t k0 = vec_index(nf, 0, lc0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float4* q = reinterpret_cast<float4*>(t_f + k0 + c * kNLC);
+    float4 v = *q;
+    v.x += s[c].x;
+    v.y += s[c].y;
+    v.z += s[c].z;
+    v.w += s[c].w;
+    *q = v;
   }
 }
 
-// t = omega D^-1 b on the active interior nodes (pre-smoothing from a zero guess).
-__global__ void __launch_bounds__(kThreads) k_mg_jacobi(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
-                                                        const uint8_t* __restrict__ flags,
+// b_c = P^T r_f (full weighting) over a coarse level's node list.
+__global__ void __launch_bounds__(256) k_mg_restrict_flat(const int64_t* __restrict__ list, int64_t nitems,
+                                                          const DomDev* __restrict__ doms_c,
+                                                          const DomDev* __restrict__ doms_f,
+                                                          const float* __restrict__ r_f, float* __restrict__ b_c,
+                                                          const int* __restrict__ dom_active) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nitems) return;
+  const int64_t e = __ldg(list + i / kQuads);
+  const int dom = (int)(e >> kListShift);
+  if (dom_active && !dom_active[dom]) return;
+  const DomDev C = doms_c[dom];
+  const DomDev F = doms_f[dom];
+  const int64_t nc = e & kListNodeMask;
+  const int loc = (int)(nc - C.node_off);
+  const int x = loc % C.n[0], yz = loc / C.n[0];
+  const int y = yz % C.n[1], z = yz / C.n[1];
+  const int lc0 = 4 * (int)(i % kQuads);
+  float4 s[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) s[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int fz = 2 * z + dz;
+    if (fz > F.n[2] - 1) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int fy = 2 * y + dy;
+      if (fy > F.n[1] - 1) continue;
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int fx = 2 * x + dx;
+        if (fx > F.n[0] - 1) continue;
+        const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+        const int64_t k = vec_index(node_index(F, fx, fy, fz), 0, lc0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fmaq(wgt, ldq(r_f + k + c * kNLC), s[c]);
+      }
+    }
+  }
+  const int64_t k0 = vec_index(nc, 0, lc0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) *reinterpret_cast<float4*>(b_c + k0 + c * kNLC) = s[c];
+}
+
+// t = omega D^-1 b (pre-smoothing from a zero guess) over a level's node list, for the domains
+// that have a coarser level (the record of the next level is not empty).
+__global__ void __launch_bounds__(256) k_mg_jacobi_flat(const int64_t* __restrict__ list, int64_t nitems,
+                                                        const DomDev* __restrict__ doms_next,
                                                         const float* __restrict__ binv, const float* __restrict__ b,
                                                         float omega, float* __restrict__ t_out,
                                                         const int* __restrict__ dom_active) {
-  const Tile t = tiles[blockIdx.x / 3];
-  if (dom_active && !dom_active[t.dom]) return;
-  const DomDev D = doms[t.dom];
-  const int lc = (blockIdx.x % 3) * kLcGroup + (threadIdx.x & 7);
-  const int row = threadIdx.x >> 3;
-  const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
-  if (yy < 1 || yy > D.n[1] - 2 || zz < 1 || zz > D.n[2] - 2) return;
-  for (int i = 0; i < kTileX; ++i) {
-    const int x = t.x0 + i;
-    if (x > D.n[0] - 2) break;
-    const int64_t n = node_index(D, x, yy, zz);
-    if (!(flags[n] & kNodeActive)) continue;
-    const int64_t k0 = vec_index(n, 0, lc);
-    float r[3], z[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) r[c] = b[k0 + c * kNLC];
-    block_jacobi(binv, n, omega, r, z);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) t_out[k0 + c * kNLC] = z[c];
-  }
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nitems) return;
+  const int64_t e = __ldg(list + i / kQuads);
+  const int dom = (int)(e >> kListShift);
+  if (dom_active && !dom_active[dom]) return;
+  if (doms_next[dom].n[0] == 0) return;
+  const int64_t n = e & kListNodeMask;
+  const int64_t k0 = vec_index(n, 0, 4 * (int)(i % kQuads));
+  const float4 r0 = ldq(b + k0), r1 = ldq(b + k0 + kNLC), r2 = ldq(b + k0 + 2 * kNLC);
+  const float* bp = binv + n * 6;
+  const float b0 = __ldg(bp), b1 = __ldg(bp + 1), b2 = __ldg(bp + 2), b3 = __ldg(bp + 3), b4 = __ldg(bp + 4),
+              b5 = __ldg(bp + 5);
+  float4 z0, z1, z2;
+  z0.x = omega * (b0 * r0.x + b3 * r1.x + b4 * r2.x);
+  z1.x = omega * (b3 * r0.x + b1 * r1.x + b5 * r2.x);
+  z2.x = omega * (b4 * r0.x + b5 * r1.x + b2 * r2.x);
+  z0.y = omega * (b0 * r0.y + b3 * r1.y + b4 * r2.y);
+  z1.y = omega * (b3 * r0.y + b1 * r1.y + b5 * r2.y);
+  z2.y = omega * (b4 * r0.y + b5 * r1.y + b2 * r2.y);
+  z0.z = omega * (b0 * r0.z + b3 * r1.z + b4 * r2.z);
+  z1.z = omega * (b3 * r0.z + b1 * r1.z + b5 * r2.z);
+  z2.z = omega * (b4 * r0.z + b5 * r1.z + b2 * r2.z);
+  z0.w = omega * (b0 * r0.w + b3 * r1.w + b4 * r2.w);
+  z1.w = omega * (b3 * r0.w + b1 * r1.w + b5 * r2.w);
+  z2.w = omega * (b4 * r0.w + b5 * r1.w + b2 * r2.w);
+  *reinterpret_cast<float4*>(t_out + k0) = z0;
+  *reinterpret_cast<float4*>(t_out + k0 + kNLC) = z1;
+  *reinterpret_cast<float4*>(t_out + k0 + 2 * kNLC) = z2;
 }
 
 // Coarsest level: z = Minv b over the <= 27 interior nodes of each listed domain (one CTA per
@@ -344,8 +379,6 @@ __global__ void __launch_bounds__(256) k_mg_coarse(const int* __restrict__ list,
 // -------------------------------------------------------------------------------------
 // Flat CG vector kernels of the multigrid path: one thread per (active interior node, 4 load
 // cases), 16-byte loads and stores, the list entry packs (domain << 40) | node.
-constexpr int kListShift = 40;
-constexpr int64_t kListNodeMask = (int64_t(1) << kListShift) - 1;
 
 __device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
   const float4 q = *reinterpret_cast<const float4*>(p);
