@@ -62,11 +62,11 @@ def parse():
     p.add_argument("--profile-step", action="store_true",
                    help="one warm-up and one timed-free mixed solve only (for ncu captures)")
     p.add_argument("--elem", type=int, default=8, choices=[8, 20], help="element type of --profile-step")
-    p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4"],
+    p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c3", "c4", "me2"],
                    help="c1 (default): the headline line; c0/c2/c3/c4 print their own measurement lines")
     a = p.parse_args()
     if a.ndom is None:
-        a.ndom = {"c2": 256, "c3": 2000, "c4": 64}.get(a.config, 512)
+        a.ndom = {"c2": 256, "c3": 2000, "c4": 64, "me2": 128}.get(a.config, 512)
     return a
 
 
@@ -341,6 +341,54 @@ def run_config(args, dtc):
                      "rotation_fp64_tflops": (rot["flops_per_launch"] * rot["launches"] / (rot["ms_total"] / 1e3)
                                               / 1e12 if rot and rot["ms_total"] > 0 else None),
                      "voxels": int(sum(int(L) ** 3 for L in Ls))})
+    elif args.config == "me2":
+        # macro order 2 (20-node macro element, 60 load cases): HEX08 domains of 32^3, BV/TV
+        # U(0.10, 0.40), per-voxel E; mixed (multigrid, the reference's reaction projection) vs
+        # plain FP64, each at its calibrated rtol; the oracle at rtol 1e-10 on 4 domains
+        n = args.ndom
+        grays, _ = make_inputs(dtc, n, args.L)
+        doms = [dtc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=syn.modulus_of_gray(g))
+                for g in grays]
+        sample = doms[:: max(1, n // 8)]
+        with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device=local, macro_order=2) as ref:
+            truth = ref.solve(sample)
+        out = {}
+        ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8]
+        for arm, kw in (("mixed", dict(precision="mixed", inner_precond="mg", mixed_matvec=args.matvec)),
+                        ("fp64", dict(precision="fp64"))):
+            for rt in ladder:
+                with dtc.Solver(rtol=rt, rotation_search=False, device=local, macro_order=2, **kw) as sv:
+                    err = _err(sv.solve(sample), truth)
+                if err <= 0.5 * TARGET:
+                    break
+            with dtc.Solver(rtol=rt, rotation_search=False, device=local, macro_order=2, **kw) as sv:
+
+                def step():
+                    sv.solve(doms)
+                    return sv.stats()["ms_solve"]
+                dev, wall = _timed(step, steps, warm)
+            out[arm] = {"domains_per_s": n / (dev / 1e3), "ms_per_step": dev, "rtol": rt, "max_rel_err": err,
+                        "e2e_domains_per_s": n / wall}
+        orc = ge.load_oracle()
+        odoms = [orc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, macro_order=2,
+                            E_voxel=syn.modulus_of_gray(g)) for g in grays[:4]]
+        t0 = time.perf_counter()
+        oref = orc.solve_batch(odoms, nthreads=4)
+        tcpu = time.perf_counter() - t0
+        with dtc.Solver(precision="mixed", rtol=out["mixed"]["rtol"], rotation_search=False, device=local,
+                        macro_order=2, inner_precond="mg") as sv:
+            res = sv.solve(doms[:4])
+
+        def rel(a, b):
+            return float(np.abs(a - b).max() / np.abs(b).max())
+        line.update({"workload": f"macro order 2 (60 load cases): {n} HEX08 domains of {args.L}^3, "
+                                 "BV/TV U(0.10,0.40), per-voxel E", "mixed": out["mixed"], "fp64_plain": out["fp64"],
+                     "speedup_mixed_over_fp64": out["mixed"]["domains_per_s"] / out["fp64"]["domains_per_s"],
+                     "vs_oracle": {"sample": 4, "oracle_rtol": 1e-10, "oracle_s": tcpu,
+                                   "max_rel_err_c": max(rel(r["c"], t["c"]) for r, t in zip(res, oref)),
+                                   "max_rel_err_ff": max(rel(r["ff"], t["ff"]) for r, t in zip(res, oref)),
+                                   "max_rel_err_kmacro": max(rel(r["kmacro"], t["kmacro"])
+                                                             for r, t in zip(res, oref))}})
     elif args.config == "c4":
         # adjoint: 64 HEX08 domains of 48^3, loss ||C - C_target||_F^2, gradient vs one forward solve
         n = args.ndom

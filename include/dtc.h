@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define DTC_ABI_VERSION 1
+#define DTC_ABI_VERSION 2
 
 typedef enum dtc_status {
   DTC_OK = 0,
@@ -101,6 +101,15 @@ typedef struct dtc_options {
                               is freed keeps the full bound */
   int32_t device_mesher;   /* 1: mesh the domains on the device (the reference numbering, bit
                               for bit the host planner's result); 0: on host threads */
+  int32_t macro_order;     /* 'Element order on macro scale' (mod_dtc_main_subroutines.f90:498-508):
+                              1 (or 0) = 8-node macro element, 24 load cases; 2 = 20-node macro
+                              element, 60 load cases (init_displ_hexe20, mod_write_deck.f90:118-279;
+                              the quadratic load-case matrix, mod_struct_calcmat.f90:1780-2028, with
+                              its typing defects repaired; quad face sums :368-401).  Order 2 solves
+                              the 60 load cases as three passes of 24 columns, forms ff by the
+                              reference's reaction projection (tensor_estimator must be 0), needs
+                              dtc_domain_out.macro2 on every record, and has no adjoint
+                              (keep_displacements must be 0) */
 } dtc_options;
 
 typedef struct dtc_domain_in {
@@ -120,6 +129,16 @@ typedef struct dtc_domain_in {
   double nu;               /* POISSON_RATIO; all domains of one call share it */
   double rve_strain;       /* RVE_STRAIN: eps of the load-case matrix vv */
 } dtc_domain_in;
+
+/* The leaves of a macro order 2 record whose size differs from the 24-load-case record: the
+ * reference sizes ff and the effective numerical stiffness no_lc x no_lc
+ * (mod_struct_calcmat.f90:158-160,289-303) and solves no_lc = 60 load cases. */
+typedef struct dtc_macro2_out {
+  int64_t iters[60];       /* CG iterations per load case */
+  double relres[60];       /* final ||D^-1 r|| / ||D^-1 b|| per load case */
+  double ff[3600];         /* "Domain forces" ff(60,60), column-major */
+  double kmacro[3600];     /* "Effective numerical stiffness" ff * vv^-1 (60 x 60) */
+} dtc_macro2_out;
 
 typedef struct dtc_domain_out {
   int32_t status;          /* DTC_DOMAIN_* */
@@ -145,6 +164,10 @@ typedef struct dtc_domain_out {
                               room for 72*(L0+1)(L1+1)(L2+1) doubles (HEX08) or
                               72*(2L0+1)(2L1+1)(2L2+1) (HEX20) always suffices */
   double* force;           /* optional: 24 x 3nn reaction forces AA_org*u, same layout */
+  dtc_macro2_out* macro2;  /* macro_order 2: caller-owned, required; receives iters, relres, ff and
+                              kmacro, while the 24-sized fields above stay zero (displ/force then
+                              hold 60 x 3nn values: room for 180*(grid nodes) doubles).  Ignored
+                              for macro order 1 */
 } dtc_domain_out;
 
 typedef struct dtc_mesh_out {
@@ -156,7 +179,10 @@ typedef struct dtc_mesh_out {
   int64_t* elems;          /* optional: elem_type*ne node ids, 1-based, 0 = dropped node */
   double* nodes;           /* optional: 3*nn coordinates */
   int64_t* bnode_ids;      /* optional: nb constrained node ids in node order */
-  double* bnode_vals;      /* optional: 24 x 3nb prescribed displacements, column-major */
+  double* bnode_vals;      /* optional: nl x 3nb prescribed displacements, column-major, nl = 24
+                              (macro order 1) or 60 (macro order 2) */
+  int32_t macro_order;     /* in: macro element order of bnode_vals, 1 (or 0) or 2 */
+  int32_t pad_;
 } dtc_mesh_out;
 
 typedef struct dtc_handle dtc_handle;

@@ -68,9 +68,14 @@ class Domain:
 _OUT_DTYPE = capi.numpy_dtype(capi.DomainOut)
 
 
-def _results(outs, keep):
+_M2_DTYPE = capi.numpy_dtype(capi.Macro2Out)
+
+
+def _results(outs, keep, macro2=None):
     """Result dicts of a dtc_domain_out array: each field copied once for the whole batch, then
-    per-domain rows (the 24 x 24 / 6 x 6 / 3 x 3 leaves are column-major, as in the record)."""
+    per-domain rows (the 24 x 24 / 6 x 6 / 3 x 3 leaves are column-major, as in the record).
+    macro2: the dtc_macro2_out array of a macro order 2 solve, whose 60-load-case leaves replace
+    iters, relres, ff and kmacro."""
     raw = (C.c_char * C.sizeof(outs)).from_buffer(outs)
     a = np.frombuffer(raw, dtype=_OUT_DTYPE)
     n = len(a)
@@ -81,6 +86,13 @@ def _results(outs, keep):
     mat = {k: np.array(a[k]).reshape((n,) + shape[::-1]).transpose(0, 2, 1)
            for k, shape in (("ff", (24, 24)), ("kmacro", (24, 24)), ("c", (6, 6)), ("ee", (6, 6)),
                             ("cr1_aa", (3, 3)), ("cr1_ee", (6, 6)), ("cr2_aa", (3, 3)), ("cr2_ee", (6, 6)))}
+    nl = 24
+    if macro2 is not None:
+        nl = 60
+        m2 = np.frombuffer((C.c_char * C.sizeof(macro2)).from_buffer(macro2), dtype=_M2_DTYPE)
+        ar["iters"], ar["relres"] = np.array(m2["iters"]), np.array(m2["relres"])
+        for k in ("ff", "kmacro"):
+            mat[k] = np.array(m2[k]).reshape(n, 60, 60).transpose(0, 2, 1)
     res = []
     for i in range(n):
         r = {k: sc[k][i] for k in ("status", "refine_steps", "domain_number", "ne", "nn", "nb", "n_free_dof",
@@ -92,8 +104,8 @@ def _results(outs, keep):
                     "ee": mat[k + "_ee"][i], "crit": sc[k + "_crit"][i], "iters": sc[k + "_iters"][i]}
         if keep:
             nn = r["nn"]
-            r["displ"] = keep[i][0][: 24 * 3 * nn].reshape(24, 3 * nn)
-            r["force"] = keep[i][1][: 24 * 3 * nn].reshape(24, 3 * nn)
+            r["displ"] = keep[i][0][: nl * 3 * nn].reshape(nl, 3 * nn)
+            r["force"] = keep[i][1][: nl * 3 * nn].reshape(nl, 3 * nn)
         res.append(r)
     return res
 
@@ -104,7 +116,7 @@ class Solver:
     def __init__(self, precision="fp64", rtol=1e-3, max_it=500000, inner_rtol=0.0, max_refine=12,
                  rotation_search=True, device=0, host_threads=0, keep_displacements=False,
                  profile_kernels=False, mixed_matvec="simt", inner_precond="block", estimator="reaction",
-                 chunk_domains=0, graphs=True, tc_wait_spins=0, device_mesher=False):
+                 chunk_domains=0, graphs=True, tc_wait_spins=0, device_mesher=False, macro_order=1):
         self.lib = capi.load()
         o = capi.Options()
         self.lib.dtc_default_options(C.byref(o))
@@ -120,6 +132,8 @@ class Solver:
         o.graph_chunks = 0 if graphs else 1
         o.tc_wait_spins = int(tc_wait_spins)
         o.device_mesher = int(bool(device_mesher))
+        o.macro_order = int(macro_order)
+        self.macro_order = int(macro_order)
         self.options = o
         h = C.c_void_p()
         rc = self.lib.dtc_create(C.byref(h), C.byref(o))
@@ -149,17 +163,28 @@ class Solver:
         n = len(domains)
         ins = (capi.DomainIn * n)(*[d.struct for d in domains])
         outs = (capi.DomainOut * n)()
+        m2 = self._macro2(outs)
+        nl = 60 if m2 is not None else 24
         keep = []
         if want_fields:
             for i, d in enumerate(domains):
                 m = 1 if d.elem_type == HEX08 else 2   # HEX20 nodes live on the doubled grid
-                cap = 24 * 3 * (m * d.L[0] + 1) * (m * d.L[1] + 1) * (m * d.L[2] + 1)
+                cap = nl * 3 * (m * d.L[0] + 1) * (m * d.L[1] + 1) * (m * d.L[2] + 1)
                 fd, ff_ = np.zeros(cap), np.zeros(cap)
                 keep.append((fd, ff_))
                 outs[i].displ = fd.ctypes.data_as(C.POINTER(C.c_double))
                 outs[i].force = ff_.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.dtc_solve_batch(self.handle, ins, n, outs))
-        return _results(outs, keep if want_fields else None)
+        return _results(outs, keep if want_fields else None, m2)
+
+    def _macro2(self, outs):
+        """Macro order 2: one dtc_macro2_out per record (the 60-load-case leaves)."""
+        if self.macro_order != 2:
+            return None
+        m2 = (capi.Macro2Out * len(outs))()
+        for i in range(len(outs)):
+            outs[i].macro2 = C.cast(C.byref(m2, i * C.sizeof(capi.Macro2Out)), C.POINTER(capi.Macro2Out))
+        return m2
 
     def solve_device_moduli(self, domains, e_ptrs):
         """solve() with each domain's per-voxel moduli in device memory: e_ptrs[i] is the device
@@ -167,9 +192,10 @@ class Solver:
         n = len(domains)
         ins = (capi.DomainIn * n)(*[d.struct for d in domains])
         outs = (capi.DomainOut * n)()
+        m2 = self._macro2(outs)
         ptrs = (C.c_void_p * n)(*[C.c_void_p(int(p)) if p else None for p in e_ptrs])
         self._check(self.lib.dtc_solve_batch_device_moduli(self.handle, ins, n, outs, ptrs))
-        return _results(outs, None)
+        return _results(outs, None, m2)
 
     def energy_grad_device(self, dloss_dc, grad_ptrs):
         """energy_grad() into device memory: grad_ptrs[i] is the device address of the L0*L1*L2
@@ -179,12 +205,12 @@ class Solver:
         ptrs = (C.c_void_p * n)(*[C.c_void_p(int(p)) for p in grad_ptrs])
         self._check(self.lib.dtc_energy_grad_device(self.handle, dl.ctypes.data_as(C.POINTER(C.c_double)), ptrs, n))
 
-    def mesh_batch(self, domains):
+    def mesh_batch(self, domains, macro_order=1):
         """mesh_domain() for many domains of one element type, computed on the device
         (dtc_mesh_batch)."""
         n = len(domains)
         ins = (capi.DomainIn * n)(*[d.struct for d in domains])
-        made = [_mesh_out(d) for d in domains]
+        made = [_mesh_out(d, macro_order) for d in domains]
         outs = (capi.MeshOut * n)(*[m[0] for m in made])
         self._check(self.lib.dtc_mesh_batch(self.handle, ins, n, outs))
         return [_mesh_result(d, outs[i], made[i][1]) for i, d in enumerate(domains)]
@@ -237,7 +263,8 @@ def element_stiffness(elem_type, E, a, nu):
     return ke
 
 
-def _mesh_out(domain):
+def _mesh_out(domain, macro_order=1):
+    nl = 60 if macro_order == 2 else 24
     L = domain.L
     nen = domain.elem_type
     m = 1 if nen == HEX08 else 2
@@ -246,8 +273,9 @@ def _mesh_out(domain):
     elems = np.zeros(nen * max_elems, np.int64)
     nodes = np.zeros(3 * max_nodes)
     bids = np.zeros(max_nodes, np.int64)
-    bvals = np.zeros(24 * 3 * max_nodes)
+    bvals = np.zeros(nl * 3 * max_nodes)
     o = capi.MeshOut()
+    o.macro_order = macro_order
     o.cap_elems, o.cap_nodes = max_elems, max_nodes
     o.elems = elems.ctypes.data_as(C.POINTER(C.c_int64))
     o.nodes = nodes.ctypes.data_as(C.POINTER(C.c_double))
@@ -258,17 +286,19 @@ def _mesh_out(domain):
 
 def _mesh_result(domain, o, keep):
     elems, nodes, bids, bvals = keep
+    nl = 60 if o.macro_order == 2 else 24
     nen = domain.elem_type
     ne, nn, nb = o.ne, o.nn, o.nb
     return {"status": o.status, "ne": ne, "nn": nn, "nb": nb, "last_elem_partial": bool(o.last_elem_partial),
             "elems": elems[: nen * ne].reshape(ne, nen), "nodes": nodes[: 3 * nn].reshape(nn, 3),
-            "bnode_ids": bids[:nb], "bnode_vals": bvals[: 24 * 3 * nb].reshape(24, 3 * nb, order="F")}
+            "bnode_ids": bids[:nb], "bnode_vals": bvals[: nl * 3 * nb].reshape(nl, 3 * nb, order="F")}
 
 
-def mesh_domain(domain):
-    """Reference mesh + boundary conditions of one domain (host only, no GPU needed)."""
+def mesh_domain(domain, macro_order=1):
+    """Reference mesh + boundary conditions of one domain (host only, no GPU needed); the
+    prescribed values are those of the 24 (macro order 1) or 60 (macro order 2) load cases."""
     lib = capi.load()
-    o, keep = _mesh_out(domain)
+    o, keep = _mesh_out(domain, macro_order)
     rc = lib.dtc_mesh_domain(C.byref(domain.struct), C.byref(o))
     if rc != capi.DTC_OK:
         raise DTCError(rc, "dtc_mesh_domain failed")

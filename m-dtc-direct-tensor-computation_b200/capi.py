@@ -10,7 +10,7 @@ from pathlib import Path
 
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libdtc.so"
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 DTC_OK, DTC_ERR_INVALID_ARGUMENT, DTC_ERR_CUDA, DTC_ERR_OUT_OF_MEMORY, DTC_ERR_NO_DEVICE, \
     DTC_ERR_ABI_MISMATCH, DTC_ERR_INTERNAL = range(7)
@@ -30,7 +30,7 @@ class Options(C.Structure):
         ("keep_displacements", C.c_int32), ("profile_kernels", C.c_int32),
         ("mixed_matvec", C.c_int32), ("inner_precond", C.c_int32),
         ("tensor_estimator", C.c_int32), ("chunk_domains", C.c_int32), ("graph_chunks", C.c_int32),
-        ("tc_wait_spins", C.c_int32), ("device_mesher", C.c_int32),
+        ("tc_wait_spins", C.c_int32), ("device_mesher", C.c_int32), ("macro_order", C.c_int32),
     ]
 
 
@@ -42,6 +42,11 @@ class DomainIn(C.Structure):
         ("delta", C.c_double * 3), ("phdsize", C.c_double * 3),
         ("E", C.c_double), ("nu", C.c_double), ("rve_strain", C.c_double),
     ]
+
+
+class Macro2Out(C.Structure):
+    _fields_ = [("iters", C.c_int64 * 60), ("relres", C.c_double * 60), ("ff", C.c_double * 3600),
+                ("kmacro", C.c_double * 3600)]
 
 
 class DomainOut(C.Structure):
@@ -57,6 +62,7 @@ class DomainOut(C.Structure):
         ("cr2_ee", C.c_double * 36), ("cr2_crit", C.c_double),
         ("cr1_iters", C.c_int32), ("cr2_iters", C.c_int32), ("density", C.c_double),
         ("displ", C.POINTER(C.c_double)), ("force", C.POINTER(C.c_double)),
+        ("macro2", C.POINTER(Macro2Out)),
     ]
 
 
@@ -88,6 +94,7 @@ class MeshOut(C.Structure):
         ("cap_elems", C.c_int64), ("cap_nodes", C.c_int64),
         ("elems", C.POINTER(C.c_int64)), ("nodes", C.POINTER(C.c_double)),
         ("bnode_ids", C.POINTER(C.c_int64)), ("bnode_vals", C.POINTER(C.c_double)),
+        ("macro_order", C.c_int32), ("pad_", C.c_int32),
     ]
 
 

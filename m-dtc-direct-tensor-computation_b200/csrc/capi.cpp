@@ -64,34 +64,37 @@ void plan_all(const dtc_domain_in* in, int64_t n, MeshPlan* plans, bool numberin
 
 // The last element kept only by the compaction quirk contributes its 3x3 diagonal block at
 // its surviving node; that node is decoupled, so its displacement is the prescribed value
-// on the boundary and 0 inside, and its reaction Ke_ll * u enters ff like any other node.
-void quirk_correction(const dtc_domain_in& in, const MeshPlan& mp, double nu, dtc_domain_out* o) {
+// on the boundary and 0 inside, and its reaction Ke_ll * u enters ff like any other node
+// (projected on the 8 or 20 macro shape functions of the macro order).
+void quirk_correction(const dtc_domain_in& in, const MeshPlan& mp, double nu, int order, dtc_domain_out* o) {
   if (!mp.last_partial || !mp.last_on_boundary) return;
   const int nen = mp.nen, nd = 3 * nen;
-  std::vector<double> kh(nd * nd);
+  const int nm = macro_nodes(order), nl = macro_loadcases(order);
+  std::vector<double> kh(nd * nd), uu((size_t)nm * 3 * nl);
   voxel_stiffness(nen, nu, kh.data());
   const double a = in.phdsize[0] * in.delta[0];
   const double E = in.E_voxel ? (double)in.E_voxel[mp.last_voxel] : in.E;
   const double s = E * a;
-  double x[3], lo[3], hi[3], xi[3], N[8], uu[8 * 3 * 24];
+  double x[3], lo[3], hi[3], xi[3], N[20];
   grid_coordinate(in, nen, mp.last_grid, x);
   for (int d = 0; d < 3; ++d) {
     lo[d] = (double)(in.xa_n[d] - 1) * in.delta[d];
     hi[d] = (double)(in.xa_n[d] + in.L[d] - 1) * in.delta[d];
   }
   geom_to_xi(x, lo, hi, xi);
-  macro_shape8(xi, N);
-  macro_modes(1e-6, uu);
+  macro_shape(order, xi, N);
+  macro_modes_of_order(order, 1e-6, uu.data());
+  double* ff = order == 2 ? o->macro2->ff : o->ff;
   const int ln = mp.last_local;
-  for (int lc = 0; lc < 24; ++lc) {
+  for (int lc = 0; lc < nl; ++lc) {
     double g[3], F[3];
-    for (int c = 0; c < 3; ++c) g[c] = boundary_value(uu, N, c, lc);
+    for (int c = 0; c < 3; ++c) g[c] = boundary_value_n(nm, uu.data(), N, c, lc);
     for (int c = 0; c < 3; ++c) {
       F[c] = 0.0;
       for (int cj = 0; cj < 3; ++cj) F[c] += s * kh[(3 * ln + c) + nd * (3 * ln + cj)] * g[cj];
     }
     for (int k = 0; k < 3; ++k)
-      for (int l = 0; l < 8; ++l) o->ff[(k * 8 + l) + 24 * lc] += F[k] * N[l];
+      for (int l = 0; l < nm; ++l) ff[(k * nm + l) + nl * lc] += F[k] * N[l];
     if (o->displ || o->force) {
       const int64_t id = mp.nn - 1;  // the last node keeps the last id
       for (int c = 0; c < 3; ++c) {
@@ -143,8 +146,12 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
     return DTC_ERR_INVALID_ARGUMENT;
   if (o.inner_precond < 0 || o.inner_precond > 2 || o.mixed_matvec < 0 || o.mixed_matvec > 2 ||
       o.tensor_estimator < 0 || o.tensor_estimator > 1 || o.chunk_domains < 0 || o.graph_chunks < 0 ||
-      o.graph_chunks > 1 || o.device_mesher < 0 || o.device_mesher > 1)
+      o.graph_chunks > 1 || o.device_mesher < 0 || o.device_mesher > 1 || o.macro_order < 0 || o.macro_order > 2)
     return DTC_ERR_INVALID_ARGUMENT;
+  if (o.macro_order == 0) o.macro_order = 1;
+  // macro order 2: the reaction projection of the reference (the energy products would couple
+  // the three column passes) and no adjoint (it is derived for the 24 linear load cases)
+  if (o.macro_order == 2 && (o.tensor_estimator != 0 || o.keep_displacements != 0)) return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
   h->opt = o;
@@ -179,14 +186,18 @@ dtc_status fill_mesh_out(const dtc_domain_in* in, const MeshPlan& mp, dtc_mesh_o
     if (out->cap_elems < mp.ne) return DTC_ERR_INVALID_ARGUMENT;
     std::memcpy(out->elems, mp.elems.data(), sizeof(int64_t) * mp.elems.size());
   }
+  if (out->macro_order < 0 || out->macro_order > 2) return DTC_ERR_INVALID_ARGUMENT;
   if (out->nodes || out->bnode_ids || out->bnode_vals) {
     if (out->cap_nodes < mp.nn) return DTC_ERR_INVALID_ARGUMENT;
-    double lo[3], hi[3], uu[8 * 3 * 24];
+    const int order = out->macro_order == 2 ? 2 : 1;
+    const int nm = macro_nodes(order), nl = macro_loadcases(order);
+    double lo[3], hi[3];
+    std::vector<double> uu((size_t)nm * 3 * nl);
     for (int d = 0; d < 3; ++d) {
       lo[d] = (double)(in->xa_n[d] - 1) * in->delta[d];
       hi[d] = (double)(in->xa_n[d] + in->L[d] - 1) * in->delta[d];
     }
-    macro_modes(1e-6, uu);
+    macro_modes_of_order(order, 1e-6, uu.data());
     int64_t b = 0;
     for (int64_t id = 0; id < mp.nn; ++id) {
       double x[3];
@@ -195,11 +206,12 @@ dtc_status fill_mesh_out(const dtc_domain_in* in, const MeshPlan& mp, dtc_mesh_o
       if (!grid_on_boundary(in->L, nen, mp.node_grid[id])) continue;
       if (out->bnode_ids) out->bnode_ids[b] = id + 1;
       if (out->bnode_vals) {
-        double xi[3], N[8];
+        double xi[3], N[20];
         geom_to_xi(x, lo, hi, xi);
-        macro_shape8(xi, N);
+        macro_shape(order, xi, N);
         for (int c = 0; c < 3; ++c)
-          for (int lc = 0; lc < 24; ++lc) out->bnode_vals[lc + 24 * (3 * b + c)] = boundary_value(uu, N, c, lc);
+          for (int lc = 0; lc < nl; ++lc)
+            out->bnode_vals[lc + nl * (3 * b + c)] = boundary_value_n(nm, uu.data(), N, c, lc);
       }
       ++b;
     }
@@ -254,7 +266,12 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     if (validate_domain(in[i], msg)) { h->err = "domain " + std::to_string(i) + ": " + msg; return DTC_ERR_INVALID_ARGUMENT; }
     if (in[i].nu != in[0].nu) { h->err = "all domains of one call must share nu"; return DTC_ERR_INVALID_ARGUMENT; }
     if (in[i].elem_type != in[0].elem_type) { h->err = "all domains of one call must share elem_type"; return DTC_ERR_INVALID_ARGUMENT; }
+    if (h->opt.macro_order == 2 && !out[i].macro2) {
+      h->err = "domain " + std::to_string(i) + ": macro order 2 needs dtc_domain_out.macro2";
+      return DTC_ERR_INVALID_ARGUMENT;
+    }
   }
+  const int order = h->opt.macro_order;
   std::vector<MeshPlan> plans((size_t)n);
   bool want_fields = false;
   for (int64_t i = 0; i < n; ++i) want_fields = want_fields || out[i].displ || out[i].force;
@@ -307,8 +324,10 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
       dtc_domain_out* o = &out[i];
       double* keep_d = o->displ;
       double* keep_f = o->force;
+      dtc_macro2_out* keep_m = o->macro2;
       std::memset(o, 0, sizeof(*o));
-      o->displ = keep_d; o->force = keep_f;
+      o->displ = keep_d; o->force = keep_f; o->macro2 = keep_m;
+      if (order == 2) std::memset(o->macro2, 0, sizeof(*o->macro2));
       o->domain_number = in[i].domain_number;
       o->status = plans[i].status;
       o->ne = plans[i].ne; o->nn = plans[i].nn; o->nb = plans[i].nb;
@@ -376,8 +395,8 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
   std::vector<const double*> ees;
   std::vector<dtc_domain_out*> rot_out;
   for (DomainTask& t : tasks) {
-    quirk_correction(*t.in, *t.plan, in[0].nu, t.out);
-    homogenise(t.out->ff, t.in->L, t.in->delta, t.in->rve_strain, t.out);
+    quirk_correction(*t.in, *t.plan, in[0].nu, order, t.out);
+    homogenise(order, order == 2 ? t.out->macro2->ff : t.out->ff, t.in->L, t.in->delta, t.in->rve_strain, t.out);
     t.out->density = (double)t.plan->ne / ((double)t.in->L[0] * (double)t.in->L[1] * (double)t.in->L[2]);
     bool finite = true;
     for (int q = 0; q < 36; ++q) finite = finite && std::isfinite(t.out->ee[q]);

@@ -201,6 +201,110 @@ double boundary_value(const double* uu, const double N[8], int c, int lc) {
   return s;
 }
 
+void macro_shape20(const double xi[3], double N[20]) {
+  // ANSYS 20-node brick as phi_NN_hexe20 writes it: corners 1-8, then the mid-edge nodes of
+  // the bottom ring (9-12), the top ring (13-16) and the vertical edges (17-20); every product
+  // is evaluated left to right as there
+  const double f = 1.0 / 8.0, q = 1.0 / 4.0, e = 1.0, z = 2.0;
+  const double x = xi[0], y = xi[1], w = xi[2];
+  N[0] = f * (e - x) * (e - y) * (e - w) * (-x - y - w - z);
+  N[1] = f * (e + x) * (e - y) * (e - w) * (x - y - w - z);
+  N[2] = f * (e + x) * (e + y) * (e - w) * (x + y - w - z);
+  N[3] = f * (e - x) * (e + y) * (e - w) * (-x + y - w - z);
+  N[4] = f * (e - x) * (e - y) * (e + w) * (-x - y + w - z);
+  N[5] = f * (e + x) * (e - y) * (e + w) * (x - y + w - z);
+  N[6] = f * (e + x) * (e + y) * (e + w) * (x + y + w - z);
+  N[7] = f * (e - x) * (e + y) * (e + w) * (-x + y + w - z);
+  N[8] = q * (e - x * x) * (e - y) * (e - w);
+  N[9] = q * (e + x) * (e - y * y) * (e - w);
+  N[10] = q * (e - x * x) * (e + y) * (e - w);
+  N[11] = q * (e - x) * (e - y * y) * (e - w);
+  N[12] = q * (e - x * x) * (e - y) * (e + w);
+  N[13] = q * (e + x) * (e - y * y) * (e + w);
+  N[14] = q * (e - x * x) * (e + y) * (e + w);
+  N[15] = q * (e - x) * (e - y * y) * (e + w);
+  N[16] = q * (e - x) * (e - y) * (e - w * w);
+  N[17] = q * (e + x) * (e - y) * (e - w * w);
+  N[18] = q * (e + x) * (e + y) * (e - w * w);
+  N[19] = q * (e - x) * (e + y) * (e - w * w);
+}
+
+namespace {
+// Nonzero entries of init_displ_hexe20 (mod_write_deck.f90:118-279) as (load case, component,
+// macro node, multiple of eps), all 1-based.  Four entries are written there with default-kind
+// (single precision) literals (`.9*eps`, `-.7*eps`): their multiples are those float values.
+struct ModeEntry { signed char lc, comp, node; double mult; };
+constexpr double F09 = (double)0.9f, F07 = (double)0.7f;
+const ModeEntry kModes20[] = {
+    {1, 1, 2, 1.0}, {1, 1, 3, 1.0}, {1, 1, 6, 1.0}, {1, 1, 7, 1.0}, {1, 1, 9, 0.5}, {1, 1, 10, 1.0},
+    {1, 1, 11, 0.5}, {1, 1, 13, 0.5}, {1, 1, 14, 1.0}, {1, 1, 15, 0.5}, {1, 1, 18, 1.0}, {1, 1, 19, 1.0},
+    {2, 2, 3, 1.0}, {2, 2, 4, 1.0}, {2, 2, 7, 1.0}, {2, 2, 8, 1.0}, {2, 2, 10, 0.5}, {2, 2, 11, 1.0},
+    {2, 2, 12, 0.5}, {2, 2, 14, 0.5}, {2, 2, 15, 1.0}, {2, 2, 16, 0.5}, {2, 2, 19, 1.0}, {2, 2, 20, 1.0},
+    {3, 3, 5, 1.0}, {3, 3, 6, 1.0}, {3, 3, 7, 1.0}, {3, 3, 8, 1.0}, {3, 3, 13, 1.0}, {3, 3, 14, 1.0},
+    {3, 3, 15, 1.0}, {3, 3, 16, 1.0}, {3, 3, 17, 0.5}, {3, 3, 18, 0.5}, {3, 3, 19, 0.5}, {3, 3, 20, 0.5},
+    {4, 1, 1, 1.0}, {4, 1, 2, 1.0}, {4, 1, 5, 1.0}, {4, 1, 6, 1.0}, {4, 1, 9, 1.0}, {4, 1, 10, 0.5},
+    {4, 1, 12, 0.5}, {4, 1, 13, 1.0}, {4, 1, 14, 0.5}, {4, 1, 16, 0.5}, {4, 1, 17, 1.0}, {4, 1, 18, 1.0},
+    {5, 1, 1, 1.0}, {5, 1, 2, 1.0}, {5, 1, 3, 1.0}, {5, 1, 4, 1.0}, {5, 1, 9, 1.0}, {5, 1, 10, 1.0},
+    {5, 1, 11, 1.0}, {5, 1, 12, 1.0}, {5, 1, 17, 0.5}, {5, 1, 18, 0.5}, {5, 1, 19, 0.5}, {5, 1, 20, 0.5},
+    {6, 2, 5, 1.0}, {6, 2, 6, 1.0}, {6, 2, 7, 1.0}, {6, 2, 8, 1.0}, {6, 2, 13, 1.0}, {6, 2, 14, 1.0},
+    {6, 2, 15, 1.0}, {6, 2, 16, 1.0}, {6, 2, 17, 0.5}, {6, 2, 18, 0.5}, {6, 2, 19, 0.5}, {6, 2, 20, 0.5},
+    {7, 1, 8, 1.0}, {7, 1, 15, 0.5}, {7, 1, 20, 0.5}, {8, 2, 1, -2.0}, {8, 2, 9, 0.5}, {8, 2, 17, 0.5},
+    {9, 2, 2, -1.0}, {9, 2, 9, 0.5}, {9, 2, 18, 0.5}, {10, 3, 1, -1.0}, {10, 3, 9, 0.5}, {10, 3, 12, 0.1},
+    {10, 3, 17, 0.5}, {11, 3, 2, -2.0}, {11, 3, 10, 0.5}, {11, 3, 18, 0.5}, {12, 3, 11, 0.1}, {12, 3, 19, F09},
+    {13, 3, 20, 5.0}, {14, 1, 4, 0.2}, {14, 1, 12, 0.5}, {14, 1, 20, 5.0}, {15, 1, 5, 1.0}, {15, 1, 13, 0.5},
+    {16, 1, 6, 5.0}, {16, 1, 18, 0.2}, {17, 1, 14, 0.5}, {17, 1, 19, 0.3}, {18, 1, 15, 0.1}, {18, 1, 20, 0.1},
+    {18, 3, 6, -F07}, {18, 3, 13, -0.1}, {18, 3, 14, -1.0}, {19, 2, 9, 0.5}, {19, 2, 12, 0.5}, {19, 2, 17, 0.5},
+    {19, 3, 7, -3.0}, {19, 3, 14, -1.5}, {19, 3, 19, -1.5}, {20, 2, 16, 0.1}, {20, 3, 8, -3.0}, {20, 3, 15, -0.1},
+    {21, 2, 3, 5.0}, {21, 2, 10, 0.5}, {21, 2, 19, 0.5}, {22, 2, 11, 5.0}, {22, 2, 20, 0.5}, {23, 2, 16, 2.0},
+    {24, 2, 13, 5.0}, {24, 2, 19, -0.5}, {25, 3, 9, 2.0}, {26, 3, 10, 5.0}, {27, 2, 11, -0.1}, {27, 3, 11, 1.0},
+    {28, 3, 12, 4.0}, {29, 2, 13, 0.1}, {29, 3, 13, -4.0}, {30, 1, 14, -0.1}, {30, 3, 6, 2.0}, {31, 2, 15, -0.1},
+    {31, 3, 3, 5.0}, {32, 3, 16, -0.5}, {33, 1, 6, 0.1}, {33, 1, 17, -1.0}, {34, 2, 18, -4.0}, {35, 2, 19, -1.0},
+    {36, 2, 20, 2.0}, {37, 1, 1, 3.0}, {38, 2, 2, -5.0}, {39, 1, 3, -3.0}, {40, 2, 4, -2.0}, {41, 1, 5, 5.0},
+    {42, 2, 6, 3.0}, {43, 1, 7, -4.0}, {44, 2, 8, 4.0}, {45, 2, 17, 2.0}, {46, 3, 4, -2.0}, {46, 3, 14, -1.5},
+    {47, 1, 18, -1.0}, {47, 1, 19, -1.0}, {47, 1, 20, 2.0}, {48, 3, 15, -1.0}, {49, 1, 10, -F09}, {49, 1, 14, -F07},
+    {49, 1, 16, 1.0}, {50, 2, 15, 1.0}, {51, 1, 9, 1.0}, {52, 2, 10, 3.0}, {53, 1, 11, -1.0}, {54, 2, 12, 5.0},
+    {55, 1, 4, -1.5}, {56, 2, 14, -5.0}, {57, 1, 15, -1.0}, {58, 1, 16, -1.0}, {59, 3, 17, 1.0}, {60, 3, 18, -1.0}};
+}  // namespace
+
+void macro_modes20(double eps, double* uu) {
+  std::fill(uu, uu + 20 * 3 * 60, 0.0);
+  for (const ModeEntry& m : kModes20) uu[(m.node - 1) + 20 * (m.comp - 1) + 60 * (m.lc - 1)] = m.mult * eps;
+}
+
+void macro_shape(int order, const double xi[3], double* N) {
+  if (order == 2) macro_shape20(xi, N);
+  else macro_shape8(xi, N);
+}
+
+void macro_modes_of_order(int order, double eps, double* uu) {
+  if (order == 2) macro_modes20(eps, uu);
+  else macro_modes(eps, uu);
+}
+
+double boundary_value_n(int nm, const double* uu, const double* N, int c, int lc) {
+  double s = 0.0;
+  for (int l = 0; l < nm; ++l) s += N[l] * uu[l + nm * c + 3 * nm * lc];
+  return s;
+}
+
+void loadcase_matrix(int order, double e, double* vv) {
+  const int nm = macro_nodes(order), nl = 3 * nm;
+  std::vector<double> uu((size_t)nm * 3 * nl);
+  macro_modes_of_order(order, e, uu.data());
+  // vv(r, lc) = uu(l, k, lc), r = (k-1)*nm + l: the load-case matrix is the boundary-mode table
+  // flattened component-major (exact for init_loadcase_el_order_lin, mod_struct_calcmat.f90:
+  // 1684-1770, and for every well-formed entry of init_loadcase_el_order_quad, :1780-2028)
+  for (int lc = 0; lc < nl; ++lc)
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < nm; ++l) vv[(nm * k + l) + nl * lc] = uu[l + nm * k + nl * lc];
+  if (order == 2) {
+    // the two entries the quadratic table writes as 0.9_rk*e where the boundary modes use the
+    // single-precision .9*eps: rows 10 and 59 of load cases 49 and 12
+    vv[9 + nl * 48] = -0.9 * e;
+    vv[58 + nl * 11] = 0.9 * e;
+  }
+}
+
 double symmetry_deviation(int n, const double* a) {
   double d = 0.0, m = 0.0;
   for (int j = 0; j < n; ++j)
@@ -211,28 +315,44 @@ double symmetry_deviation(int n, const double* a) {
   return m > 0.0 ? d / m : 0.0;
 }
 
-void homogenise(const double ff[576], const int64_t L[3], const double delta[3], double rve_strain,
+void homogenise(int order, const double* ff, const int64_t L[3], const double delta[3], double rve_strain,
                 dtc_domain_out* out) {
-  std::memcpy(out->ff, ff, sizeof(double) * 576);
-  // vv(r, lc) = uu(l, k, lc), r = (k-1)*8 + l (mod_struct_calcmat.f90:1684-1770)
-  double uu[8 * 3 * 24], vv[576];
-  macro_modes(rve_strain, uu);
-  for (int lc = 0; lc < 24; ++lc)
-    for (int k = 0; k < 3; ++k)
-      for (int l = 0; l < 8; ++l) vv[(8 * k + l) + 24 * lc] = uu[l + 8 * k + 24 * lc];
-  gauss_jordan_inverse(24, vv);
-  matmul(24, 24, 24, ff, vv, out->kmacro);
-  out->sym_k = symmetry_deviation(24, out->kmacro);
+  const int nl = macro_loadcases(order);
+  double* ff_out = order == 2 ? out->macro2->ff : out->ff;
+  double* km = order == 2 ? out->macro2->kmacro : out->kmacro;
+  if (ff_out != ff) std::memcpy(ff_out, ff, sizeof(double) * nl * nl);
+  std::vector<double> vv((size_t)nl * nl);
+  loadcase_matrix(order, rve_strain, vv.data());
+  gauss_jordan_inverse(nl, vv.data());
+  matmul(nl, nl, nl, ff, vv.data(), km);
+  out->sym_k = symmetry_deviation(nl, km);
   const double X = (double)L[0] * delta[0], Y = (double)L[1] * delta[1], Z = (double)L[2] * delta[2];
-  auto f = [&](int r, int c) { return ff[(r - 1) + 24 * c]; };  // r 1-based, c 0-based
+  auto f = [&](int r, int c) { return ff[(r - 1) + nl * c]; };  // r 1-based, c 0-based
   double fv[36];
-  for (int c = 0; c < 6; ++c) {  // mod_struct_calcmat.f90:345-359
-    fv[0 + 6 * c] = (f(2, c) + f(3, c) + f(6, c) + f(7, c)) / (Y * Z);
-    fv[1 + 6 * c] = (f(11, c) + f(12, c) + f(15, c) + f(16, c)) / (X * Z);
-    fv[2 + 6 * c] = (f(21, c) + f(22, c) + f(23, c) + f(24, c)) / (X * Y);
-    fv[3 + 6 * c] = 0.5 * ((f(3, c) + f(4, c) + f(7, c) + f(8, c)) / (X * Z) + (f(10, c) + f(11, c) + f(14, c) + f(15, c)) / (Y * Z));
-    fv[4 + 6 * c] = 0.5 * ((f(5, c) + f(6, c) + f(7, c) + f(8, c)) / (X * Y) + (f(18, c) + f(19, c) + f(22, c) + f(23, c)) / (Y * Z));
-    fv[5 + 6 * c] = 0.5 * ((f(13, c) + f(14, c) + f(15, c) + f(16, c)) / (X * Y) + (f(19, c) + f(20, c) + f(23, c) + f(24, c)) / (X * Z));
+  if (order == 2) {
+    for (int c = 0; c < 6; ++c) {  // mod_struct_calcmat.f90:368-401: the 8 nodes of each face
+      fv[0 + 6 * c] = (f(2, c) + f(3, c) + f(6, c) + f(7, c) + f(10, c) + f(14, c) + f(18, c) + f(19, c)) / (Y * Z);
+      fv[1 + 6 * c] = (f(23, c) + f(24, c) + f(27, c) + f(28, c) + f(31, c) + f(35, c) + f(39, c) + f(40, c)) / (X * Z);
+      fv[2 + 6 * c] = (f(45, c) + f(46, c) + f(47, c) + f(48, c) + f(53, c) + f(54, c) + f(55, c) + f(56, c)) / (X * Y);
+      fv[3 + 6 * c] =
+          0.5 * ((f(3, c) + f(4, c) + f(7, c) + f(8, c) + f(11, c) + f(15, c) + f(19, c) + f(20, c)) / (X * Z) +
+                 (f(22, c) + f(23, c) + f(26, c) + f(27, c) + f(30, c) + f(34, c) + f(38, c) + f(39, c)) / (Y * Z));
+      fv[4 + 6 * c] =
+          0.5 * ((f(5, c) + f(6, c) + f(7, c) + f(8, c) + f(13, c) + f(14, c) + f(15, c) + f(16, c)) / (X * Y) +
+                 (f(42, c) + f(43, c) + f(46, c) + f(47, c) + f(50, c) + f(54, c) + f(58, c) + f(59, c)) / (Y * Z));
+      fv[5 + 6 * c] =
+          0.5 * ((f(25, c) + f(26, c) + f(27, c) + f(28, c) + f(33, c) + f(34, c) + f(35, c) + f(36, c)) / (X * Y) +
+                 (f(43, c) + f(44, c) + f(47, c) + f(48, c) + f(51, c) + f(55, c) + f(59, c) + f(60, c)) / (X * Z));
+    }
+  } else {
+    for (int c = 0; c < 6; ++c) {  // mod_struct_calcmat.f90:345-359
+      fv[0 + 6 * c] = (f(2, c) + f(3, c) + f(6, c) + f(7, c)) / (Y * Z);
+      fv[1 + 6 * c] = (f(11, c) + f(12, c) + f(15, c) + f(16, c)) / (X * Z);
+      fv[2 + 6 * c] = (f(21, c) + f(22, c) + f(23, c) + f(24, c)) / (X * Y);
+      fv[3 + 6 * c] = 0.5 * ((f(3, c) + f(4, c) + f(7, c) + f(8, c)) / (X * Z) + (f(10, c) + f(11, c) + f(14, c) + f(15, c)) / (Y * Z));
+      fv[4 + 6 * c] = 0.5 * ((f(5, c) + f(6, c) + f(7, c) + f(8, c)) / (X * Y) + (f(18, c) + f(19, c) + f(22, c) + f(23, c)) / (Y * Z));
+      fv[5 + 6 * c] = 0.5 * ((f(13, c) + f(14, c) + f(15, c) + f(16, c)) / (X * Y) + (f(19, c) + f(20, c) + f(23, c) + f(24, c)) / (X * Z));
+    }
   }
   // C = fv * meps, meps = diag(1e6, 1e6, 1e6, -1e6, -1e6, 1e6) (:434-439)
   const double meps[6] = {1e6, 1e6, 1e6, -1e6, -1e6, 1e6};

@@ -23,9 +23,34 @@ void macro_modes(double eps, double* uu);
 // Boundary value of load case lc, component c at a point with shape values N.
 double boundary_value(const double* uu, const double N[8], int c, int lc);
 
-// Homogenisation from the domain forces ff (mod_struct_calcmat.f90:216-500):
-// K_macro = ff * vv^-1, fv from the face sums, C = fv * meps, EE = (C + C^T)/2.
-void homogenise(const double ff[576], const int64_t L[3], const double delta[3], double rve_strain,
+// The macro element: order 1 = 8-node trilinear brick with 24 load cases, order 2 = 20-node
+// serendipity brick with 60 load cases ('Element order on macro scale',
+// f-src/mod_dtc_main_subroutines.f90:498-508).
+inline int macro_nodes(int order) { return order == 2 ? 20 : 8; }
+inline int macro_loadcases(int order) { return order == 2 ? 60 : 24; }
+
+// Quadratic macro shape functions N_1..N_20 in ANSYS node order (phi_NN_hexe20,
+// mod_linfe.f90:827-888) and the boundary modes uu(20,3,60) of init_displ_hexe20
+// (mod_write_deck.f90:118-279), column-major.
+void macro_shape20(const double xi[3], double N[20]);
+void macro_modes20(double eps, double* uu);
+
+// Either order: N (8 or 20 values), uu(nm,3,nl), and the value of load case lc, component c.
+void macro_shape(int order, const double xi[3], double* N);
+void macro_modes_of_order(int order, double eps, double* uu);
+double boundary_value_n(int nm, const double* uu, const double* N, int c, int lc);
+
+// Load-case matrix vv(nl,nl) for eps = e (init_loadcase_el_order_lin / _quad,
+// mod_struct_calcmat.f90:1684-2028): the boundary-mode table flattened component-major.  For
+// order 2 this is the quadratic table of the reference with its typing defects repaired (a row
+// labelled 59 that belongs at 49, 22 entries written without the factor e, one surplus
+// value in row 54); every other entry of that table is reproduced exactly.
+void loadcase_matrix(int order, double e, double* vv);
+
+// Homogenisation from the domain forces ff (nl x nl, mod_struct_calcmat.f90:216-500):
+// K_macro = ff * vv^-1, fv from the face sums (:345-359 order 1, :368-401 order 2),
+// C = fv * meps, EE = (C + C^T)/2.  Order 2 writes ff and K_macro to out->macro2.
+void homogenise(int order, const double* ff, const int64_t L[3], const double delta[3], double rve_strain,
                 dtc_domain_out* out);
 
 // Domain forces from the energy products M(a,b) = u_a^T K u_b of the 24 load-case solutions:

@@ -34,7 +34,10 @@ namespace dtc {
 
 __constant__ double c_khat64[576];   // unit voxel stiffness, column-major (symmetric)
 __constant__ float c_khat32[576];
-__constant__ double c_uu[8 * 3 * kNLC];  // macro modes uu(8,3,24) for eps = 1e-6
+// the 24 load-case columns of the current column pass of the macro modes for eps = 1e-6:
+// uu(nm,3,24) column-major, nm = 8 (macro order 1) or 20 (macro order 2); columns past the
+// last load case are zero
+__constant__ double c_uu[20 * 3 * kNLC];
 __constant__ double c_k20_64[3600];       // unit HEX20 element matrix (ring node order)
 
 template <typename T> struct KhatC;
@@ -387,6 +390,41 @@ __device__ __forceinline__ void shape8(const double xi[3], double N[8]) {
   N[4] = g1x * g1y * g2z; N[5] = g2x * g1y * g2z; N[6] = g2x * g2y * g2z; N[7] = g1x * g2y * g2z;
 }
 
+// ANSYS 20-node macro shape functions, as the host's macro_shape20 (phi_NN_hexe20,
+// mod_linfe.f90:827-888)
+__device__ __forceinline__ void shape20(const double xi[3], double N[20]) {
+  const double f = 1.0 / 8.0, q = 1.0 / 4.0, e = 1.0, z = 2.0;
+  const double x = xi[0], y = xi[1], w = xi[2];
+  N[0] = f * (e - x) * (e - y) * (e - w) * (-x - y - w - z);
+  N[1] = f * (e + x) * (e - y) * (e - w) * (x - y - w - z);
+  N[2] = f * (e + x) * (e + y) * (e - w) * (x + y - w - z);
+  N[3] = f * (e - x) * (e + y) * (e - w) * (-x + y - w - z);
+  N[4] = f * (e - x) * (e - y) * (e + w) * (-x - y + w - z);
+  N[5] = f * (e + x) * (e - y) * (e + w) * (x - y + w - z);
+  N[6] = f * (e + x) * (e + y) * (e + w) * (x + y + w - z);
+  N[7] = f * (e - x) * (e + y) * (e + w) * (-x + y + w - z);
+  N[8] = q * (e - x * x) * (e - y) * (e - w);
+  N[9] = q * (e + x) * (e - y * y) * (e - w);
+  N[10] = q * (e - x * x) * (e + y) * (e - w);
+  N[11] = q * (e - x) * (e - y * y) * (e - w);
+  N[12] = q * (e - x * x) * (e - y) * (e + w);
+  N[13] = q * (e + x) * (e - y * y) * (e + w);
+  N[14] = q * (e - x * x) * (e + y) * (e + w);
+  N[15] = q * (e - x) * (e - y * y) * (e + w);
+  N[16] = q * (e - x) * (e - y) * (e - w * w);
+  N[17] = q * (e + x) * (e - y) * (e - w * w);
+  N[18] = q * (e + x) * (e + y) * (e - w * w);
+  N[19] = q * (e - x) * (e + y) * (e - w * w);
+}
+template <int NM>
+__device__ __forceinline__ void macro_shape_dev(const double xi[3], double (&N)[NM]) {
+  if constexpr (NM == 20) shape20(xi, N);
+  else shape8(xi, N);
+}
+
+// Prescribed values of the current column pass on the domain-box nodes: component c of load
+// case lc is sum_l N_l(xi(x)) uu(l, c, lc) (determine_prescribed_displ, mod_write_deck.f90:22-51).
+template <int NM>
 __global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __restrict__ tiles,
                                                               const DomDev* __restrict__ doms,
                                                               const uint8_t* __restrict__ flags,
@@ -399,13 +437,13 @@ __global__ void __launch_bounds__(kThreads) k_boundary_values(const Tile* __rest
   const int64_t n = node_index(D, x, y, z);
   const uint8_t f = flags[n];
   if (!(f & kNodeActive) || !(f & kNodeBoundary)) return;
-  double xi[3], N[8];
+  double xi[3], N[NM];
   node_xi(D, x, y, z, xi);
-  shape8(xi, N);
+  macro_shape_dev<NM>(xi, N);
   for (int c = 0; c < 3; ++c)
     for (int lc = 0; lc < kNLC; ++lc) {
       double s = 0.0;
-      for (int l = 0; l < 8; ++l) s += N[l] * c_uu[l + 8 * c + 24 * lc];
+      for (int l = 0; l < NM; ++l) s += N[l] * c_uu[l + NM * c + 3 * NM * lc];
       X[vec_index(n, c, lc)] = s;
     }
 }
@@ -744,45 +782,56 @@ __global__ void k_add_inner_its(ColState* __restrict__ ost, const ColState* __re
 
 // -------------------------------------------------------------------------------------
 // Projection of the reaction forces on the macro shape functions
-// (mod_struct_calcmat.f90:246-280): ff((k-1)*8+l, lc) += F(k, n) * N_l(xi(x_n)), all nodes.
+// (mod_struct_calcmat.f90:246-280): ff((k-1)*NM+l, lc) += F(k, n) * N_l(xi(x_n)), all nodes,
+// for the 24 load cases of one column pass; ff is nl x nl per domain (nl = 3 NM) and the
+// pass covers columns col0 .. col0+23 (those below nl).
+template <int NM>
 __global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                      const uint8_t* __restrict__ flags, const double* __restrict__ F,
-                                                     double* __restrict__ ff) {
-  __shared__ double part[16][8][25];
+                                                     double* __restrict__ ff, int col0) {
+  constexpr int NR = 3 * NM;
+  __shared__ double part[4][8][NR + 1];
   const Tile t = tiles[blockIdx.x / 3];
   const DomDev D = doms[t.dom];
   const int lcl = threadIdx.x & 7, lc = (blockIdx.x % 3) * kLcGroup + lcl;
   const int row = threadIdx.x >> 3;
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
-  double acc[24];
+  double acc[NR];
 #pragma unroll
-  for (int k = 0; k < 24; ++k) acc[k] = 0.0;
+  for (int k = 0; k < NR; ++k) acc[k] = 0.0;
   if (yy < D.n[1] && zz < D.n[2]) {
     for (int i = 0; i < kTileX; ++i) {
       const int xx = t.x0 + i;
       if (xx >= D.n[0]) break;
       const int64_t n = node_index(D, xx, yy, zz);
       if (!(flags[n] & kNodeActive)) continue;
-      double xi[3], N[8];
+      double xi[3], N[NM];
       node_xi(D, xx, yy, zz, xi);
-      shape8(xi, N);
+      macro_shape_dev<NM>(xi, N);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const double f = F[vec_index(n, k, lc)];
 #pragma unroll
-        for (int l = 0; l < 8; ++l) acc[k * 8 + l] += f * N[l];
+        for (int l = 0; l < NM; ++l) acc[k * NM + l] += f * N[l];
       }
     }
   }
+  // the 4 rows of a warp that share a load case (lanes lcl, lcl + 8, + 16, + 24), then the warps
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-  for (int k = 0; k < 24; ++k) part[row][lcl][k] = acc[k];
+  for (int k = 0; k < NR; ++k) {
+    double v = acc[k];
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    if (lane < 8) part[warp][lane][k] = v;
+  }
   __syncthreads();
-  for (int j = threadIdx.x; j < 8 * 24; j += kThreads) {
-    const int l8 = j / 24, k = j % 24;
-    double s = 0.0;
-    for (int r2 = 0; r2 < 16; ++r2) s += part[r2][l8][k];
-    const int lcg = (blockIdx.x % 3) * kLcGroup + l8;
-    atomicAdd(ff + (int64_t)t.dom * 576 + k + 24 * lcg, s);
+  const int nl = NR;
+  for (int j = threadIdx.x; j < 8 * NR; j += kThreads) {
+    const int l8 = j / NR, k = j % NR;
+    const double s = part[0][l8][k] + part[1][l8][k] + part[2][l8][k] + part[3][l8][k];
+    const int col = col0 + (blockIdx.x % 3) * kLcGroup + l8;
+    if (col < nl) atomicAdd(ff + (int64_t)t.dom * nl * nl + k + (int64_t)nl * col, s);
   }
 }
 
@@ -2075,8 +2124,6 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     float kh32[576];
     voxel_stiffness(8, nu, kh);
     for (int i = 0; i < 576; ++i) kh32[i] = (float)kh[i];
-    double uu[8 * 3 * 24];
-    macro_modes(1e-6, uu);   // the hard-coded boundary eps (mod_write_deck.f90:61)
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat64, kh, sizeof(kh), 0, cudaMemcpyHostToDevice, s));
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32, kh32, sizeof(kh32), 0, cudaMemcpyHostToDevice, s));
     float2 khr[4 * 3 * 24];
@@ -2088,7 +2135,6 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
             khr[((2 * b + c) * 3 + r) * 24 + col] = make_float2(kh32[col * 24 + 3 * l0 + r], kh32[col * 24 + 3 * l1 + r]);
       }
     DTC_CUDA(cudaMemcpyToSymbolAsync(c_khat32r2, khr, sizeof(khr), 0, cudaMemcpyHostToDevice, s));
-    DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, uu, sizeof(uu), 0, cudaMemcpyHostToDevice, s));
     if (int e = upload_tc_operand(kh, s, msg)) return e;
     if (I.tensor_matvec || tune) {
       if (int e = set_tc_spin_limit(opt.tc_wait_spins, s, msg)) return e;
@@ -2172,7 +2218,11 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   if ((e = ensure(I, bAlphaF, sizeof(float) * ncol, msg))) return e;
   if ((e = ensure(I, bDomAct, sizeof(int) * ndom, msg))) return e;
   if ((e = ensure(I, bCount, sizeof(int), msg))) return e;
-  if ((e = ensure(I, bFf, sizeof(double) * 576 * ndom, msg))) return e;
+  // macro order 2 solves its 60 load cases as three column passes of 24 over the same batch
+  const int order = opt.macro_order == 2 ? 2 : 1;
+  const int nm = macro_nodes(order), nl = macro_loadcases(order);
+  const int ncp = (nl + kNLC - 1) / kNLC;
+  if ((e = ensure(I, bFf, sizeof(double) * nl * nl * ndom, msg))) return e;
   if ((e = ensure(I, bErr, sizeof(int), msg))) return e;
   DTC_CUDA(cudaMemsetAsync(I.bufs[bErr], 0, sizeof(int), s));
 
@@ -2194,7 +2244,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv32], 0, sizeof(float) * node_total * 3, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bX], 0, vbytes64, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bR64], 0, vbytes64, s));
-  DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * 576 * ndom, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * nl * nl * ndom, s));
   // device time of the solve, inputs resident: from here (voxel factors and work lists
   // uploaded) to the last kernel, measured with CUDA events on the solver stream
   if (!I.ev_solve[0]) {
@@ -2218,188 +2268,241 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemsetAsync(I.bufs[bBinv32], 0, sizeof(float) * node_total * 6, s));
     k_node_setup<NEN><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
                                                     B<float>(I, bDinv32), B<float>(I, bBinv32));
-    k_boundary_values<<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, fl, X);
-    L += 2;
+    ++L;
   }
   if ((e = launch_check(msg))) return e;
   const dim3 gi((unsigned)(3 * std::max<int64_t>(nti, 1))), ga((unsigned)(3 * std::max<int64_t>(nta, 1)));
   ColState* ost = B<ColState>(I, bOst);
-  if (!mixed) {
-    // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
-    DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
-    DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
-    apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
-    ++L;
-    if ((e = run_cg<double, false, NEN>(I, ndom, W, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
-                            opt.rtol, nullptr, opt.max_it, L, msg)))
+  const bool use_mg = mixed && opt.inner_precond == 2 && nti > 0;
+  MgPlan mgp;
+  MgDev mgd{};
+  if (use_mg) {   // multigrid hierarchy: built on the host from the voxel factors, set up on the device
+    if (hb.has_mg) {
+      mgp = std::move(hb.mg);
+    } else {
+      const auto tb = std::chrono::steady_clock::now();
+      build_mg(mgp, doms, svox, tiles_i, nu, NEN, opt.host_threads);
+      stats_.kc[kcHostMgBuild].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+      stats_.kc[kcHostMgBuild].launches += 1;
+    }
+    const int64_t cn = std::max<int64_t>(mgp.nodes, 1);
+    if ((e = ensure(I, bZ32, vbytes32, msg)) || (e = ensure(I, bT32, vbytes32, msg)) ||
+        (e = ensure(I, bMgDoms, sizeof(DomDev) * mgp.doms.size(), msg)) ||
+        (e = ensure(I, bMgTiles, sizeof(Tile) * std::max<size_t>(mgp.tiles.size(), 1), msg)) ||
+        (e = ensure(I, bMgSvox, sizeof(float) * std::max<size_t>(mgp.svox.size(), 1), msg)) ||
+        (e = ensure(I, bMgFlags, cn, msg)) || (e = ensure(I, bMgDinv64, sizeof(double) * 3 * cn, msg)) ||
+        (e = ensure(I, bMgDinv32, sizeof(float) * 3 * cn, msg)) ||
+        (e = ensure(I, bMgBinv32, sizeof(float) * 6 * cn, msg)) ||
+        (e = ensure(I, bMgB, sizeof(float) * 72 * cn, msg)) || (e = ensure(I, bMgT, sizeof(float) * 72 * cn, msg)) ||
+        (e = ensure(I, bMgZ, sizeof(float) * 72 * cn, msg)) ||
+        (e = ensure(I, bMgMinv, sizeof(float) * mgp.minv.size(), msg)) ||
+        (e = ensure(I, bMgList, sizeof(int) * std::max<size_t>(mgp.lists.size(), 1), msg)) ||
+        (e = ensure(I, bMgNodes, sizeof(int64_t) * std::max<size_t>(mgp.nodes_l.size(), 1), msg)))
       return e;
-    DTC_CUDA(cudaMemcpyAsync(ost, I.bufs[bSt], sizeof(ColState) * ncol, cudaMemcpyDeviceToDevice, s));
-  } else {
-    // every FP32 work vector starts at zero: the stencil reads boundary and void entries
-    DTC_CUDA(cudaMemsetAsync(I.bufs[bR32], 0, vbytes32, s));
-    DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
-    DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
-    // multigrid hierarchy (HEX08): built on the host from the voxel factors, set up on the device
-    const bool use_mg = opt.inner_precond == 2 && nti > 0;
-    MgPlan mgp;
-    MgDev mgd{};
-    if (use_mg) {
-      if (hb.has_mg) {
-        mgp = std::move(hb.mg);
-      } else {
-        const auto tb = std::chrono::steady_clock::now();
-        build_mg(mgp, doms, svox, tiles_i, nu, NEN, opt.host_threads);
-        stats_.kc[kcHostMgBuild].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
-        stats_.kc[kcHostMgBuild].launches += 1;
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgDoms], mgp.doms.data(), sizeof(DomDev) * mgp.doms.size(),
+                             cudaMemcpyHostToDevice, s));
+    if (!mgp.tiles.empty())
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgTiles], mgp.tiles.data(), sizeof(Tile) * mgp.tiles.size(),
+                               cudaMemcpyHostToDevice, s));
+    if (!mgp.svox.empty())
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgSvox], mgp.svox.data(), sizeof(float) * mgp.svox.size(),
+                               cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgMinv], mgp.minv.data(), sizeof(float) * mgp.minv.size(),
+                             cudaMemcpyHostToDevice, s));
+    if (!mgp.lists.empty())
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgList], mgp.lists.data(), sizeof(int) * mgp.lists.size(),
+                               cudaMemcpyHostToDevice, s));
+    if (!mgp.nodes_l.empty())
+      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgNodes], mgp.nodes_l.data(), sizeof(int64_t) * mgp.nodes_l.size(),
+                               cudaMemcpyHostToDevice, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bMgFlags], 0, cn, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bMgBinv32], 0, sizeof(float) * 6 * cn, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bMgB], 0, sizeof(float) * 72 * cn, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bMgT], 0, sizeof(float) * 72 * cn, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bMgZ], 0, sizeof(float) * 72 * cn, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
+    DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));
+    for (int l = 1; l < mgp.nlev; ++l)
+      if (mgp.all_n[l] > 0) {
+        k_node_setup<8><<<(unsigned)mgp.all_n[l], kThreads, 0, s>>>(
+            B<Tile>(I, bMgTiles) + mgp.all_off[l], B<DomDev>(I, bMgDoms) + (size_t)l * ndom, B<float>(I, bMgSvox),
+            B<uint8_t>(I, bMgFlags), B<double>(I, bMgDinv64), B<float>(I, bMgDinv32), B<float>(I, bMgBinv32));
+        ++L;
       }
-      const int64_t cn = std::max<int64_t>(mgp.nodes, 1);
-      if ((e = ensure(I, bZ32, vbytes32, msg)) || (e = ensure(I, bT32, vbytes32, msg)) ||
-          (e = ensure(I, bMgDoms, sizeof(DomDev) * mgp.doms.size(), msg)) ||
-          (e = ensure(I, bMgTiles, sizeof(Tile) * std::max<size_t>(mgp.tiles.size(), 1), msg)) ||
-          (e = ensure(I, bMgSvox, sizeof(float) * std::max<size_t>(mgp.svox.size(), 1), msg)) ||
-          (e = ensure(I, bMgFlags, cn, msg)) || (e = ensure(I, bMgDinv64, sizeof(double) * 3 * cn, msg)) ||
-          (e = ensure(I, bMgDinv32, sizeof(float) * 3 * cn, msg)) ||
-          (e = ensure(I, bMgBinv32, sizeof(float) * 6 * cn, msg)) ||
-          (e = ensure(I, bMgB, sizeof(float) * 72 * cn, msg)) || (e = ensure(I, bMgT, sizeof(float) * 72 * cn, msg)) ||
-          (e = ensure(I, bMgZ, sizeof(float) * 72 * cn, msg)) ||
-          (e = ensure(I, bMgMinv, sizeof(float) * mgp.minv.size(), msg)) ||
-          (e = ensure(I, bMgList, sizeof(int) * std::max<size_t>(mgp.lists.size(), 1), msg)) ||
-          (e = ensure(I, bMgNodes, sizeof(int64_t) * std::max<size_t>(mgp.nodes_l.size(), 1), msg)))
-        return e;
-      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgDoms], mgp.doms.data(), sizeof(DomDev) * mgp.doms.size(),
-                               cudaMemcpyHostToDevice, s));
-      if (!mgp.tiles.empty())
-        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgTiles], mgp.tiles.data(), sizeof(Tile) * mgp.tiles.size(),
-                                 cudaMemcpyHostToDevice, s));
-      if (!mgp.svox.empty())
-        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgSvox], mgp.svox.data(), sizeof(float) * mgp.svox.size(),
-                                 cudaMemcpyHostToDevice, s));
-      DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgMinv], mgp.minv.data(), sizeof(float) * mgp.minv.size(),
-                               cudaMemcpyHostToDevice, s));
-      if (!mgp.lists.empty())
-        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgList], mgp.lists.data(), sizeof(int) * mgp.lists.size(),
-                                 cudaMemcpyHostToDevice, s));
-      if (!mgp.nodes_l.empty())
-        DTC_CUDA(cudaMemcpyAsync(I.bufs[bMgNodes], mgp.nodes_l.data(), sizeof(int64_t) * mgp.nodes_l.size(),
-                                 cudaMemcpyHostToDevice, s));
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgFlags], 0, cn, s));
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgBinv32], 0, sizeof(float) * 6 * cn, s));
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgB], 0, sizeof(float) * 72 * cn, s));
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgT], 0, sizeof(float) * 72 * cn, s));
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bMgZ], 0, sizeof(float) * 72 * cn, s));
+    if ((e = launch_check(msg))) return e;
+    mgd.P = &mgp;
+    mgd.ndom = ndom;
+    mgd.tiles = B<Tile>(I, bMgTiles);
+    mgd.doms0 = dd;
+    mgd.doms = B<DomDev>(I, bMgDoms);
+    mgd.svox0 = B<float>(I, bSvox);
+    mgd.svox = B<float>(I, bMgSvox);
+    mgd.binv0 = B<float>(I, bBinv32);
+    mgd.binv = B<float>(I, bMgBinv32);
+    mgd.minv = B<float>(I, bMgMinv);
+    mgd.flags0 = fl;
+    mgd.flags = B<uint8_t>(I, bMgFlags);
+    mgd.lists = B<int>(I, bMgList);
+    mgd.nodes = B<int64_t>(I, bMgNodes);
+    mgd.b = B<float>(I, bMgB);
+    mgd.t = B<float>(I, bMgT);
+    mgd.z = B<float>(I, bMgZ);
+    mgd.t0 = B<float>(I, bT32);
+    mgd.z0 = B<float>(I, bZ32);
+    mgd.nen0 = NEN;
+    mgd.bricks0 = W.bi;
+    mgd.nbricks0 = W.nbi;
+    mgd.nodes0 = W.nodes;
+    mgd.nnodes0 = W.nnodes;
+    mgd.ke32 = W.ke32;
+    mgd.ke20tc = W.ke20tc;
+    mgd.err = W.err;
+    if (tune) {
+      if ((e = autotune_sweep(I, stats_, W, mgd, doms, svox, NEN, msg))) return e;
+      if (!I.tensor_matvec) W.ke20tc = mgd.ke20tc = nullptr;   // HEX20: the brick kernel won
+      // the timed launches wrote the fine multigrid vectors and the dot accumulators
       DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));
-      for (int l = 1; l < mgp.nlev; ++l)
-        if (mgp.all_n[l] > 0) {
-          k_node_setup<8><<<(unsigned)mgp.all_n[l], kThreads, 0, s>>>(
-              B<Tile>(I, bMgTiles) + mgp.all_off[l], B<DomDev>(I, bMgDoms) + (size_t)l * ndom, B<float>(I, bMgSvox),
-              B<uint8_t>(I, bMgFlags), B<double>(I, bMgDinv64), B<float>(I, bMgDinv32), B<float>(I, bMgBinv32));
-          ++L;
-        }
-      if ((e = launch_check(msg))) return e;
-      mgd.P = &mgp;
-      mgd.ndom = ndom;
-      mgd.tiles = B<Tile>(I, bMgTiles);
-      mgd.doms0 = dd;
-      mgd.doms = B<DomDev>(I, bMgDoms);
-      mgd.svox0 = B<float>(I, bSvox);
-      mgd.svox = B<float>(I, bMgSvox);
-      mgd.binv0 = B<float>(I, bBinv32);
-      mgd.binv = B<float>(I, bMgBinv32);
-      mgd.minv = B<float>(I, bMgMinv);
-      mgd.flags0 = fl;
-      mgd.flags = B<uint8_t>(I, bMgFlags);
-      mgd.lists = B<int>(I, bMgList);
-      mgd.nodes = B<int64_t>(I, bMgNodes);
-      mgd.b = B<float>(I, bMgB);
-      mgd.t = B<float>(I, bMgT);
-      mgd.z = B<float>(I, bMgZ);
-      mgd.t0 = B<float>(I, bT32);
-      mgd.z0 = B<float>(I, bZ32);
-      mgd.nen0 = NEN;
-      mgd.bricks0 = W.bi;
-      mgd.nbricks0 = W.nbi;
-      mgd.nodes0 = W.nodes;
-      mgd.nnodes0 = W.nnodes;
-      mgd.ke32 = W.ke32;
-      mgd.ke20tc = W.ke20tc;
-      mgd.err = W.err;
-      if (tune) {
-        if ((e = autotune_sweep(I, stats_, W, mgd, doms, svox, NEN, msg))) return e;
-        if (!I.tensor_matvec) W.ke20tc = mgd.ke20tc = nullptr;   // HEX20: the brick kernel won
-        // the timed launches wrote the fine multigrid vectors and the dot accumulators
-        DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
-        DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));
-        DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
-        DTC_CUDA(cudaMemsetAsync(I.bufs[bZr], 0, sizeof(double) * ncol, s));
-      }
-    }
-    // inner FP32 solves aim straight at the outer target when FP32 can reach it
-    const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);
-    const int max_refine = opt.max_refine > 0 ? opt.max_refine : 12;
-    int64_t inner_budget = opt.max_it;
-    for (int step = 0; step <= max_refine; ++step) {
       DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
-      if (nti) {
-        apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
-        k_residual_norm<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<double>(I, bDinv64), R64, B<double>(I, bZz));
-        L += 2;
-      }
-      k_outer_check<<<ndom, 32, 0, s>>>(ost, B<double>(I, bZz), B<double>(I, bTarget), B<int>(I, bDomAct), opt.rtol,
-                                        step == 0);
-      k_count_active<<<1, 256, 0, s>>>(B<int>(I, bDomAct), ndom, B<int>(I, bCount));
-      L += 2;
-      if ((e = launch_check(msg))) return e;
-      int h_count = 0;
-      DTC_CUDA(cudaMemcpyAsync(&h_count, I.bufs[bCount], sizeof(int), cudaMemcpyDeviceToHost, s));
-      DTC_CUDA(cudaStreamSynchronize(s));
-      if (h_count == 0 || step == max_refine || inner_budget <= 0) break;
-      if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
-      DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
-      if (use_mg)
-        e = run_cg_mg<NEN>(I, ndom, W, mgd, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
-                      inner, B<double>(I, bTarget), inner_budget, L, msg);
-      else if (opt.inner_precond >= 1)
-        e = run_cg<float, true, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
-                                B<float>(I, bW32), B<float>(I, bBinv32), inner, B<double>(I, bTarget), inner_budget,
-                                L, msg);
-      else
-        e = run_cg<float, false, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
-                                 B<float>(I, bW32), B<float>(I, bDinv32), inner, B<double>(I, bTarget), inner_budget,
-                                 L, msg);
-      if (e) return e;
-      if (nti) { k_apply_correction<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<float>(I, bX32), X, ost); ++L; }
-      k_add_inner_its<<<(unsigned)((ncol + 255) / 256), 256, 0, s>>>(ost, B<ColState>(I, bSt), (int64_t)ncol);
-      ++L;
-      if ((e = launch_check(msg))) return e;
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bZr], 0, sizeof(double) * ncol, s));
     }
   }
-  // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff)
-  DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
-  if (nta) {
-    apply_k<double, NEN, true, false>(W, dd, B<float>(I, bSvox), fl, X, R64, 1.0, nullptr, nullptr, s);
-    if (opt.tensor_estimator == 1)
-      k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf));
-    else
-      k_project<<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf));
-    L += 2;
-  }
-  if ((e = launch_check(msg))) return e;
-  DTC_CUDA(cudaEventRecord(I.ev_solve[1], s));
-  std::vector<double> ff((size_t)576 * ndom);
-  std::vector<ColState> cs(ncol);
-  DTC_CUDA(cudaMemcpyAsync(ff.data(), I.bufs[bFf], sizeof(double) * ff.size(), cudaMemcpyDeviceToHost, s));
-  DTC_CUDA(cudaMemcpyAsync(cs.data(), ost, sizeof(ColState) * ncol, cudaMemcpyDeviceToHost, s));
-  // optional displacement / force output in reference numbering
+
+  // the boundary modes (eps = 1e-6, the hard-coded boundary displacement of
+  // mod_write_deck.f90:61) and, per column pass, its 24 columns in c_uu
+  std::vector<double> modes((size_t)nm * 3 * nl), slices((size_t)ncp * 20 * 3 * kNLC, 0.0);
+  macro_modes_of_order(order, 1e-6, modes.data());
+  for (int cp = 0; cp < ncp; ++cp)
+    for (int lc = 0; lc < kNLC && cp * kNLC + lc < nl; ++lc)
+      for (int c = 0; c < 3; ++c)
+        for (int l = 0; l < nm; ++l)
+          slices[(size_t)cp * 20 * 3 * kNLC + l + nm * c + 3 * nm * lc] = modes[l + nm * c + (size_t)3 * nm * (cp * kNLC + lc)];
   bool want_fields = false;
   for (int d = 0; d < ndom; ++d) want_fields = want_fields || tasks[tidx[d]].out->displ || tasks[tidx[d]].out->force;
+  std::vector<ColState> cs(ncol * ncp);
   std::vector<double> hX, hF;
-  if (want_fields) {
-    hX.resize(node_total * 3 * kNLC);
-    hF.resize(node_total * 3 * kNLC);
-    DTC_CUDA(cudaMemcpyAsync(hX.data(), X, vbytes64, cudaMemcpyDeviceToHost, s));
-    DTC_CUDA(cudaMemcpyAsync(hF.data(), R64, vbytes64, cudaMemcpyDeviceToHost, s));
+  for (int cp = 0; cp < ncp; ++cp) {
+    if (cp > 0) {   // a later column pass starts from zero vectors like the first
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bX], 0, vbytes64, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bR64], 0, vbytes64, s));
+      if (mixed) {
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bR32], 0, vbytes32, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
+        if (use_mg) {
+          DTC_CUDA(cudaMemsetAsync(I.bufs[bZ32], 0, vbytes32, s));
+          DTC_CUDA(cudaMemsetAsync(I.bufs[bT32], 0, vbytes32, s));
+        }
+      }
+    }
+    DTC_CUDA(cudaMemcpyToSymbolAsync(c_uu, slices.data() + (size_t)cp * 20 * 3 * kNLC, sizeof(double) * 20 * 3 * kNLC,
+                                     0, cudaMemcpyHostToDevice, s));
+    if (nta) {
+      if (order == 2) k_boundary_values<20><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, fl, X);
+      else k_boundary_values<8><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, fl, X);
+      ++L;
+    }
+    if ((e = launch_check(msg))) return e;
+    if (!mixed) {
+      // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
+      DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
+      apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
+      ++L;
+      if ((e = run_cg<double, false, NEN>(I, ndom, W, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
+                              opt.rtol, nullptr, opt.max_it, L, msg)))
+        return e;
+      DTC_CUDA(cudaMemcpyAsync(ost, I.bufs[bSt], sizeof(ColState) * ncol, cudaMemcpyDeviceToDevice, s));
+    } else {
+      // every FP32 work vector starts at zero: the stencil reads boundary and void entries
+      if (cp == 0) {
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bR32], 0, vbytes32, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bX32], 0, vbytes32, s));
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bP32], 0, vbytes32, s));
+      }
+      // inner FP32 solves aim straight at the outer target when FP32 can reach it
+      const double inner = opt.inner_rtol > 0 ? opt.inner_rtol : std::max(0.3 * opt.rtol, 1e-7);
+      const int max_refine = opt.max_refine > 0 ? opt.max_refine : 12;
+      int64_t inner_budget = opt.max_it;
+      for (int step = 0; step <= max_refine; ++step) {
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
+        if (nti) {
+          apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
+          k_residual_norm<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<double>(I, bDinv64), R64, B<double>(I, bZz));
+          L += 2;
+        }
+        k_outer_check<<<ndom, 32, 0, s>>>(ost, B<double>(I, bZz), B<double>(I, bTarget), B<int>(I, bDomAct), opt.rtol,
+                                          step == 0);
+        k_count_active<<<1, 256, 0, s>>>(B<int>(I, bDomAct), ndom, B<int>(I, bCount));
+        L += 2;
+        if ((e = launch_check(msg))) return e;
+        int h_count = 0;
+        DTC_CUDA(cudaMemcpyAsync(&h_count, I.bufs[bCount], sizeof(int), cudaMemcpyDeviceToHost, s));
+        DTC_CUDA(cudaStreamSynchronize(s));
+        if (h_count == 0 || step == max_refine || inner_budget <= 0) break;
+        if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
+        DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
+        if (use_mg)
+          e = run_cg_mg<NEN>(I, ndom, W, mgd, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
+                        inner, B<double>(I, bTarget), inner_budget, L, msg);
+        else if (opt.inner_precond >= 1)
+          e = run_cg<float, true, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
+                                  B<float>(I, bW32), B<float>(I, bBinv32), inner, B<double>(I, bTarget), inner_budget,
+                                  L, msg);
+        else
+          e = run_cg<float, false, NEN>(I, ndom, W, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32),
+                                   B<float>(I, bW32), B<float>(I, bDinv32), inner, B<double>(I, bTarget), inner_budget,
+                                   L, msg);
+        if (e) return e;
+        if (nti) { k_apply_correction<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<float>(I, bX32), X, ost); ++L; }
+        k_add_inner_its<<<(unsigned)((ncol + 255) / 256), 256, 0, s>>>(ost, B<ColState>(I, bSt), (int64_t)ncol);
+        ++L;
+        if ((e = launch_check(msg))) return e;
+      }
+    }
+    // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff)
+    DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
+    if (nta) {
+      apply_k<double, NEN, true, false>(W, dd, B<float>(I, bSvox), fl, X, R64, 1.0, nullptr, nullptr, s);
+      if (opt.tensor_estimator == 1)
+        k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf));
+      else if (order == 2)
+        k_project<20><<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf), cp * kNLC);
+      else
+        k_project<8><<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf), 0);
+      L += 2;
+    }
+    if ((e = launch_check(msg))) return e;
+    DTC_CUDA(cudaMemcpyAsync(cs.data() + ncol * cp, ost, sizeof(ColState) * ncol, cudaMemcpyDeviceToHost, s));
+    // optional displacement / force output in reference numbering (load cases of this pass)
+    if (want_fields) {
+      hX.resize(node_total * 3 * kNLC);
+      hF.resize(node_total * 3 * kNLC);
+      DTC_CUDA(cudaMemcpyAsync(hX.data(), X, vbytes64, cudaMemcpyDeviceToHost, s));
+      DTC_CUDA(cudaMemcpyAsync(hF.data(), R64, vbytes64, cudaMemcpyDeviceToHost, s));
+      DTC_CUDA(cudaStreamSynchronize(s));
+      for (int d = 0; d < ndom; ++d) {
+        dtc_domain_out* o = tasks[tidx[d]].out;
+        if (!o->displ && !o->force) continue;
+        const MeshPlan& mp = *tasks[tidx[d]].plan;
+        const int64_t nn = mp.nn;
+        const DomDev& D = doms[d];
+        for (int64_t id = 0; id < nn; ++id) {
+          const int64_t node = D.node_off + mp.node_grid[id];  // the mesher's grid index is the device node index
+          for (int c = 0; c < 3; ++c)
+            for (int lc = 0; lc < kNLC && cp * kNLC + lc < nl; ++lc) {
+              const size_t src = (size_t)((node * 3 + c) * kNLC + lc);
+              const size_t dst = (size_t)(cp * kNLC + lc) * 3 * nn + 3 * id + c;
+              if (o->displ) o->displ[dst] = hX[src];
+              if (o->force) o->force[dst] = hF[src];
+            }
+        }
+      }
+    }
   }
+  DTC_CUDA(cudaEventRecord(I.ev_solve[1], s));
+  std::vector<double> ff((size_t)nl * nl * ndom);
+  DTC_CUDA(cudaMemcpyAsync(ff.data(), I.bufs[bFf], sizeof(double) * ff.size(), cudaMemcpyDeviceToHost, s));
   int h_err = 0;
   DTC_CUDA(cudaMemcpyAsync(&h_err, I.bufs[bErr], sizeof(int), cudaMemcpyDeviceToHost, s));
   DTC_CUDA(cudaStreamSynchronize(s));
@@ -2414,14 +2517,17 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   for (int d = 0; d < ndom; ++d) {
     DomainTask& t = tasks[tidx[d]];
     dtc_domain_out* o = t.out;
-    if (opt.tensor_estimator == 1) energy_to_ff(&ff[(size_t)576 * d], o->ff);
-    else std::memcpy(o->ff, &ff[(size_t)576 * d], sizeof(double) * 576);
+    double* off = order == 2 ? o->macro2->ff : o->ff;
+    if (opt.tensor_estimator == 1) energy_to_ff(&ff[(size_t)576 * d], off);
+    else std::memcpy(off, &ff[(size_t)nl * nl * d], sizeof(double) * nl * nl);
+    int64_t* iters = order == 2 ? o->macro2->iters : o->iters;
+    double* relres = order == 2 ? o->macro2->relres : o->relres;
     int worst = DTC_DOMAIN_OK;
     int steps = 0;
-    for (int lc = 0; lc < kNLC; ++lc) {
-      const ColState& c = cs[(size_t)d * kNLC + lc];
-      o->iters[lc] = c.its;
-      o->relres[lc] = c.dp0 > 0 ? c.dp / c.dp0 : 0.0;
+    for (int j = 0; j < nl; ++j) {
+      const ColState& c = cs[ncol * (j / kNLC) + (size_t)d * kNLC + j % kNLC];
+      iters[j] = c.its;
+      relres[j] = c.dp0 > 0 ? c.dp / c.dp0 : 0.0;
       steps = std::max(steps, (int)c.pad);
       int st = DTC_DOMAIN_OK;
       if (c.reason == kDivergedIts || (mixed && c.active)) st = DTC_DOMAIN_MAX_IT;
@@ -2432,21 +2538,6 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     }
     o->refine_steps = mixed ? steps : 0;
     o->status = worst;
-    if (want_fields && (o->displ || o->force)) {
-      const MeshPlan& mp = *t.plan;
-      const int64_t nn = mp.nn;
-      const DomDev& D = doms[d];
-      for (int64_t id = 0; id < nn; ++id) {
-        const int64_t g = mp.node_grid[id];
-        const int64_t node = D.node_off + g;  // the mesher's grid index is the device node index
-        for (int c = 0; c < 3; ++c)
-          for (int lc = 0; lc < kNLC; ++lc) {
-            const size_t src = (size_t)((node * 3 + c) * kNLC + lc);
-            if (o->displ) o->displ[(size_t)lc * 3 * nn + 3 * id + c] = hX[src];
-            if (o->force) o->force[(size_t)lc * 3 * nn + 3 * id + c] = hF[src];
-          }
-      }
-    }
   }
   if (keep != kKeepNone) {
     DeviceSolver::Impl::AdjChunk c;

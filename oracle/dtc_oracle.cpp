@@ -62,6 +62,106 @@ void loadcase_matrix(double eps, double* vv) {
       for (int l = 0; l < 8; ++l) vv[(k * 8 + l) + 24 * lc] = uu[l + 8 * k + 24 * lc];
 }
 
+// Boundary modes of the quadratic macro element, init_displ_hexe20 (mod_write_deck.f90:
+// 118-279): one row per statement `uu(:,c,lc) = [20 values]` of the source, values in units
+// of eps.  S9 / S7 are the default-kind (single precision) literals `.9` and `.7` the source
+// multiplies eps by in four places.
+const double S9 = (double)0.9f, S7 = (double)0.7f;
+struct Mode20Row { int lc, comp; double f[20]; };
+const Mode20Row kModes20[] = {
+    {1, 1, {0, 1, 1, 0, 0, 1, 1, 0, .5, 1, .5, 0, .5, 1, .5, 0, 0, 1, 1, 0}},
+    {2, 2, {0, 0, 1, 1, 0, 0, 1, 1, 0, .5, 1, .5, 0, .5, 1, .5, 0, 0, 1, 1}},
+    {3, 3, {0, 0, 0, 0, 1, 1, 1, 1, 0, 0, 0, 0, 1, 1, 1, 1, .5, .5, .5, .5}},
+    {4, 1, {1, 1, 0, 0, 1, 1, 0, 0, 1, .5, 0, .5, 1, .5, 0, .5, 1, 1, 0, 0}},
+    {5, 1, {1, 1, 1, 1, 0, 0, 0, 0, 1, 1, 1, 1, 0, 0, 0, 0, .5, .5, .5, .5}},
+    {6, 2, {0, 0, 0, 0, 1, 1, 1, 1, 0, 0, 0, 0, 1, 1, 1, 1, .5, .5, .5, .5}},
+    {7, 1, {0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, .5}},
+    {8, 2, {-2, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0}},
+    {9, 2, {0, -1, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0}},
+    {10, 3, {-1, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, .1, 0, 0, 0, 0, .5, 0, 0, 0}},
+    {11, 3, {0, -2, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0}},
+    {12, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, .1, 0, 0, 0, 0, 0, 0, 0, S9, 0}},
+    {13, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 5}},
+    {14, 1, {0, 0, 0, .2, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, 0, 0, 0, 5}},
+    {15, 1, {0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, 0, 0, 0}},
+    {16, 1, {0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, .2, 0, 0}},
+    {17, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, .3, 0}},
+    {18, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, .1, 0, 0, 0, 0, .1}},
+    {18, 3, {0, 0, 0, 0, 0, -S7, 0, 0, 0, 0, 0, 0, -.1, -1, 0, 0, 0, 0, 0, 0}},
+    {19, 2, {0, 0, 0, 0, 0, 0, 0, 0, .5, 0, 0, .5, 0, 0, 0, 0, .5, 0, 0, 0}},
+    {19, 3, {0, 0, 0, 0, 0, 0, -3, 0, 0, 0, 0, 0, 0, -1.5, 0, 0, 0, 0, -1.5, 0}},
+    {20, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, .1, 0, 0, 0, 0}},
+    {20, 3, {0, 0, 0, 0, 0, 0, 0, -3, 0, 0, 0, 0, 0, 0, -.1, 0, 0, 0, 0, 0}},
+    {21, 2, {0, 0, 5, 0, 0, 0, 0, 0, 0, .5, 0, 0, 0, 0, 0, 0, 0, 0, .5, 0}},
+    {22, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 0, 0, 0, 0, .5}},
+    {23, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 2, 0, 0, 0, 0}},
+    {24, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 0, -.5, 0}},
+    {25, 3, {0, 0, 0, 0, 0, 0, 0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {26, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {27, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -.1, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {27, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {28, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 4, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {29, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, .1, 0, 0, 0, 0, 0, 0, 0}},
+    {29, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -4, 0, 0, 0, 0, 0, 0, 0}},
+    {30, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -.1, 0, 0, 0, 0, 0, 0}},
+    {30, 3, {0, 0, 0, 0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {31, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -.1, 0, 0, 0, 0, 0}},
+    {31, 3, {0, 0, 5, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {32, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -.5, 0, 0, 0, 0}},
+    {33, 1, {0, 0, 0, 0, 0, .1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0, 0}},
+    {34, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -4, 0, 0}},
+    {35, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0}},
+    {36, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 2}},
+    {37, 1, {3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {38, 2, {0, -5, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {39, 1, {0, 0, -3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {40, 2, {0, 0, 0, -2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {41, 1, {0, 0, 0, 0, 5, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {42, 2, {0, 0, 0, 0, 0, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {43, 1, {0, 0, 0, 0, 0, 0, -4, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {44, 2, {0, 0, 0, 0, 0, 0, 0, 4, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {45, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 2, 0, 0, 0}},
+    {46, 3, {0, 0, 0, -2, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1.5, 0, 0, 0, 0, 0, 0}},
+    {47, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, -1, 2}},
+    {48, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0, 0, 0, 0}},
+    {49, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, -S9, 0, 0, 0, -S7, 0, 1, 0, 0, 0, 0}},
+    {50, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0}},
+    {51, 1, {0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {52, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {53, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {54, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {55, 1, {0, 0, 0, -1.5, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}},
+    {56, 2, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -5, 0, 0, 0, 0, 0, 0}},
+    {57, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0, 0, 0, 0}},
+    {58, 1, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0, 0, 0}},
+    {59, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0}},
+    {60, 3, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0, 0}},
+};
+
+void boundary_modes20(double eps, double* uu) {  // uu(20,3,60) column-major
+  std::fill(uu, uu + 20 * 3 * 60, 0.0);
+  for (const Mode20Row& m : kModes20)
+    for (int l = 0; l < 20; ++l)
+      uu[l + 20 * (m.comp - 1) + 60 * (m.lc - 1)] = m.f[l] == 0 ? 0.0 : m.f[l] * eps;
+}
+
+// init_loadcase_el_order_quad (mod_struct_calcmat.f90:1780-2028), vv(60,60).  The source table
+// is not usable as written: its row 49 is labelled 59 (so vv(49,:) stays zero and vv is
+// singular), 22 entries lack the factor e, and row 54 has 61 values.  Every other entry
+// equals the component-major flattening of the boundary modes for eps = e, except two that
+// the table writes with the double literal 0.9_rk where the modes use the single-precision .9
+// (row 10 of load case 49, row 59 of load case 12).  The oracle uses that flattening with the
+// two double entries, i.e. the table with its defects repaired.
+void loadcase_matrix_quad(double e, double* vv) {
+  std::vector<double> uu(20 * 3 * 60);
+  boundary_modes20(e, uu.data());
+  for (int lc = 0; lc < 60; ++lc)
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 20; ++l) vv[(k * 20 + l) + 60 * lc] = uu[l + 20 * k + 60 * lc];
+  vv[9 + 60 * 48] = -0.9 * e;
+  vv[58 + 60 * 11] = 0.9 * e;
+}
+
 // ---------------------------------------------------------------------------------------
 // Shape functions and the geometry -> xi map (mod_linfe.f90:19-84)
 inline double g1(double xi) { return 0.5 * (1.0 - xi); }
@@ -75,6 +175,34 @@ inline void phi_nn_hexe8(const double xi[3], double N[8]) {
   N[5] = g2(xi[0]) * g1(xi[1]) * g2(xi[2]);
   N[6] = g2(xi[0]) * g2(xi[1]) * g2(xi[2]);
   N[7] = g1(xi[0]) * g2(xi[1]) * g2(xi[2]);
+}
+// phi_NN_hexe20 (mod_linfe.f90:827-888): ANSYS 20-node brick, products left to right
+inline void phi_nn_hexe20(const double xi[3], double N[20]) {
+  const double f = 1. / 8., ff = 1. / 4., e = 1., z = 2.;
+  N[0] = f * (e - xi[0]) * (e - xi[1]) * (e - xi[2]) * (-xi[0] - xi[1] - xi[2] - z);
+  N[1] = f * (e + xi[0]) * (e - xi[1]) * (e - xi[2]) * (xi[0] - xi[1] - xi[2] - z);
+  N[2] = f * (e + xi[0]) * (e + xi[1]) * (e - xi[2]) * (xi[0] + xi[1] - xi[2] - z);
+  N[3] = f * (e - xi[0]) * (e + xi[1]) * (e - xi[2]) * (-xi[0] + xi[1] - xi[2] - z);
+  N[4] = f * (e - xi[0]) * (e - xi[1]) * (e + xi[2]) * (-xi[0] - xi[1] + xi[2] - z);
+  N[5] = f * (e + xi[0]) * (e - xi[1]) * (e + xi[2]) * (xi[0] - xi[1] + xi[2] - z);
+  N[6] = f * (e + xi[0]) * (e + xi[1]) * (e + xi[2]) * (xi[0] + xi[1] + xi[2] - z);
+  N[7] = f * (e - xi[0]) * (e + xi[1]) * (e + xi[2]) * (-xi[0] + xi[1] + xi[2] - z);
+  N[8] = ff * (e - xi[0] * xi[0]) * (e - xi[1]) * (e - xi[2]);
+  N[9] = ff * (e + xi[0]) * (e - xi[1] * xi[1]) * (e - xi[2]);
+  N[10] = ff * (e - xi[0] * xi[0]) * (e + xi[1]) * (e - xi[2]);
+  N[11] = ff * (e - xi[0]) * (e - xi[1] * xi[1]) * (e - xi[2]);
+  N[12] = ff * (e - xi[0] * xi[0]) * (e - xi[1]) * (e + xi[2]);
+  N[13] = ff * (e + xi[0]) * (e - xi[1] * xi[1]) * (e + xi[2]);
+  N[14] = ff * (e - xi[0] * xi[0]) * (e + xi[1]) * (e + xi[2]);
+  N[15] = ff * (e - xi[0]) * (e - xi[1] * xi[1]) * (e + xi[2]);
+  N[16] = ff * (e - xi[0]) * (e - xi[1]) * (e - xi[2] * xi[2]);
+  N[17] = ff * (e + xi[0]) * (e - xi[1]) * (e - xi[2] * xi[2]);
+  N[18] = ff * (e + xi[0]) * (e + xi[1]) * (e - xi[2] * xi[2]);
+  N[19] = ff * (e - xi[0]) * (e + xi[1]) * (e - xi[2] * xi[2]);
+}
+inline void phi_nn_macro(int nm, const double xi[3], double* N) {
+  if (nm == 20) phi_nn_hexe20(xi, N);
+  else phi_nn_hexe8(xi, N);
 }
 inline void t_geom_xi(const double node[3], const double xa[3], const double xe[3], double t[3]) {
   for (int d = 0; d < 3; ++d) t[d] = 2.0 / (xe[d] - xa[d]) * node[d] - (xe[d] + xa[d]) / (xe[d] - xa[d]);
@@ -338,10 +466,11 @@ bool gen_quadmesh(const orc_domain_in& in, Mesh& m) {
 
 // ---------------------------------------------------------------------------------------
 // Boundary conditions: generate_boundaries (mod_struct_preprocess.f90:490-738) with one
-// mesh part, and determine_prescribed_displ (mod_write_deck.f90:22-51), macro order 1.
+// mesh part, and determine_prescribed_displ (mod_write_deck.f90:22-51) for the macro order
+// (8 macro nodes / 24 load cases or 20 / 60).
 struct BC {
   std::vector<int64_t> ids;   // constrained node ids in node order
-  std::vector<double> vals;   // (24, 3*nb) column-major
+  std::vector<double> vals;   // (nl, 3*nb) column-major
 };
 
 void generate_boundaries(const orc_domain_in& in, const Mesh& m, BC& bc, double min_c[3], double max_c[3]) {
@@ -351,8 +480,10 @@ void generate_boundaries(const orc_domain_in& in, const Mesh& m, BC& bc, double 
     max_c[d] = (double)(in.xa_n[d] + in.L[d] - 1) * in.delta[d];   // xe_n * delta
     dim_c[d] = (double)in.L[d] * in.delta[d];                       // x_D_phy
   }
-  std::vector<double> uu(8 * 3 * 24);
-  boundary_modes(kEpsBC, uu.data());
+  const int nm = in.macro_order == 2 ? 20 : 8, nl = 3 * nm;
+  std::vector<double> uu(nm * 3 * nl);
+  if (nm == 20) boundary_modes20(kEpsBC, uu.data());
+  else boundary_modes(kEpsBC, uu.data());
   for (int64_t i = 0; i < m.nn; ++i) {
     const double* c = &m.nodes[3 * i];
     bool on = ((c[2] - min_c[2]) <= (dim_c[2] * kDeltaB)) || ((max_c[2] - c[2]) <= (dim_c[2] * kDeltaB)) ||
@@ -362,17 +493,17 @@ void generate_boundaries(const orc_domain_in& in, const Mesh& m, BC& bc, double 
   }
   // bnode_vals(lc, 3*(b-1)+comp), column-major; each value is a left-to-right Fortran SUM
   const int64_t nb = (int64_t)bc.ids.size();
-  bc.vals.assign(24 * 3 * nb, 0.0);
+  bc.vals.assign(nl * 3 * nb, 0.0);
   for (int64_t b = 0; b < nb; ++b) {
     const double* c = &m.nodes[3 * (bc.ids[b] - 1)];
-    double xi[3], N[8];
+    double xi[3], N[20];
     t_geom_xi(c, min_c, max_c, xi);
-    phi_nn_hexe8(xi, N);
+    phi_nn_macro(nm, xi, N);
     for (int comp = 0; comp < 3; ++comp)
-      for (int lc = 0; lc < 24; ++lc) {
+      for (int lc = 0; lc < nl; ++lc) {
         double s = 0.0;
-        for (int l = 0; l < 8; ++l) s += N[l] * uu[l + 8 * comp + 24 * lc];
-        bc.vals[lc + 24 * (3 * b + comp)] = s;
+        for (int l = 0; l < nm; ++l) s += N[l] * uu[l + nm * comp + nl * lc];
+        bc.vals[lc + nl * (3 * b + comp)] = s;
       }
   }
 }
@@ -386,7 +517,7 @@ struct CSR {
   std::vector<double> val;
   void mult(const double* x, double* y, int nrhs) const {  // y = A x, x/y [n][nrhs]
     for (int64_t i = 0; i < n; ++i) {
-      double acc[24];
+      double acc[60];
       for (int r = 0; r < nrhs; ++r) acc[r] = 0.0;
       for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
         const double a = val[p];
@@ -839,7 +970,8 @@ int run_domain(const orc_domain_in* in, orc_domain_out* out, bool solve) {
   if (st) { out->status = st; return st; }
   out->status = ORC_OK;
   out->ne = out->nn = out->nb = 0;
-  for (int i = 0; i < 24; ++i) out->iters[i] = 0;
+  const int nm = in->macro_order == 2 ? 20 : 8, nl = 3 * nm;   // macro nodes, load cases
+  for (int i = 0; i < 60; ++i) out->iters[i] = 0;
   Mesh m;
   if (!gen_quadmesh(*in, m)) { out->status = ORC_EMPTY; return ORC_EMPTY; }
   out->ne = m.ne; out->nn = m.nn;
@@ -867,12 +999,12 @@ int run_domain(const orc_domain_in* in, orc_domain_out* out, bool solve) {
   // bc dofs and values per load case
   std::vector<int64_t> gdof(3 * nb);
   for (int64_t b = 0; b < nb; ++b) for (int c = 0; c < 3; ++c) gdof[3 * b + c] = 3 * (bc.ids[b] - 1) + c;
-  std::vector<double> XX(n * 24, 0.0), F(n * 24, 0.0);
+  std::vector<double> XX(n * nl, 0.0), F(n * nl, 0.0);
   for (int64_t k = 0; k < 3 * nb; ++k)
-    for (int lc = 0; lc < 24; ++lc) XX[gdof[k] * 24 + lc] = -bc.vals[lc + 24 * k];
-  Aorg.mult(XX.data(), F.data(), 24);                       // F_lc = A (-u_c)  (:674-933)
-  for (int64_t k = 0; k < 3 * nb; ++k) for (int lc = 0; lc < 24; ++lc) F[gdof[k] * 24 + lc] = 0.0;
-  // MatZeroRowsColumns(AA, bc, diag = 0) (:945-951); b is already consistent for all 24
+    for (int lc = 0; lc < nl; ++lc) XX[gdof[k] * nl + lc] = -bc.vals[lc + nl * k];
+  Aorg.mult(XX.data(), F.data(), nl);                       // F_lc = A (-u_c)  (:674-933)
+  for (int64_t k = 0; k < 3 * nb; ++k) for (int lc = 0; lc < nl; ++lc) F[gdof[k] * nl + lc] = 0.0;
+  // MatZeroRowsColumns(AA, bc, diag = 0) (:945-951); b is already consistent for every load case
   CSR Az = A;
   std::vector<char> isbc(n, 0);
   for (int64_t k = 0; k < 3 * nb; ++k) isbc[gdof[k]] = 1;
@@ -886,42 +1018,60 @@ int run_domain(const orc_domain_in* in, orc_domain_out* out, bool solve) {
     for (int64_t p = Az.ptr[i]; p < Az.ptr[i + 1]; ++p) if (Az.col[p] == i) d = Az.val[p];
     dinv[i] = 1.0 / (d == 0.0 ? 1.0 : d);
   }
-  std::vector<double> X(n * 24);
-  int reasons[24];
-  pcg_batch(Az, dinv, F.data(), X.data(), 24, in->rtol, in->max_it, out->iters, reasons);
-  for (int lc = 0; lc < 24; ++lc) {
+  std::vector<double> X(n * nl);
+  int reasons[60];
+  pcg_batch(Az, dinv, F.data(), X.data(), nl, in->rtol, in->max_it, out->iters, reasons);
+  for (int lc = 0; lc < nl; ++lc) {
     if (reasons[lc] == -3 && out->status == ORC_OK) out->status = ORC_MAX_IT;
     if (reasons[lc] == -8 && out->status == ORC_OK) out->status = ORC_BREAKDOWN;
     if ((reasons[lc] == -9 || reasons[lc] == -4) && out->status == ORC_OK) out->status = ORC_NONFINITE;
   }
   // reactions: XX[bc] = u_c ; F = AA_org XX  (:1092-1123)
-  for (int64_t k = 0; k < 3 * nb; ++k) for (int lc = 0; lc < 24; ++lc) X[gdof[k] * 24 + lc] = bc.vals[lc + 24 * k];
-  Aorg.mult(X.data(), F.data(), 24);
+  for (int64_t k = 0; k < 3 * nb; ++k) for (int lc = 0; lc < nl; ++lc) X[gdof[k] * nl + lc] = bc.vals[lc + nl * k];
+  Aorg.mult(X.data(), F.data(), nl);
   if (out->displ && out->cap_nodes >= m.nn)
-    for (int lc = 0; lc < 24; ++lc) for (int64_t i = 0; i < n; ++i) out->displ[lc * n + i] = X[i * 24 + lc];
+    for (int lc = 0; lc < nl; ++lc) for (int64_t i = 0; i < n; ++i) out->displ[lc * n + i] = X[i * nl + lc];
   if (out->force && out->cap_nodes >= m.nn)
-    for (int lc = 0; lc < 24; ++lc) for (int64_t i = 0; i < n; ++i) out->force[lc * n + i] = F[i * 24 + lc];
+    for (int lc = 0; lc < nl; ++lc) for (int64_t i = 0; i < n; ++i) out->force[lc * n + i] = F[i * nl + lc];
 
   // calc_effective_material_parameters (mod_struct_calcmat.f90:23-1673)
-  double vv[576];
-  loadcase_matrix(in->rve_strain, vv);
-  inverse(24, vv);
-  double* ff = out->ff;
-  std::fill(ff, ff + 576, 0.0);
-  for (int lc = 0; lc < 24; ++lc)
+  std::vector<double> vv(nl * nl);
+  if (nm == 20) loadcase_matrix_quad(in->rve_strain, vv.data());
+  else loadcase_matrix(in->rve_strain, vv.data());
+  inverse(nl, vv.data());
+  double* ff = out->ff;   // ff(nl, nl), column-major
+  std::fill(ff, ff + nl * nl, 0.0);
+  for (int lc = 0; lc < nl; ++lc)
     for (int64_t j = 0; j < m.nn; ++j) {
-      double xi[3], N[8];
+      double xi[3], N[20];
       t_geom_xi(&m.nodes[3 * j], min_c, max_c, xi);
-      phi_nn_hexe8(xi, N);
+      phi_nn_macro(nm, xi, N);
       for (int k = 0; k < 3; ++k)
-        for (int l = 0; l < 8; ++l) ff[(k * 8 + l) + 24 * lc] = ff[(k * 8 + l) + 24 * lc] + F[(3 * j + k) * 24 + lc] * N[l];
+        for (int l = 0; l < nm; ++l) ff[(k * nm + l) + nl * lc] = ff[(k * nm + l) + nl * lc] + F[(3 * j + k) * nl + lc] * N[l];
     }
-  matmul(24, 24, 24, ff, vv, out->kmacro);
-  out->sym_k = check_sym(24, out->kmacro);
+  matmul(nl, nl, nl, ff, vv.data(), out->kmacro);
+  out->sym_k = check_sym(nl, out->kmacro);
   double xdp[3] = {(double)in->L[0] * in->delta[0], (double)in->L[1] * in->delta[1], (double)in->L[2] * in->delta[2]};
   double fv[36];
-  auto f = [&](int r, int c) { return ff[(r - 1) + 24 * (c - 1)]; };
-  for (int ii = 1; ii <= 6; ++ii) {   // :345-359
+  auto f = [&](int r, int c) { return ff[(r - 1) + nl * (c - 1)]; };
+  if (nm == 20) for (int ii = 1; ii <= 6; ++ii) {   // :368-401, the 8 nodes of each face
+    fv[0 + 6 * (ii - 1)] = (f(2, ii) + f(3, ii) + f(6, ii) + f(7, ii) + f(10, ii) + f(14, ii) + f(18, ii) + f(19, ii)) /
+                           (xdp[1] * xdp[2]);
+    fv[1 + 6 * (ii - 1)] = (f(23, ii) + f(24, ii) + f(27, ii) + f(28, ii) + f(31, ii) + f(35, ii) + f(39, ii) + f(40, ii)) /
+                           (xdp[0] * xdp[2]);
+    fv[2 + 6 * (ii - 1)] = (f(45, ii) + f(46, ii) + f(47, ii) + f(48, ii) + f(53, ii) + f(54, ii) + f(55, ii) + f(56, ii)) /
+                           (xdp[0] * xdp[1]);
+    fv[3 + 6 * (ii - 1)] =
+        0.5 * ((f(3, ii) + f(4, ii) + f(7, ii) + f(8, ii) + f(11, ii) + f(15, ii) + f(19, ii) + f(20, ii)) / (xdp[0] * xdp[2]) +
+               (f(22, ii) + f(23, ii) + f(26, ii) + f(27, ii) + f(30, ii) + f(34, ii) + f(38, ii) + f(39, ii)) / (xdp[1] * xdp[2]));
+    fv[4 + 6 * (ii - 1)] =
+        0.5 * ((f(5, ii) + f(6, ii) + f(7, ii) + f(8, ii) + f(13, ii) + f(14, ii) + f(15, ii) + f(16, ii)) / (xdp[0] * xdp[1]) +
+               (f(42, ii) + f(43, ii) + f(46, ii) + f(47, ii) + f(50, ii) + f(54, ii) + f(58, ii) + f(59, ii)) / (xdp[1] * xdp[2]));
+    fv[5 + 6 * (ii - 1)] =
+        0.5 * ((f(25, ii) + f(26, ii) + f(27, ii) + f(28, ii) + f(33, ii) + f(34, ii) + f(35, ii) + f(36, ii)) / (xdp[0] * xdp[1]) +
+               (f(43, ii) + f(44, ii) + f(47, ii) + f(48, ii) + f(51, ii) + f(55, ii) + f(59, ii) + f(60, ii)) / (xdp[0] * xdp[2]));
+  }
+  else for (int ii = 1; ii <= 6; ++ii) {   // :345-359
     fv[0 + 6 * (ii - 1)] = (f(2, ii) + f(3, ii) + f(6, ii) + f(7, ii)) / (xdp[1] * xdp[2]);
     fv[1 + 6 * (ii - 1)] = (f(11, ii) + f(12, ii) + f(15, ii) + f(16, ii)) / (xdp[0] * xdp[2]);
     fv[2 + 6 * (ii - 1)] = (f(21, ii) + f(22, ii) + f(23, ii) + f(24, ii)) / (xdp[0] * xdp[1]);
@@ -968,6 +1118,8 @@ int orc_element_stiffness(int32_t nen, double E, double a, double nu, double* ke
 
 void orc_boundary_modes(double eps, double* uu) { boundary_modes(eps, uu); }
 void orc_loadcase_matrix(double eps, double* vv) { loadcase_matrix(eps, vv); }
+void orc_boundary_modes20(double eps, double* uu) { boundary_modes20(eps, uu); }
+void orc_loadcase_matrix_quad(double eps, double* vv) { loadcase_matrix_quad(eps, vv); }
 void orc_rotation_search(const double* ee, orc_domain_out* out) { rotation_search(ee, out); }
 
 }  // extern "C"

@@ -51,14 +51,17 @@ typedef struct {
   int64_t max_it;
   const int32_t* phi;    /* L0*L1*L2 gray values, x fastest */
   const float* E_voxel;  /* optional per-voxel modulus (extension); NULL -> E everywhere */
+  int32_t macro_order;   /* 'Element order on macro scale': 1 (or 0) -> 8 macro nodes, nl = 24
+                            load cases; 2 -> 20 macro nodes, nl = 60 */
+  int32_t pad_;
 } orc_domain_in;
 
 typedef struct {
   int32_t status;
   int64_t ne, nn, nb;              /* elements, nodes, constrained nodes */
-  int64_t iters[24];
-  double ff[576];                  /* "Domain forces" ff(24,24) */
-  double kmacro[576];              /* "Effective numerical stiffness" ff*vv^-1 */
+  int64_t iters[60];               /* per load case (first nl used) */
+  double ff[3600];                 /* "Domain forces" ff(nl,nl), column-major with leading dimension nl */
+  double kmacro[3600];             /* "Effective numerical stiffness" ff*vv^-1, nl x nl */
   double sym_k;
   double c[36];                    /* "Effective stiffness" fv*meps */
   double sym_c;
@@ -74,13 +77,13 @@ typedef struct {
   int64_t* elem_voxel;             /* ne: 0-based voxel index x+L0*(y+L1*z) of each element */
   double* nodes;                   /* 3*nn coordinates */
   int64_t* bnode_ids;              /* nb constrained node ids, in node order */
-  double* bnode_vals;              /* 24 x (3*nb) prescribed values, column-major like bnode_vals(24,3nb) */
-  double* displ;                   /* 24 x 3nn solutions incl. BC values (lc-major) */
-  double* force;                   /* 24 x 3nn reaction forces AA_org*u (lc-major) */
+  double* bnode_vals;              /* nl x (3*nb) prescribed values, column-major like bnode_vals(nl,3nb) */
+  double* displ;                   /* nl x 3nn solutions incl. BC values (lc-major) */
+  double* force;                   /* nl x 3nn reaction forces AA_org*u (lc-major) */
   int64_t cr1_ang[3], cr2_ang[3];  /* argmin indices (alpha, phi, eta) in units of 10^-jj degree */
 } orc_domain_out;
 
-/* Full path for one domain: mesh -> BC -> assembly -> 24 CG solves -> reactions ->
+/* Full path for one domain: mesh -> BC -> assembly -> nl CG solves -> reactions ->
  * ff -> K_macro -> C -> EE -> rotation search. */
 int orc_solve_domain(const orc_domain_in* in, orc_domain_out* out);
 
@@ -97,6 +100,11 @@ int orc_element_stiffness(int32_t nen, double E, double a, double nu, double* ke
 /* Boundary-mode table uu(8,3,24) (column-major) for eps, and vv(24,24) for eps. */
 void orc_boundary_modes(double eps, double* uu);
 void orc_loadcase_matrix(double eps, double* vv);
+
+/* Macro order 2: uu(20,3,60) of init_displ_hexe20 and the repaired quadratic load-case
+ * matrix vv(60,60) (init_loadcase_el_order_quad; see loadcase_matrix_quad). */
+void orc_boundary_modes20(double eps, double* uu);
+void orc_loadcase_matrix_quad(double eps, double* vv);
 
 /* Rotation search alone, on a symmetric 6x6 tensor ee (column-major); fills the cr1_* and
  * cr2_* fields of out. */

@@ -24,14 +24,15 @@ class OrcIn(C.Structure):
         ("E", C.c_double), ("nu", C.c_double), ("rve_strain", C.c_double),
         ("rtol", C.c_double), ("max_it", C.c_int64),
         ("phi", C.POINTER(C.c_int32)), ("E_voxel", C.POINTER(C.c_float)),
+        ("macro_order", C.c_int32), ("pad_", C.c_int32),
     ]
 
 
 class OrcOut(C.Structure):
     _fields_ = [
         ("status", C.c_int32), ("ne", C.c_int64), ("nn", C.c_int64), ("nb", C.c_int64),
-        ("iters", C.c_int64 * 24),
-        ("ff", C.c_double * 576), ("kmacro", C.c_double * 576), ("sym_k", C.c_double),
+        ("iters", C.c_int64 * 60),
+        ("ff", C.c_double * 3600), ("kmacro", C.c_double * 3600), ("sym_k", C.c_double),
         ("c", C.c_double * 36), ("sym_c", C.c_double),
         ("ee", C.c_double * 36), ("sym_ee", C.c_double),
         ("cr1_angle", C.c_double), ("cr1_n", C.c_double * 3), ("cr1_aa", C.c_double * 9),
@@ -68,6 +69,8 @@ def lib():
         _lib.orc_element_stiffness.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
         _lib.orc_boundary_modes.argtypes = [C.c_double, C.POINTER(C.c_double)]
         _lib.orc_loadcase_matrix.argtypes = [C.c_double, C.POINTER(C.c_double)]
+        _lib.orc_boundary_modes20.argtypes = [C.c_double, C.POINTER(C.c_double)]
+        _lib.orc_loadcase_matrix_quad.argtypes = [C.c_double, C.POINTER(C.c_double)]
         _lib.orc_rotation_search.argtypes = [C.POINTER(C.c_double), C.POINTER(OrcOut)]
     return _lib
 
@@ -99,12 +102,24 @@ def loadcase_matrix(eps=1e-6):
     return vv
 
 
+def boundary_modes20(eps=1e-6):
+    uu = np.zeros((20, 3, 60), order="F")
+    lib().orc_boundary_modes20(eps, _dptr(uu))
+    return uu
+
+
+def loadcase_matrix_quad(eps=1e-6):
+    vv = np.zeros((60, 60), order="F")
+    lib().orc_loadcase_matrix_quad(eps, _dptr(vv))
+    return vv
+
+
 class Domain:
     """One domain's input, held with its backing numpy arrays alive."""
 
     def __init__(self, phi, *, llimit=1, nen=8, delta=0.05, phdsize=None, E=5600.0, nu=0.3,
                  rve_strain=1e-6, rtol=1e-10, max_it=500000, xa_n=(2, 2, 2), rotation=False,
-                 E_voxel=None):
+                 E_voxel=None, macro_order=1):
         phi = np.asarray(phi)
         assert phi.ndim == 3, "phi is indexed [z, y, x] (x fastest in memory)"
         self.phi = np.ascontiguousarray(phi, dtype=np.int32)
@@ -126,8 +141,10 @@ class Domain:
         self.s.phi = self.phi.ctypes.data_as(C.POINTER(C.c_int32))
         self.s.E_voxel = (self.E_voxel.ctypes.data_as(C.POINTER(C.c_float))
                           if self.E_voxel is not None else C.POINTER(C.c_float)())
+        self.s.macro_order = int(macro_order)
         self.L = L
         self.nen = nen
+        self.nl = 60 if macro_order == 2 else 24
 
 
 def _out_struct(dom, with_arrays):
@@ -144,9 +161,9 @@ def _out_struct(dom, with_arrays):
         keep["elem_voxel"] = np.zeros(me, np.int64)
         keep["nodes"] = np.zeros(3 * mn)
         keep["bnode_ids"] = np.zeros(mn, np.int64)
-        keep["bnode_vals"] = np.zeros(24 * 3 * mn)
-        keep["displ"] = np.zeros(24 * 3 * mn)
-        keep["force"] = np.zeros(24 * 3 * mn)
+        keep["bnode_vals"] = np.zeros(dom.nl * 3 * mn)
+        keep["displ"] = np.zeros(dom.nl * 3 * mn)
+        keep["force"] = np.zeros(dom.nl * 3 * mn)
         o.cap_elems, o.cap_nodes = me, mn
         o.elems, o.elem_voxel = _iptr(keep["elems"]), _iptr(keep["elem_voxel"])
         o.nodes = _dptr(keep["nodes"])
@@ -156,11 +173,12 @@ def _out_struct(dom, with_arrays):
 
 
 def _result(dom, o, keep):
+    nl = dom.nl if dom is not None else 24
     r = {
         "status": o.status, "ne": o.ne, "nn": o.nn, "nb": o.nb,
-        "iters": np.array(o.iters[:]),
-        "ff": np.array(o.ff[:]).reshape(24, 24, order="F"),
-        "kmacro": np.array(o.kmacro[:]).reshape(24, 24, order="F"),
+        "iters": np.array(o.iters[:nl]),
+        "ff": np.array(o.ff[: nl * nl]).reshape(nl, nl, order="F"),
+        "kmacro": np.array(o.kmacro[: nl * nl]).reshape(nl, nl, order="F"),
         "sym_k": o.sym_k, "c": np.array(o.c[:]).reshape(6, 6, order="F"), "sym_c": o.sym_c,
         "ee": np.array(o.ee[:]).reshape(6, 6, order="F"), "sym_ee": o.sym_ee,
         "density": o.density,
@@ -179,9 +197,9 @@ def _result(dom, o, keep):
         r["elem_voxel"] = keep["elem_voxel"][:ne]
         r["nodes"] = keep["nodes"][: 3 * nn].reshape(nn, 3)
         r["bnode_ids"] = keep["bnode_ids"][:nb]
-        r["bnode_vals"] = keep["bnode_vals"][: 24 * 3 * nb].reshape(24, 3 * nb, order="F")
-        r["displ"] = keep["displ"][: 24 * 3 * nn].reshape(24, 3 * nn)
-        r["force"] = keep["force"][: 24 * 3 * nn].reshape(24, 3 * nn)
+        r["bnode_vals"] = keep["bnode_vals"][: nl * 3 * nb].reshape(nl, 3 * nb, order="F")
+        r["displ"] = keep["displ"][: nl * 3 * nn].reshape(nl, 3 * nn)
+        r["force"] = keep["force"][: nl * 3 * nn].reshape(nl, 3 * nn)
     return r
 
 

@@ -35,7 +35,8 @@ def test_struct_layouts_match_the_header(dtc, tmp_path):
     """ctypes mirrors of the C structs have the size and field offsets the C compiler gives."""
     import subprocess
     structs = {"dtc_options": dtc.capi.Options, "dtc_domain_in": dtc.capi.DomainIn,
-               "dtc_domain_out": dtc.capi.DomainOut, "dtc_mesh_out": dtc.capi.MeshOut}
+               "dtc_domain_out": dtc.capi.DomainOut, "dtc_mesh_out": dtc.capi.MeshOut,
+               "dtc_macro2_out": dtc.capi.Macro2Out}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dtc.h"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -83,6 +84,22 @@ def test_create_reports_missing_device_or_abi(dtc):
         assert lib.dtc_create(C.byref(h), C.byref(o)) == dtc.capi.DTC_ERR_NO_DEVICE
         with pytest.raises(dtc.DTCError):
             dtc.Solver()
+
+
+def test_macro_order_option_validation(dtc):
+    """Macro order 2 takes the reference's reaction projection and has no adjoint: other
+    combinations are refused before any device is touched."""
+    lib = dtc.capi.load()
+    h = C.c_void_p()
+    for order, est, keep in ((3, 0, 0), (-1, 0, 0), (2, 1, 0), (2, 0, 1)):
+        o = dtc.capi.Options()
+        lib.dtc_default_options(C.byref(o))
+        o.macro_order, o.tensor_estimator, o.keep_displacements = order, est, keep
+        assert lib.dtc_create(C.byref(h), C.byref(o)) == dtc.capi.DTC_ERR_INVALID_ARGUMENT
+    out = dtc.capi.MeshOut()
+    out.macro_order = 3
+    d = dtc.Domain(np.ones((3, 3, 3), np.int16))
+    assert lib.dtc_mesh_domain(C.byref(d.struct), C.byref(out)) == dtc.capi.DTC_ERR_INVALID_ARGUMENT
 
 
 def test_result_records_convert_fieldwise(dtc):

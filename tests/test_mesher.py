@@ -5,10 +5,10 @@ import numpy as np
 import pytest
 
 
-def compare(dtc, orc, phi, nen=8, **kw):
+def compare(dtc, orc, phi, nen=8, macro_order=1, **kw):
     d = dtc.Domain(phi, elem_type=nen, **kw)
-    od = orc.Domain(phi, nen=nen, **kw)
-    m = dtc.mesh_domain(d)
+    od = orc.Domain(phi, nen=nen, macro_order=macro_order, **kw)
+    m = dtc.mesh_domain(d, macro_order=macro_order)
     r = orc.mesh_domain(od)
     assert m["status"] == r["status"]
     if r["status"] == 0:
@@ -28,6 +28,20 @@ def test_random_volumes(dtc, orc, nen):
         p = rng.random() * 0.7
         phi = (rng.random((L[2], L[1], L[0])) < p).astype(np.int16) * int(rng.integers(1, 30000))
         compare(dtc, orc, phi, nen=nen, delta=0.05, xa_n=tuple(int(v) for v in rng.integers(1, 40, 3)))
+
+
+@pytest.mark.parametrize("nen", [8, 20])
+def test_quadratic_macro_boundary_values(dtc, orc, nen):
+    """Macro order 2: the 60 prescribed values of every constrained node (determine_prescribed_displ
+    with init_displ_hexe20 and phi_NN_hexe20, mod_write_deck.f90:22-51,118-279) bit for bit."""
+    rng = np.random.default_rng(5 + nen)
+    for _ in range(12):
+        L = rng.integers(2, 8, size=3)
+        phi = (rng.random((L[2], L[1], L[0])) < 0.6).astype(np.int16) * 1000
+        m, r = compare(dtc, orc, phi, nen=nen, macro_order=2, delta=0.05,
+                       xa_n=tuple(int(v) for v in rng.integers(1, 40, 3)))
+        if r["status"] == 0:
+            assert m["bnode_vals"].shape == (60, 3 * m["nb"])
 
 
 @pytest.mark.parametrize("dtype", [np.int8, np.int16, np.int32])

@@ -14,27 +14,34 @@ def hooke(E, nu):
     return C
 
 
+@pytest.mark.parametrize("macro_order", [1, 2])
 @pytest.mark.parametrize("nen", [8, 20])
-def test_solid_cube_gives_isotropic_hooke(orc, nen):
-    """TC01 isotropic (regression/TC01-1_test_dev_dtc_isotropic-std-HEX08-ME1.meta): a fully
-    solid domain; trilinear and serendipity elements reproduce the affine modes exactly."""
+def test_solid_cube_gives_isotropic_hooke(orc, nen, macro_order):
+    """TC01 isotropic (regression/TC01-1_test_dev_dtc_isotropic-std-HEX08-ME1.meta and -ME2): a
+    fully solid domain; trilinear and serendipity elements reproduce the affine modes exactly,
+    and the first six load cases of either macro element are those modes."""
     E, nu = 5600.0, 0.3
-    r = orc.solve_domain(orc.Domain(np.full((4, 4, 4), 14250), E=E, nu=nu, delta=0.01, rtol=1e-13, nen=nen))
+    r = orc.solve_domain(orc.Domain(np.full((4, 4, 4), 14250), E=E, nu=nu, delta=0.01, rtol=1e-13, nen=nen,
+                                    macro_order=macro_order))
     assert r["status"] == 0
+    assert r["ff"].shape == ((60, 60) if macro_order == 2 else (24, 24))
     C = hooke(E, nu)
     assert np.abs(r["c"] - C).max() / C.max() < 1e-9
     assert r["density"] == 1.0
 
 
-def test_kmacro_symmetric_and_rigid_modes(orc):
+@pytest.mark.parametrize("macro_order", [1, 2])
+def test_kmacro_symmetric_and_rigid_modes(orc, macro_order):
     syn_phi = np.random.default_rng(4).random((6, 6, 6)) < 0.6
-    r = orc.solve_domain(orc.Domain(syn_phi.astype(np.int32) * 20000, rtol=1e-12))
+    r = orc.solve_domain(orc.Domain(syn_phi.astype(np.int32) * 20000, rtol=1e-12, macro_order=macro_order))
     K = r["kmacro"]
+    nm = 20 if macro_order == 2 else 8
+    assert K.shape == (3 * nm, 3 * nm)
     assert r["sym_k"] < 1e-6
-    # translations of the macro element produce no force: dof index (k-1)*8 + l
+    # translations of the macro element produce no force: dof index (k-1)*nm + l
     for c in range(3):
-        t = np.zeros(24)
-        t[c * 8:(c + 1) * 8] = 1.0
+        t = np.zeros(3 * nm)
+        t[c * nm:(c + 1) * nm] = 1.0
         assert np.abs(K @ t).max() < 1e-6 * np.abs(K).max()
 
 
