@@ -286,7 +286,7 @@ def run_config(args, dtc):
         ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8]
         for arm, kw in (("mixed", dict(precision="mixed", estimator="energy", inner_precond="mg",
                                        mixed_matvec=args.matvec)),
-                        ("fp64", dict(precision="fp64"))):
+                        ("fp64", dict(precision="fp64", mixed_matvec=args.matvec))):
             # loosest rtol whose tensors stay within TARGET/2 of FP64 at 1e-10 on the sample
             for rt in ladder:
                 with dtc.Solver(rtol=rt, rotation_search=False, device=local, **kw) as sv:
@@ -319,14 +319,17 @@ def run_config(args, dtc):
         doms = [dtc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=syn.modulus_of_gray(g),
                            domain_number=i) for i, g in enumerate(grays)]
         with dtc.Solver(precision="mixed", rtol=3e-5, rotation_search=True, device=local, estimator="energy",
-                        inner_precond="mg") as sv:
+                        inner_precond="mg", mixed_matvec=args.matvec) as sv:
             res = []
 
             def step():
                 res[:] = sv.solve(doms)
                 return sv.stats()["ms_solve"]
             dev, wall = _timed(step, steps, warm)
-            rot = sv.kernel_stats().get("rotation_search_f64", {})
+            kst = sv.kernel_stats()
+            rot = kst.get("rotation_search_f64", {})
+            tuned = {k[len("autotune_"):]: round(1e3 * v["ms_total"] / max(v["launches"], 1), 1)
+                     for k, v in kst.items() if k.startswith("autotune_")}
         sample = [i for i in range(0, n, max(1, n // 12))]
         with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device=local) as ref:
             truth = ref.solve([doms[i] for i in sample])
@@ -340,11 +343,14 @@ def run_config(args, dtc):
                          1e3 * rot["ms_total"] / n if rot else None,
                      "rotation_fp64_tflops": (rot["flops_per_launch"] * rot["launches"] / (rot["ms_total"] / 1e3)
                                               / 1e12 if rot and rot["ms_total"] > 0 else None),
-                     "voxels": int(sum(int(L) ** 3 for L in Ls))})
+                     "voxels": int(sum(int(L) ** 3 for L in Ls)),
+                     "matvec": args.matvec,
+                     "autotune_us_per_launch_summed_over_passes_and_classes": tuned or None})
     elif args.config == "me2":
         # macro order 2 (20-node macro element, 60 load cases): HEX08 domains of 32^3, BV/TV
-        # U(0.10, 0.40), per-voxel E; mixed (multigrid, the reference's reaction projection) vs
-        # plain FP64, each at its calibrated rtol; the oracle at rtol 1e-10 on 4 domains
+        # U(0.10, 0.40), per-voxel E; mixed (multigrid, energy estimator over the 60 x 60 Gram
+        # matrix of the three column passes) vs plain FP64 (the reference's reaction projection),
+        # each at its calibrated rtol; the oracle at rtol 1e-10 on 4 domains
         n = args.ndom
         grays, _ = make_inputs(dtc, n, args.L)
         doms = [dtc.Domain(g, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, E_voxel=syn.modulus_of_gray(g))
@@ -354,8 +360,9 @@ def run_config(args, dtc):
             truth = ref.solve(sample)
         out = {}
         ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8]
-        for arm, kw in (("mixed", dict(precision="mixed", inner_precond="mg", mixed_matvec=args.matvec)),
-                        ("fp64", dict(precision="fp64"))):
+        for arm, kw in (("mixed", dict(precision="mixed", inner_precond="mg", mixed_matvec=args.matvec,
+                                       estimator=args.estimator)),
+                        ("fp64", dict(precision="fp64", mixed_matvec=args.matvec))):
             for rt in ladder:
                 with dtc.Solver(rtol=rt, rotation_search=False, device=local, macro_order=2, **kw) as sv:
                     err = _err(sv.solve(sample), truth)
@@ -376,7 +383,7 @@ def run_config(args, dtc):
         oref = orc.solve_batch(odoms, nthreads=4)
         tcpu = time.perf_counter() - t0
         with dtc.Solver(precision="mixed", rtol=out["mixed"]["rtol"], rotation_search=False, device=local,
-                        macro_order=2, inner_precond="mg") as sv:
+                        macro_order=2, inner_precond="mg", estimator=args.estimator) as sv:
             res = sv.solve(doms[:4])
 
         def rel(a, b):
@@ -519,7 +526,7 @@ def main():
     ladder = [1e-3, 3e-4, 1e-4, 3e-5, 1e-5, 3e-6, 1e-6, 3e-7, 1e-7, 3e-8, 1e-8, 3e-9, 1e-9]
     arms = {"mixed": dict(precision="mixed", estimator=args.estimator, inner_precond=args.precond,
                           mixed_matvec=args.matvec),
-            "fp64": dict(precision="fp64", estimator="reaction")}
+            "fp64": dict(precision="fp64", estimator="reaction", mixed_matvec=args.matvec)}
     rtol_of, err_of = {}, {}
     for arm, kw in arms.items():
         for rt in ladder if args.rtol <= 0 else [args.rtol]:
@@ -566,7 +573,7 @@ def main():
     fp64 = None
     if not args.no_fp64:
         with dtc.Solver(precision="fp64", rtol=rtol_of["fp64"], max_it=args.max_it, rotation_search=False,
-                        device=local) as plain:
+                        device=local, mixed_matvec=args.matvec) as plain:
             plain.solve(doms)
             fp64_ms = plain.stats()["ms_solve"]
         fp64_ms = reduce_over_ranks([fp64_ms], "max")[0]
@@ -603,8 +610,11 @@ def main():
     autotune = None
     if tune:
         us = {k[len("autotune_"):]: 1e3 * v["ms_total"] / max(v["launches"], 1) for k, v in tune.items()}
-        autotune = {"post_smoothing_sweep_us": us,
-                    "pick": "tensor" if us.get("tc_sweep", 1e30) < us.get("simt_sweep", 1e30) else "simt"}
+        autotune = {"timed_us_per_launch": us,
+                    "pick": "tensor" if us.get("tc_sweep", 1e30) < us.get("simt_sweep", 1e30) else "simt",
+                    "note": "simt_sweep / tc_sweep: fine post-smoothing; *_4cta / *_5cta: the SIMT residual, "
+                            "post-smoothing and CG-application sweeps at 4 or 5 CTAs per SM; f64_*: the FP64 "
+                            "sweep at 1 or 3 CTAs per SM"}
     top = max((k for k in ks if ks[k]["bytes_per_launch"] > 0), key=lambda k: ks[k]["ms_total"])
     kt = ks[top]
     t_launch = kt["ms_total"] / kt["launches"] / 1e3

@@ -78,9 +78,13 @@ typedef struct dtc_options {
                               (dtc_get_kernel_stats); adds event records, off for production */
   int32_t mixed_matvec;    /* stiffness contraction of the FP32 inner solve: 0 = SIMT FP32,
                               1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy),
-                              2 = autotuned: HEX08 multigrid solves time both sweep kernels on
-                              the batch's own tiles and keep the faster, cached per device and
-                              size class (dtc_get_kernel_stats lists the timings) */
+                              2 = autotuned: multigrid solves time both kernels of the fine-level
+                              operator on the batch's own tiles and keep the faster; for the HEX08
+                              SIMT sweeps also the register budget (4 or 5 CTAs per SM) of each of
+                              the residual, post-smoothing and CG-application sweeps, and for
+                              every HEX08 solve that of the FP64 sweep (1 or 3 CTAs per SM);
+                              cached per device and size class (dtc_get_kernel_stats lists the
+                              timings as autotune_* classes) */
   int32_t inner_precond;   /* preconditioner of the FP32 inner solve: 0 = Jacobi (as PETSc's
                               PCJACOBI), 1 = node-block Jacobi (3x3 diagonal blocks),
                               2 = multigrid V-cycle on halved voxel grids (HEX20 domains are
@@ -106,10 +110,10 @@ typedef struct dtc_options {
                               element, 60 load cases (init_displ_hexe20, mod_write_deck.f90:118-279;
                               the quadratic load-case matrix, mod_struct_calcmat.f90:1780-2028, with
                               its typing defects repaired; quad face sums :368-401).  Order 2 solves
-                              the 60 load cases as three passes of 24 columns, forms ff by the
-                              reference's reaction projection (tensor_estimator must be 0), needs
-                              dtc_domain_out.macro2 on every record, and has no adjoint
-                              (keep_displacements must be 0) */
+                              the 60 load cases as three passes of 24 columns (with the energy
+                              estimator the solutions of the first two stay on the device for the
+                              60 x 60 Gram matrix), needs dtc_domain_out.macro2 on every record,
+                              and has no adjoint (keep_displacements must be 0) */
 } dtc_options;
 
 typedef struct dtc_domain_in {

@@ -105,7 +105,11 @@ void quirk_correction(const dtc_domain_in& in, const MeshPlan& mp, double nu, in
   }
 }
 
-int64_t device_bytes_per_node() { return 72 * (4 * 8 + 4 * 4) + 64; }
+// device bytes per node of a pass: four FP64 and four FP32 nodal vectors and per-node data;
+// macro order 2 with the energy estimator keeps two more FP64 solutions (the earlier column passes)
+int64_t device_bytes_per_node(const dtc_options& o) {
+  return 72 * (4 * 8 + 4 * 4) + 64 + (o.macro_order == 2 && o.tensor_estimator == 1 ? 2 * 72 * 8 : 0);
+}
 
 }  // namespace
 
@@ -149,9 +153,8 @@ dtc_status dtc_create(dtc_handle** handle, const dtc_options* opt) {
       o.graph_chunks > 1 || o.device_mesher < 0 || o.device_mesher > 1 || o.macro_order < 0 || o.macro_order > 2)
     return DTC_ERR_INVALID_ARGUMENT;
   if (o.macro_order == 0) o.macro_order = 1;
-  // macro order 2: the reaction projection of the reference (the energy products would couple
-  // the three column passes) and no adjoint (it is derived for the 24 linear load cases)
-  if (o.macro_order == 2 && (o.tensor_estimator != 0 || o.keep_displacements != 0)) return DTC_ERR_INVALID_ARGUMENT;
+  // macro order 2 has no adjoint (it is derived for the 24 linear load cases)
+  if (o.macro_order == 2 && o.keep_displacements != 0) return DTC_ERR_INVALID_ARGUMENT;
   dtc_handle* h = new (std::nothrow) dtc_handle();
   if (!h) return DTC_ERR_OUT_OF_MEMORY;
   h->opt = o;
@@ -296,7 +299,7 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     for (int64_t k = 0; k < n; ++k) {
       const dtc_domain_in& d = in[k];
       const int mg = d.elem_type == DTC_HEX20 ? 2 : 1;   // HEX20 nodes live on the doubled grid
-      const double nb = (double)(mg * d.L[0] + 1) * (mg * d.L[1] + 1) * (mg * d.L[2] + 1) * device_bytes_per_node();
+      const double nb = (double)(mg * d.L[0] + 1) * (mg * d.L[1] + 1) * (mg * d.L[2] + 1) * device_bytes_per_node(h->opt);
       const int64_t cnt = k - cuts.back();
       const bool full = (h->opt.chunk_domains > 0 && cnt >= h->opt.chunk_domains) ||
                         (pipe > 0 && cuts.size() == 1 && cnt >= pipe);

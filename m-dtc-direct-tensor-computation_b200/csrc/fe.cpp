@@ -364,18 +364,20 @@ void homogenise(int order, const double* ff, const int64_t L[3], const double de
   out->sym_ee = symmetry_deviation(6, out->ee);
 }
 
-void energy_to_ff(const double gram[576], double ff[576]) {
-  double uu[8 * 3 * 24], vv[576];
-  macro_modes(1e-6, uu);
-  for (int lc = 0; lc < 24; ++lc)
+void energy_to_ff(int order, const double* gram, double* ff) {
+  const int nm = macro_nodes(order), nl = macro_loadcases(order);
+  // the load-case matrix of the modes actually prescribed (eps = 1e-6, mod_write_deck.f90:61)
+  std::vector<double> uu((size_t)nm * 3 * nl), vv((size_t)nl * nl);
+  macro_modes_of_order(order, 1e-6, uu.data());
+  for (int lc = 0; lc < nl; ++lc)
     for (int k = 0; k < 3; ++k)
-      for (int l = 0; l < 8; ++l) vv[(8 * k + l) + 24 * lc] = uu[l + 8 * k + 24 * lc];
-  gauss_jordan_inverse(24, vv);
-  for (int lc = 0; lc < 24; ++lc)
-    for (int r = 0; r < 24; ++r) {
+      for (int l = 0; l < nm; ++l) vv[(nm * k + l) + (size_t)nl * lc] = uu[l + nm * k + (size_t)nl * lc];
+  gauss_jordan_inverse(nl, vv.data());
+  for (int lc = 0; lc < nl; ++lc)
+    for (int r = 0; r < nl; ++r) {
       double s = 0.0;
-      for (int a = 0; a < 24; ++a) s += vv[a + 24 * r] * gram[a + 24 * lc];
-      ff[r + 24 * lc] = s;
+      for (int a = 0; a < nl; ++a) s += vv[a + (size_t)nl * r] * gram[a + (size_t)nl * lc];
+      ff[r + (size_t)nl * lc] = s;
     }
 }
 

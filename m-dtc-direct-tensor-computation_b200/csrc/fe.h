@@ -53,11 +53,11 @@ void loadcase_matrix(int order, double e, double* vv);
 void homogenise(int order, const double* ff, const int64_t L[3], const double delta[3], double rve_strain,
                 dtc_domain_out* out);
 
-// Domain forces from the energy products M(a,b) = u_a^T K u_b of the 24 load-case solutions:
+// Domain forces from the energy products M(a,b) = u_a^T K u_b of the nl load-case solutions:
 // ff(r, lc) = sum_a vvbc^-1(a, r) M(a, lc), vvbc the load-case matrix of the boundary modes
 // actually prescribed (eps = 1e-6, mod_write_deck.f90:61).  Equal to the reaction projection
-// (mod_struct_calcmat.f90:254-280) at the exact solution.
-void energy_to_ff(const double gram[576], double ff[576]);
+// (mod_struct_calcmat.f90:254-280) at the exact solution.  gram and ff are nl x nl.
+void energy_to_ff(int order, const double* gram, double* ff);
 
 // Rotation search results -> output record (mod_struct_calcmat.f90:1014-1137, 1462-1603):
 // ang = argmin indices in units of 10^-jj degree, jj = refinement iterations.

@@ -216,9 +216,10 @@ template <> struct Win<float, true> : Win<float, false> {
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
 // node of the grid (reaction forces).
-// FP32: at most 128 registers (4 CTAs of 128 threads per SM)
-template <typename T, bool ALL, bool DOT>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_matvec(const Tile* __restrict__ tiles,
+// MINB: CTAs per SM the register allocation is sized for; FP32 4 (at most 128 registers) or 5,
+// FP64 1 (255) or 3 (168), chosen per batch class by the sweep autotuner
+template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 4 : 1)>
+__global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restrict__ tiles,
                                                                           const DomDev* __restrict__ doms,
                                                      const float* __restrict__ svox, const T* __restrict__ u,
                                                      T* __restrict__ y, double scale, double* __restrict__ acc,
@@ -835,15 +836,17 @@ __global__ void __launch_bounds__(kThreads) k_project(const Tile* __restrict__ t
   }
 }
 
-// Energy products M(a,b) = u_a . (K u_b) over all nodes, 24 x 24 per domain (FP64).  With
+// Energy products M(a,b) = u_a . (K u_b) over all nodes, per domain (FP64).  With
 // F = K u from the reaction pass, M is the Gram matrix of the load-case solutions in the
 // stiffness inner product; ff = vv^-T M equals the reaction projection at the exact solution
-// and its error is quadratic in the solution error.
+// and its error is quadratic in the solution error.  gram is ldg x ldg per domain; X holds the
+// load cases row0.. of the block rows, F those of the block columns col0.. (the column passes of
+// macro order 2 fill a 72 x 72 Gram block by block).
 __global__ void __launch_bounds__(kThreads) k_energy_gram(const Tile* __restrict__ tiles,
                                                           const DomDev* __restrict__ doms,
                                                           const uint8_t* __restrict__ flags,
                                                           const double* __restrict__ X, const double* __restrict__ F,
-                                                          double* __restrict__ gram) {
+                                                          double* __restrict__ gram, int ldg, int row0, int col0) {
   __shared__ double part[16][8][25];
   const Tile t = tiles[blockIdx.x / 3];
   const DomDev D = doms[t.dom];
@@ -876,7 +879,7 @@ __global__ void __launch_bounds__(kThreads) k_energy_gram(const Tile* __restrict
     double sum = 0.0;
     for (int r2 = 0; r2 < 16; ++r2) sum += part[r2][l8][a];
     const int bg = (blockIdx.x % 3) * kLcGroup + l8;
-    atomicAdd(gram + (int64_t)t.dom * 576 + a + 24 * bg, sum);
+    atomicAdd(gram + (int64_t)t.dom * ldg * ldg + (row0 + a) + (int64_t)ldg * (col0 + bg), sum);
   }
 }
 
@@ -952,7 +955,7 @@ enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, b
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
            bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF,
-           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bMgNodes, bMgNodesC, bNumBufs };
+           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bMgNodes, bMgNodesC, bXkeep, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -1050,6 +1053,8 @@ struct Work {
   const float* ke32;
   const float* ke20tc;  // HEX20 FP32 applications on tcgen05: split matrix in the B layout, else null
   int* err;             // mbarrier time-out flag of the tensor-core kernels
+  int minb32 = 4;       // HEX08 slab sweeps: CTAs per SM of the FP32 CG application (4 or 5)
+  int minb64 = 1;       //                    and of every FP64 application (1 or 3)
 };
 
 // y = scale * K u on the interior (ALL = false) or every node; DOT: acc[col] += u . y.
@@ -1058,8 +1063,16 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
              double* acc, const int* act, cudaStream_t s) {
   if constexpr (NEN == 8) {
     const int64_t nt = ALL ? W.nta : W.nti;
-    if (nt > 0)
-      k_matvec<T, ALL, DOT><<<(unsigned)(3 * nt), kThreads, 0, s>>>(ALL ? W.ta : W.ti, dd, svox, u, y, scale, acc, act);
+    if (nt <= 0) return;
+    const unsigned g = (unsigned)(3 * nt);
+    const Tile* tl = ALL ? W.ta : W.ti;
+    if constexpr (sizeof(T) == 4) {
+      if (W.minb32 == 5) k_matvec<T, ALL, DOT, 5><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
+      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
+    } else {
+      if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
+      else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
+    }
   } else {
     const T* ke;
     if constexpr (sizeof(T) == 8) ke = W.ke64;
@@ -1397,7 +1410,17 @@ struct MgDev {
   const float* ke32;     // HEX20 unit element matrix (FP32)
   const float* ke20tc;   // its tensor-core operand, or null (brick SIMT kernel)
   int* err;
+  int minb_res = 4, minb_post = 4;   // HEX08 fine-level residual / post-smoothing sweeps: CTAs per SM
 };
+
+// The fine-level HEX08 residual and post-smoothing sweeps with the tuned register budget.
+template <int MODE, bool DOT>
+void launch_mg_matvec(int minb, unsigned g, cudaStream_t s, const Tile* t, const DomDev* d, const float* sv,
+                      const float* bi, const float* b, const float* u, float* y, float om, double* a1, double* a2,
+                      const int* act) {
+  if (minb == 5) k_mg_matvec<MODE, DOT, 5><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act);
+  else k_mg_matvec<MODE, DOT, 4><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act);
+}
 
 // t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_flat)
 void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, double* zz, double* zr, const int* act,
@@ -1465,6 +1488,8 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
     ++launches;
   } else if (fine && I.tensor_matvec) {
     launch_sweep_tc(kTcRes, tsm, nsm, dl, sv, fl, bi, b, cur, rbuf, 1.0f, om, nullptr, nullptr, act, M.err, s);
+  } else if (fine) {
+    launch_mg_matvec<kMgRes, false>(M.minb_res, g, s, tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   } else {
     k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   }
@@ -1501,7 +1526,7 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   } else if (l == 0 && I.tensor_matvec)
     launch_sweep_tc(kTcPost, tsm, nsm, dl, sv, fl, bi, b, t, z, 1.0f, P.omega0, zz, zr, act, M.err, s);
   else if (l == 0)
-    k_mg_matvec<kMgPost, true><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
+    launch_mg_matvec<kMgPost, true>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
   else if (twice) {
     // z holds the corrected iterate: t = z + w D^-1 (b - K z), then z = t + w D^-1 (b - K t)
     k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, z, t, P.omega, nullptr, nullptr, act);
@@ -1846,7 +1871,11 @@ struct TuneKey {
 };
 struct TuneResult {
   int pick;            // 0 = SIMT, 1 = tensor cores
-  float ms[2];         // the timed launches of each candidate
+  float ms[2];         // the timed launches of each candidate (post-smoothing; SIMT at 4 CTAs/SM)
+  // HEX08 SIMT slab sweeps: CTAs per SM of the residual, post-smoothing and CG application
+  // sweeps, and the timed launches at 4 and 5 CTAs per SM (index 0 / 1)
+  int minb[3] = {4, 4, 4};
+  float shape_ms[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneResult> g_tune_choice;
@@ -1858,14 +1887,37 @@ void record_tuning(SolverStats& st, const TuneResult& r) {
   st.kc[kcTuneSimt].ms += r.ms[0];
   st.kc[kcTuneTc].launches += kTuneReps;
   st.kc[kcTuneTc].ms += r.ms[1];
+  const int cls[3][2] = {{kcTuneRes4, kcTuneRes5}, {kcTuneSimt, kcTunePost5}, {kcTuneApply4, kcTuneApply5}};
+  for (int k = 0; k < 3; ++k)
+    for (int v = 0; v < 2; ++v)
+      if (r.shape_ms[k][v] > 0.f && !(k == 1 && v == 0)) {
+        st.kc[cls[k][v]].launches += kTuneReps;
+        st.kc[cls[k][v]].ms += r.shape_ms[k][v];
+      }
 }
 
-// HEX20 fine levels: the SIMT brick kernel and the tcgen05 brick kernel apply K to the fine
-// multigrid vector on the interior bricks (the operator of the residual and post-smoothing
-// steps and of the CG application).
-int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const MgDev& M,
-                   const std::vector<DomDev>& doms, const std::vector<float>& svox, int nen, std::string& msg) {
-  cudaStream_t s = I.stream;
+// CUDA-event time of kTuneReps launches after one untimed launch.
+template <class F>
+int time_launches(cudaStream_t s, F&& launch, float& ms, std::string& msg) {
+  cudaEvent_t ev[2];
+  DTC_CUDA(cudaEventCreate(&ev[0]));
+  DTC_CUDA(cudaEventCreate(&ev[1]));
+  launch();
+  cudaEventRecord(ev[0], s);
+  for (int r = 0; r < kTuneReps; ++r) launch();
+  cudaEventRecord(ev[1], s);
+  const cudaError_t ec = cudaEventSynchronize(ev[1]);
+  if (ec == cudaSuccess) cudaEventElapsedTime(&ms, ev[0], ev[1]);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (ec != cudaSuccess) {
+    msg = std::string("autotune: ") + cudaGetErrorString(ec);
+    return DTC_ERR_CUDA;
+  }
+  return launch_check(msg);
+}
+
+TuneKey tune_key(int device, int nen, const std::vector<DomDev>& doms, const std::vector<float>& svox) {
   std::vector<int> Ls;
   for (const DomDev& D : doms) Ls.push_back(std::max(D.L[0], std::max(D.L[1], D.L[2])));
   std::nth_element(Ls.begin(), Ls.begin() + Ls.size() / 2, Ls.end());
@@ -1873,14 +1925,33 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const 
   int64_t kept = 0;
   for (float v : svox) kept += v != 0.0f;
   const double frac = svox.empty() ? 0.0 : (double)kept / (double)svox.size();
-  const TuneKey key{I.device, nen, (int)std::lround(4.0 * std::log2(std::max(lmed, 1))),
-                    frac < 0.15 ? 0 : frac < 0.30 ? 1 : 2};
+  return TuneKey{device, nen, (int)std::lround(4.0 * std::log2(std::max(lmed, 1))), frac < 0.15 ? 0 : frac < 0.30 ? 1 : 2};
+}
+
+// The fine-level operator of an FP32 multigrid solve, chosen per device, element type and size
+// class (median domain edge in quarter octaves, kept-voxel fraction below 0.15 / 0.30 / above)
+// by CUDA-event timings on the batch's own tiles and vectors:
+//  * HEX08: the SIMT slab sweep or the tcgen05 sweep (timed on the post-smoothing sweep); for
+//    the SIMT sweep also the register budget of each of its three kernels -- residual,
+//    post-smoothing, CG application -- at 4 CTAs per SM (128 registers) or 5 (102);
+//  * HEX20: the SIMT brick kernel or the tcgen05 brick kernel (the operator of the residual and
+//    post-smoothing steps and of the CG application).
+int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, const std::vector<DomDev>& doms,
+                   const std::vector<float>& svox, int nen, std::string& msg) {
+  cudaStream_t s = I.stream;
+  const TuneKey key = tune_key(I.device, nen, doms, svox);
+  auto adopt = [&](const TuneResult& r) {
+    I.tensor_matvec = r.pick == 1;
+    M.minb_res = r.minb[0];
+    M.minb_post = r.minb[1];
+    W.minb32 = r.minb[2];
+    record_tuning(st, r);
+  };
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune_choice.find(key);
     if (it != g_tune_choice.end()) {
-      I.tensor_matvec = it->second.pick == 1;
-      record_tuning(st, it->second);
+      adopt(it->second);
       return DTC_OK;
     }
   }
@@ -1890,11 +1961,9 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const 
   const float* b = B<float>(I, bR32);
   double* zz = B<double>(I, bZz);
   double* zr = B<double>(I, bZr);
-  cudaEvent_t ev[2];
-  DTC_CUDA(cudaEventCreate(&ev[0]));
-  DTC_CUDA(cudaEventCreate(&ev[1]));
-  float ms[2] = {0.f, 0.f};
-  const int reps = kTuneReps;
+  const unsigned g = (unsigned)(3 * nsm);
+  TuneResult r{0, {0.f, 0.f}};
+  int e;
   for (int cand = 0; cand < 2; ++cand) {
     auto launch = [&]() {
       if (nen == 20) {
@@ -1905,34 +1974,83 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, const Work& W, const 
           launch_ebe_tc(M.bricks0, M.nbricks0, M.doms0, M.svox0, M.flags0, W.ke20tc, M.t0, M.z0, -1.0, nullptr,
                         nullptr, M.err, s);
       } else if (cand == 0) {
-        k_mg_matvec<kMgPost, true><<<(unsigned)(3 * nsm), kThreads, 0, s>>>(tsm, M.doms0, M.svox0, M.binv0, b, M.t0,
-                                                                           M.z0, M.P->omega0, zz, zr, nullptr);
+        k_mg_matvec<kMgPost, true, 4><<<g, kThreads, 0, s>>>(tsm, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0,
+                                                             M.P->omega0, zz, zr, nullptr);
       } else {
         launch_sweep_tc(kTcPost, tsm, nsm, M.doms0, M.svox0, M.flags0, M.binv0, b, M.t0, M.z0, 1.0f, M.P->omega0, zz,
                         zr, nullptr, M.err, s);
       }
     };
-    launch();
-    cudaEventRecord(ev[0], s);
-    for (int r = 0; r < reps; ++r) launch();
-    cudaEventRecord(ev[1], s);
-    const cudaError_t ec = cudaEventSynchronize(ev[1]);
-    if (ec != cudaSuccess) {
-      cudaEventDestroy(ev[0]);
-      cudaEventDestroy(ev[1]);
-      msg = std::string("autotune: ") + cudaGetErrorString(ec);
-      return DTC_ERR_CUDA;
-    }
-    cudaEventElapsedTime(&ms[cand], ev[0], ev[1]);
+    if ((e = time_launches(s, launch, r.ms[cand], msg))) return e;
   }
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
-  if (int e = launch_check(msg)) return e;
-  const TuneResult r{ms[1] < ms[0] ? 1 : 0, {ms[0], ms[1]}};
-  I.tensor_matvec = r.pick == 1;
-  record_tuning(st, r);
+  r.pick = r.ms[1] < r.ms[0] ? 1 : 0;
+  if (nen == 8 && r.pick == 0) {
+    // register budgets of the three SIMT sweeps (the post-smoothing at 4 CTAs/SM is ms[0])
+    r.shape_ms[1][0] = r.ms[0];
+    for (int v = 0; v < 2; ++v) {
+      const int minb = 4 + v;
+      auto res = [&]() {
+        launch_mg_matvec<kMgRes, false>(minb, g, s, tsm, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0,
+                                        nullptr, nullptr, nullptr);
+      };
+      if ((e = time_launches(s, res, r.shape_ms[0][v], msg))) return e;
+      if (v == 1) {
+        auto post = [&]() {
+          launch_mg_matvec<kMgPost, true>(minb, g, s, tsm, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0, zz,
+                                          zr, nullptr);
+        };
+        if ((e = time_launches(s, post, r.shape_ms[1][v], msg))) return e;
+      }
+      Work Wv = W;
+      Wv.minb32 = minb;
+      auto apply = [&]() {
+        apply_k<float, 8, false, true>(Wv, M.doms0, M.svox0, M.flags0, M.t0, M.z0, 1.0, zz, nullptr, s);
+      };
+      if ((e = time_launches(s, apply, r.shape_ms[2][v], msg))) return e;
+    }
+    for (int k = 0; k < 3; ++k) r.minb[k] = r.shape_ms[k][1] < r.shape_ms[k][0] ? 5 : 4;
+  }
+  adopt(r);
   std::lock_guard<std::mutex> lock(g_tune_mu);
   g_tune_choice[key] = r;
+  return DTC_OK;
+}
+
+// The register budget of the HEX08 FP64 slab sweep (outer residual, reactions, plain FP64 CG):
+// 1 CTA per SM (255 registers) or 3 (168), timed on the batch's interior tiles (X -> R64, which
+// the solve overwrites next), cached per class like the FP32 choice.
+struct Tune64 { int minb; float ms[2]; };
+std::map<TuneKey, Tune64> g_tune64;
+
+int autotune_fp64(DeviceSolver::Impl& I, SolverStats& st, Work& W, const std::vector<DomDev>& doms,
+                  const std::vector<float>& svox, const double* X, double* R64, std::string& msg) {
+  const TuneKey key = tune_key(I.device, 8, doms, svox);
+  Tune64 r{1, {0.f, 0.f}};
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune64.find(key);
+    if (it != g_tune64.end()) { r = it->second; cached = true; }
+  }
+  if (!cached && W.nti > 0) {
+    for (int v = 0; v < 2; ++v) {
+      Work Wv = W;
+      Wv.minb64 = v == 0 ? 1 : 3;
+      auto launch = [&]() {
+        apply_k<double, 8, false, false>(Wv, B<DomDev>(I, bDoms), B<float>(I, bSvox), B<uint8_t>(I, bFlags), X, R64,
+                                         -1.0, nullptr, nullptr, I.stream);
+      };
+      if (int e = time_launches(I.stream, launch, r.ms[v], msg)) return e;
+    }
+    r.minb = r.ms[1] < r.ms[0] ? 3 : 1;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune64[key] = r;
+  }
+  W.minb64 = r.minb;
+  for (int v = 0; v < 2; ++v) {
+    st.kc[v == 0 ? kcTuneF64a : kcTuneF64b].launches += kTuneReps;
+    st.kc[v == 0 ? kcTuneF64a : kcTuneF64b].ms += r.ms[v];
+  }
   return DTC_OK;
 }
 
@@ -2108,7 +2226,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
                                              "project_f64", "mg_jacobi_f32", "mg_residual_f32",
                                              "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
                                              "rotation_search_f64", "autotune_simt_sweep", "autotune_tc_sweep",
-                                             "host_pack", "host_multigrid_build"};
+                                             "autotune_res_sweep_4cta", "autotune_res_sweep_5cta",
+                                             "autotune_post_sweep_5cta", "autotune_apply_sweep_4cta",
+                                             "autotune_apply_sweep_5cta", "autotune_f64_sweep_1cta",
+                                             "autotune_f64_sweep_3cta", "host_pack", "host_multigrid_build"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
@@ -2222,7 +2343,12 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   const int order = opt.macro_order == 2 ? 2 : 1;
   const int nm = macro_nodes(order), nl = macro_loadcases(order);
   const int ncp = (nl + kNLC - 1) / kNLC;
-  if ((e = ensure(I, bFf, sizeof(double) * nl * nl * ndom, msg))) return e;
+  // the energy estimator's Gram matrix is ldg x ldg per domain (the passes' 24-column blocks);
+  // the solutions of every pass but the last stay on the device for the cross-pass blocks
+  const bool energy = opt.tensor_estimator == 1;
+  const int ldg = kNLC * ncp;
+  if ((e = ensure(I, bFf, sizeof(double) * std::max(nl * nl, energy ? ldg * ldg : 0) * ndom, msg))) return e;
+  if (energy && ncp > 1 && (e = ensure(I, bXkeep, vbytes64 * (ncp - 1), msg))) return e;
   if ((e = ensure(I, bErr, sizeof(int), msg))) return e;
   DTC_CUDA(cudaMemsetAsync(I.bufs[bErr], 0, sizeof(int), s));
 
@@ -2244,14 +2370,13 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv32], 0, sizeof(float) * node_total * 3, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bX], 0, vbytes64, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bR64], 0, vbytes64, s));
-  DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * nl * nl * ndom, s));
+  DTC_CUDA(cudaMemsetAsync(I.bufs[bFf], 0, sizeof(double) * std::max(nl * nl, energy ? ldg * ldg : 0) * ndom, s));
   // device time of the solve, inputs resident: from here (voxel factors and work lists
   // uploaded) to the last kernel, measured with CUDA events on the solver stream
   if (!I.ev_solve[0]) {
     DTC_CUDA(cudaEventCreate(&I.ev_solve[0]));
     DTC_CUDA(cudaEventCreate(&I.ev_solve[1]));
   }
-  DTC_CUDA(cudaEventRecord(I.ev_solve[0], s));
   const Tile* ti = B<Tile>(I, bTilesI);
   const Tile* ta = B<Tile>(I, bTilesA);
   const double* ke64 = NEN == 20 ? B<double>(I, bKe20) : nullptr;
@@ -2264,6 +2389,10 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   double* X = B<double>(I, bX);
   double* R64 = B<double>(I, bR64);
   int64_t& L = stats_.kernel_launches;
+  // the FP64 sweep's register budget (its cost does not depend on the values: X is zero here,
+  // R64 is scratch), before the solve's device time starts
+  if (tune && NEN == 8 && (e = autotune_fp64(I, stats_, W, doms, svox, X, R64, msg))) return e;
+  DTC_CUDA(cudaEventRecord(I.ev_solve[0], s));
   if (nta) {
     DTC_CUDA(cudaMemsetAsync(I.bufs[bBinv32], 0, sizeof(float) * node_total * 6, s));
     k_node_setup<NEN><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
@@ -2464,9 +2593,17 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
     if (nta) {
       apply_k<double, NEN, true, false>(W, dd, B<float>(I, bSvox), fl, X, R64, 1.0, nullptr, nullptr, s);
-      if (opt.tensor_estimator == 1)
-        k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf));
-      else if (order == 2)
+      if (energy) {
+        k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf), ldg, kNLC * cp, kNLC * cp);
+        for (int q = 0; q < cp; ++q) {   // u_q . K u_cp against the kept solutions of earlier passes
+          k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, B<double>(I, bXkeep) + (size_t)q * (vbytes64 / 8), R64,
+                                                B<double>(I, bFf), ldg, kNLC * q, kNLC * cp);
+          ++L;
+        }
+        if (cp + 1 < ncp)
+          DTC_CUDA(cudaMemcpyAsync(B<double>(I, bXkeep) + (size_t)cp * (vbytes64 / 8), X, vbytes64,
+                                   cudaMemcpyDeviceToDevice, s));
+      } else if (order == 2)
         k_project<20><<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf), cp * kNLC);
       else
         k_project<8><<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf), 0);
@@ -2501,7 +2638,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     }
   }
   DTC_CUDA(cudaEventRecord(I.ev_solve[1], s));
-  std::vector<double> ff((size_t)nl * nl * ndom);
+  const size_t per_dom = (size_t)std::max(nl * nl, energy ? ldg * ldg : 0);
+  std::vector<double> ff(per_dom * ndom);
   DTC_CUDA(cudaMemcpyAsync(ff.data(), I.bufs[bFf], sizeof(double) * ff.size(), cudaMemcpyDeviceToHost, s));
   int h_err = 0;
   DTC_CUDA(cudaMemcpyAsync(&h_err, I.bufs[bErr], sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -2518,8 +2656,17 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DomainTask& t = tasks[tidx[d]];
     dtc_domain_out* o = t.out;
     double* off = order == 2 ? o->macro2->ff : o->ff;
-    if (opt.tensor_estimator == 1) energy_to_ff(&ff[(size_t)576 * d], off);
-    else std::memcpy(off, &ff[(size_t)nl * nl * d], sizeof(double) * nl * nl);
+    if (energy) {
+      // the Gram blocks below the diagonal pass blocks are the transposes of those above
+      std::vector<double> gram((size_t)nl * nl);
+      const double* gd = &ff[per_dom * d];
+      for (int b = 0; b < nl; ++b)
+        for (int a = 0; a < nl; ++a)
+          gram[a + (size_t)nl * b] = (a / kNLC <= b / kNLC) ? gd[a + (size_t)ldg * b] : gd[b + (size_t)ldg * a];
+      energy_to_ff(order, gram.data(), off);
+    } else {
+      std::memcpy(off, &ff[per_dom * d], sizeof(double) * nl * nl);
+    }
     int64_t* iters = order == 2 ? o->macro2->iters : o->iters;
     double* relres = order == 2 ? o->macro2->relres : o->relres;
     int worst = DTC_DOMAIN_OK;

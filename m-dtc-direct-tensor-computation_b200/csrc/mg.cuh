@@ -50,8 +50,9 @@ __device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __
 // Residual / smoother on one level's interior tiles (the slab sweep of k_matvec).
 //   kMgRes : y = b - K u
 //   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
-template <int MODE, bool DOT>
-__global__ void __launch_bounds__(kThreads, 4) k_mg_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
+// MINB: CTAs per SM the register allocation is sized for (4: at most 128 registers; 5: 102)
+template <int MODE, bool DOT, int MINB = 4>
+__global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                         const float* __restrict__ svox,
                                                         const float* __restrict__ binv, const float* __restrict__ b,
                                                         const float* __restrict__ u, float* __restrict__ y, float omega,

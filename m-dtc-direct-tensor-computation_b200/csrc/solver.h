@@ -84,7 +84,8 @@ struct KernelClass {
 
 enum KClassId { kcMatvec32, kcMatvec64, kcUpdate32, kcUpdate64, kcDirection32, kcDirection64, kcColstate,
                 kcReaction, kcProject, kcMgJacobi, kcMgResidual, kcMgPost, kcMgTransfer, kcMgCoarse,
-                kcRotation, kcTuneSimt, kcTuneTc, kcHostPack, kcHostMgBuild,
+                kcRotation, kcTuneSimt, kcTuneTc, kcTuneRes4, kcTuneRes5, kcTunePost5, kcTuneApply4, kcTuneApply5,
+                kcTuneF64a, kcTuneF64b, kcHostPack, kcHostMgBuild,
                 kcNumClasses };   // the last two: host phases (wall ms)
 
 struct SolverStats {

@@ -87,11 +87,11 @@ def test_create_reports_missing_device_or_abi(dtc):
 
 
 def test_macro_order_option_validation(dtc):
-    """Macro order 2 takes the reference's reaction projection and has no adjoint: other
-    combinations are refused before any device is touched."""
+    """Macro order 1 or 2, and no adjoint for macro order 2: other combinations are refused
+    before any device is touched."""
     lib = dtc.capi.load()
     h = C.c_void_p()
-    for order, est, keep in ((3, 0, 0), (-1, 0, 0), (2, 1, 0), (2, 0, 1)):
+    for order, est, keep in ((3, 0, 0), (-1, 0, 0), (2, 0, 1), (2, 1, 1)):
         o = dtc.capi.Options()
         lib.dtc_default_options(C.byref(o))
         o.macro_order, o.tensor_estimator, o.keep_displacements = order, est, keep

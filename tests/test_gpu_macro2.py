@@ -68,6 +68,18 @@ def test_hex08_macro_order2_matches_oracle(dtc, hex08, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_macro_order2_energy_estimator_matches_oracle(dtc, hex08, precision):
+    """ff from the 60 x 60 energy products u_a^T K u_b, whose blocks couple the three column
+    passes (the solutions of the earlier passes stay on the device)."""
+    pairs, refs = hex08
+    kw = {"inner_precond": "mg"} if precision == "mixed" else {}
+    with dtc.Solver(precision=precision, rtol=1e-10, rotation_search=False, macro_order=2, estimator="energy",
+                    **kw) as s:
+        res = s.solve([p[0] for p in pairs])
+    check(res, refs, TOL_FP64 if precision == "fp64" else TOL_MIXED, precision == "fp64")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_hex20_macro_order2_matches_oracle(dtc, hex20, precision):
     pairs, refs = hex20
     kw = {"inner_precond": "mg"} if precision == "mixed" else {}
