@@ -908,6 +908,17 @@ struct DeviceSolver::Impl {
   double adj_nu = 0.3;
   bool tensor_matvec = false;   // FP32 inner solve on tcgen05
   bool graphs = true;           // replay CG chunks as CUDA graphs
+  // Voxel factors of the next device pass, uploaded while the current one solves: pinned host
+  // staging and device slots alternating between passes, copied on their own stream; svox_dev
+  // is the slot of the pass being solved (null: the synchronously uploaded bufs[bSvox]).
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t up_ev[2] = {nullptr, nullptr};
+  float* up_pin[2] = {nullptr, nullptr};
+  float* up_dev[2] = {nullptr, nullptr};
+  size_t up_cap[2] = {0, 0};
+  int up_next = 0;
+  float* svox_dev = nullptr;
+  float* svox() const { return svox_dev ? svox_dev : static_cast<float*>(bufs[3]); }
   cudaEvent_t ev_solve[2] = {nullptr, nullptr};
   // kernel profiling with CUDA events (opt-in)
   bool profile = false;
@@ -957,6 +968,7 @@ enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, b
            bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF,
            bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bMgNodes, bMgNodesC, bXkeep, bNumBufs };
 static_assert(bNumBufs <= 64, "buffer table");
+static_assert(bSvox == 3, "DeviceSolver::Impl::svox() reads bufs[3]");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
   if (I.caps[which] >= bytes && I.bufs[which]) return DTC_OK;
@@ -984,6 +996,13 @@ DeviceSolver::~DeviceSolver() {
     for (cudaEvent_t e : impl_->ev) cudaEventDestroy(e);
     for (cudaEvent_t e : impl_->ev_solve) if (e) cudaEventDestroy(e);
     for (void* b : impl_->bufs) if (b) cudaFree(b);
+    for (int k = 0; k < 2; ++k) {
+      if (impl_->up_ev[k]) cudaEventSynchronize(impl_->up_ev[k]);
+      if (impl_->up_pin[k]) cudaFreeHost(impl_->up_pin[k]);
+      if (impl_->up_dev[k]) cudaFree(impl_->up_dev[k]);
+      if (impl_->up_ev[k]) cudaEventDestroy(impl_->up_ev[k]);
+    }
+    if (impl_->up_stream) cudaStreamDestroy(impl_->up_stream);
     if (impl_->stream) cudaStreamDestroy(impl_->stream);
     delete impl_;
   }
@@ -1715,10 +1734,10 @@ int run_cg(DeviceSolver::Impl& I, int ndom, const Work& W, T* x, T* r, T* p, T* 
           I.end(f32 ? kcDirection32 : kcDirection64, q, 3 * vb, 0);
           q = I.begin(0);
           if (sizeof(T) == 4 && NEN == 8 && I.tensor_matvec)
-            launch_sweep_tc(kTcApply, ti, nti, dd, B<float>(I, bSvox), fl, nullptr, nullptr, (const float*)p,
+            launch_sweep_tc(kTcApply, ti, nti, dd, I.svox(), fl, nullptr, nullptr, (const float*)p,
                             (float*)w, 1.0f, 0.0f, pw, nullptr, act, B<int>(I, bErr), s);
           else
-            apply_k<T, NEN, false, true>(Wc, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
+            apply_k<T, NEN, false, true>(Wc, dd, I.svox(), fl, p, w, 1.0, pw, act, s);
           I.end(f32 ? kcMatvec32 : kcMatvec64, q, mb, mf);
           q = I.begin(0);
           k_update<T, BLOCK><<<grid, kThreads, 0, s>>>(ti, dd, fl, dinv, x, r, p, w, st, pw, zz, zr, act);
@@ -1811,10 +1830,10 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
           I.end(kcDirection32, q, 3 * vb, 0);
           q = I.begin(0);
           if (NEN == 8 && I.tensor_matvec)
-            launch_sweep_tc(kTcApply, Wc.ti, Wc.nti, dd, B<float>(I, bSvox), fl, nullptr, nullptr, p, w, 1.0f, 0.0f,
+            launch_sweep_tc(kTcApply, Wc.ti, Wc.nti, dd, I.svox(), fl, nullptr, nullptr, p, w, 1.0f, 0.0f,
                             pw, nullptr, act, B<int>(I, bErr), s);
           else
-            apply_k<float, NEN, false, true>(Wc, dd, B<float>(I, bSvox), fl, p, w, 1.0, pw, act, s);
+            apply_k<float, NEN, false, true>(Wc, dd, I.svox(), fl, p, w, 1.0, pw, act, s);
           I.end(kcMatvec32, q, mb, mf);
           q = I.begin(0);
           k_alpha<<<ndom, 32, 0, s>>>(st, pw, alphaf, act);
@@ -2037,7 +2056,7 @@ int autotune_fp64(DeviceSolver::Impl& I, SolverStats& st, Work& W, const std::ve
       Work Wv = W;
       Wv.minb64 = v == 0 ? 1 : 3;
       auto launch = [&]() {
-        apply_k<double, 8, false, false>(Wv, B<DomDev>(I, bDoms), B<float>(I, bSvox), B<uint8_t>(I, bFlags), X, R64,
+        apply_k<double, 8, false, false>(Wv, B<DomDev>(I, bDoms), I.svox(), B<uint8_t>(I, bFlags), X, R64,
                                          -1.0, nullptr, nullptr, I.stream);
       };
       if (int e = time_launches(I.stream, launch, r.ms[v], msg)) return e;
@@ -2066,6 +2085,7 @@ struct HostBatch {
   bool has_mg = false;
   MgPlan mg;
   double ms_pack = 0, ms_mg = 0;
+  int up_slot = -1;   // device slot its voxel factors were uploaded to (DeviceSolver::upload_voxels)
 };
 void HostBatchDeleter::operator()(HostBatch* p) const { delete p; }
 
@@ -2312,7 +2332,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   if ((e = ensure(I, bTilesA, sizeof(Tile) * std::max<int64_t>(nta, 1), msg))) return e;
   if ((e = ensure(I, bBricksI, sizeof(Tile) * std::max<int64_t>(nbi, 1), msg))) return e;
   if ((e = ensure(I, bBricksA, sizeof(Tile) * std::max<int64_t>(nba, 1), msg))) return e;
-  if ((e = ensure(I, bSvox, sizeof(float) * svox.size(), msg))) return e;
+  I.svox_dev = nullptr;
+  if (hb.up_slot < 0 && (e = ensure(I, bSvox, sizeof(float) * svox.size(), msg))) return e;
   if ((e = ensure(I, bFlags, node_total, msg))) return e;
   if ((e = ensure(I, bDinv64, sizeof(double) * node_total * 3, msg))) return e;
   if ((e = ensure(I, bDinv32, sizeof(float) * node_total * 3, msg))) return e;
@@ -2364,7 +2385,12 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     DTC_CUDA(cudaMemcpyAsync(I.bufs[bNodesI], nodes_i.data(), sizeof(int64_t) * nodes_i.size(), cudaMemcpyHostToDevice,
                              s));
   if (nba) DTC_CUDA(cudaMemcpyAsync(I.bufs[bBricksA], bricks_a.data(), sizeof(Tile) * nba, cudaMemcpyHostToDevice, s));
-  DTC_CUDA(cudaMemcpyAsync(I.bufs[bSvox], svox.data(), sizeof(float) * svox.size(), cudaMemcpyHostToDevice, s));
+  if (hb.up_slot >= 0) {   // uploaded while the previous pass solved: order the solve after the copy
+    DTC_CUDA(cudaStreamWaitEvent(s, I.up_ev[hb.up_slot], 0));
+    I.svox_dev = I.up_dev[hb.up_slot];
+  } else {
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bSvox], svox.data(), sizeof(float) * svox.size(), cudaMemcpyHostToDevice, s));
+  }
   DTC_CUDA(cudaMemsetAsync(I.bufs[bFlags], 0, node_total, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv64], 0, sizeof(double) * node_total * 3, s));
   DTC_CUDA(cudaMemsetAsync(I.bufs[bDinv32], 0, sizeof(float) * node_total * 3, s));
@@ -2395,7 +2421,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaEventRecord(I.ev_solve[0], s));
   if (nta) {
     DTC_CUDA(cudaMemsetAsync(I.bufs[bBinv32], 0, sizeof(float) * node_total * 6, s));
-    k_node_setup<NEN><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, B<float>(I, bSvox), fl, B<double>(I, bDinv64),
+    k_node_setup<NEN><<<(unsigned)nta, kThreads, 0, s>>>(ta, dd, I.svox(), fl, B<double>(I, bDinv64),
                                                     B<float>(I, bDinv32), B<float>(I, bBinv32));
     ++L;
   }
@@ -2464,7 +2490,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     mgd.tiles = B<Tile>(I, bMgTiles);
     mgd.doms0 = dd;
     mgd.doms = B<DomDev>(I, bMgDoms);
-    mgd.svox0 = B<float>(I, bSvox);
+    mgd.svox0 = I.svox();
     mgd.svox = B<float>(I, bMgSvox);
     mgd.binv0 = B<float>(I, bBinv32);
     mgd.binv = B<float>(I, bMgBinv32);
@@ -2536,7 +2562,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
       DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
-      apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
+      apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s);
       ++L;
       if ((e = run_cg<double, false, NEN>(I, ndom, W, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
                               opt.rtol, nullptr, opt.max_it, L, msg)))
@@ -2556,7 +2582,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       for (int step = 0; step <= max_refine; ++step) {
         DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
         if (nti) {
-          apply_k<double, NEN, false, false>(W, dd, B<float>(I, bSvox), fl, X, R64, -1.0, nullptr, nullptr, s);
+          apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s);
           k_residual_norm<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<double>(I, bDinv64), R64, B<double>(I, bZz));
           L += 2;
         }
@@ -2592,7 +2618,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
     // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff)
     DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
     if (nta) {
-      apply_k<double, NEN, true, false>(W, dd, B<float>(I, bSvox), fl, X, R64, 1.0, nullptr, nullptr, s);
+      apply_k<double, NEN, true, false>(W, dd, I.svox(), fl, X, R64, 1.0, nullptr, nullptr, s);
       if (energy) {
         k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf), ldg, kNLC * cp, kNLC * cp);
         for (int q = 0; q < cp; ++q) {   // u_q . K u_cp against the kept solutions of earlier passes
@@ -2733,6 +2759,37 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
   HostBatchPtr batch;
   if (int e = prepare(tasks, opt, nu, batch, msg)) return e;
   return solve(tasks, opt, nu, std::move(batch), msg);
+}
+
+int DeviceSolver::upload_voxels(HostBatch* hb, std::string& msg) {
+  if (!hb || hb->nen == 0 || hb->svox.empty()) return DTC_OK;
+  Impl& I = *impl_;
+  DTC_CUDA(cudaSetDevice(I.device));
+  if (!I.up_stream) {
+    DTC_CUDA(cudaStreamCreateWithFlags(&I.up_stream, cudaStreamNonBlocking));
+    DTC_CUDA(cudaEventCreateWithFlags(&I.up_ev[0], cudaEventDisableTiming));
+    DTC_CUDA(cudaEventCreateWithFlags(&I.up_ev[1], cudaEventDisableTiming));
+  }
+  const int k = I.up_next;
+  const size_t n = hb->svox.size();
+  // the slot's last reader, the pass before the one now solving, has finished; its copy too
+  DTC_CUDA(cudaEventSynchronize(I.up_ev[k]));
+  if (I.up_cap[k] < n) {
+    if (I.up_pin[k]) cudaFreeHost(I.up_pin[k]);
+    if (I.up_dev[k]) cudaFree(I.up_dev[k]);
+    I.up_pin[k] = nullptr;
+    I.up_dev[k] = nullptr;
+    I.up_cap[k] = 0;
+    DTC_CUDA(cudaMallocHost(&I.up_pin[k], sizeof(float) * n));
+    DTC_CUDA(cudaMalloc(&I.up_dev[k], sizeof(float) * n));
+    I.up_cap[k] = n;
+  }
+  std::memcpy(I.up_pin[k], hb->svox.data(), sizeof(float) * n);
+  DTC_CUDA(cudaMemcpyAsync(I.up_dev[k], I.up_pin[k], sizeof(float) * n, cudaMemcpyHostToDevice, I.up_stream));
+  DTC_CUDA(cudaEventRecord(I.up_ev[k], I.up_stream));
+  hb->up_slot = k;
+  I.up_next = 1 - k;
+  return DTC_OK;
 }
 
 void DeviceSolver::clear_kept() {
@@ -2895,7 +2952,7 @@ int DeviceSolver::energy_grad(const double* dloss_dc, float* const* grad_e, int6
     const float* sv;
     if (ch.on_device) {
       X = B<double>(I, bX);
-      sv = B<float>(I, bSvox);
+      sv = I.svox();
     } else {
       if ((e = ensure(I, bAdjX, sizeof(double) * ch.X.size(), msg)) ||
           (e = ensure(I, bAdjSvox, sizeof(float) * std::max<size_t>(ch.svox.size(), 1), msg)))

@@ -276,6 +276,20 @@ def test_hex20_tensor_core_matches_oracle(dtc, batch20, precond):
         assert rel(r["c"], ref["c"]) <= TOL_MIXED
 
 
+@pytest.mark.parametrize("precond", ["block", "mg"])
+def test_hex20_uniform_batch_matches_oracle(dtc, orc, precond):
+    """A batch of HEX20 domains of one size (as c2): mixed path against the oracle."""
+    pairs = [make_pair20(dtc, orc, (8, 8, 8), b, dtc.synth.seed_for(21, i), E_voxel=i == 2)
+             for i, b in enumerate((0.2, 0.35, 0.5))]
+    refs = orc.solve_batch([p[1] for p in pairs])
+    with dtc.Solver(precision="mixed", rtol=1e-10, rotation_search=False, inner_precond=precond) as s:
+        res = s.solve([p[0] for p in pairs])
+    for r, ref in zip(res, refs):
+        assert r["status"] == 0
+        assert rel(r["c"], ref["c"]) <= TOL_MIXED
+        assert rel(r["ff"], ref["ff"]) <= TOL_MIXED
+
+
 @pytest.mark.parametrize("precision,precond,rtol", [("fp64", "block", 1e-10), ("mixed", "mg", 1e-8)])
 def test_pipelined_passes_match_one_pass(dtc, precision, precond, rtol):
     """A batch of >= 256 domains is solved in 2 device passes, the host phase of the second
@@ -319,3 +333,24 @@ def test_autotuned_sweeps(dtc, batch):
         assert st["autotune_simt_sweep"]["launches"] == st["autotune_tc_sweep"]["launches"] == 3
         assert st["autotune_simt_sweep"]["ms_total"] > 0 and st["autotune_tc_sweep"]["ms_total"] > 0
     assert stats[0]["autotune_tc_sweep"]["ms_total"] == stats[1]["autotune_tc_sweep"]["ms_total"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_passes_match_one_pass(dtc, batch, precision):
+    """A batch cut into device passes (chunk_domains) gives the results of one pass: each later
+    pass's voxel factors are uploaded through pinned memory on their own stream while the pass
+    before solves, and the solve waits for that copy."""
+    pairs, refs = batch
+    doms = [p[0] for p in pairs]
+    kw = dict(precision=precision, rtol=1e-10, rotation_search=False)
+    if precision == "mixed":
+        kw["inner_precond"] = "mg"
+    with dtc.Solver(**kw) as s:
+        one = s.solve(doms)
+    with dtc.Solver(chunk_domains=2, **kw) as s:
+        cut = s.solve(doms)
+        again = s.solve(doms[::-1])[::-1]   # the slots alternate: a second batch reuses them
+    for a, b, c, ref in zip(one, cut, again, refs):
+        assert a["status"] == b["status"] == c["status"] == 0
+        assert rel(b["c"], a["c"]) <= 1e-7 and rel(c["c"], a["c"]) <= 1e-7
+        assert rel(b["c"], ref["c"]) <= (TOL_FP64 if precision == "fp64" else TOL_MIXED)
