@@ -63,12 +63,20 @@ def test_c0_fp64_matches_oracle(dtc, gold, cases):
         # the dot-product sums, which follows the CTA schedule) moves the crossing of the
         # threshold: measured up to 9 of ~250-340 iterations; allowed 5 %
         assert (np.abs(r["iters"] - gold["c0_iters"][i]) <= np.maximum(3, 0.05 * gold["c0_iters"][i])).all()
-        # rotation search on a tensor that differs from the oracle's in the 10th digit: the
-        # criterion agrees to that level (the argmin may move along a flat valley)
+        # rotation search on a tensor that differs from the oracle's in the 10th digit (the order of
+        # the device's dot-product and reaction sums follows the CTA schedule): the criterion
+        # agrees to that level, but where two rotations reach it within rounding the argmin may
+        # jump between them, and so may the rotated tensor (measured: 0.9 % on its diagonal for one
+        # c0 domain in one of six runs).  The rotated tensor is checked through invariants of the
+        # rotation, C_iijj (the sum of the normal block) and the Frobenius norm of the 6x6 (the
+        # rotation is orthogonal in the Mandel form), against the unrotated tensor; bit-exact
+        # argmin parity on identical tensors is tested in test_rotation_search_bit_exact and
+        # test_rotation_c0_indices_from_fixture.
         e2 = np.abs(gold["c0_ee"][i]).max() ** 2
         for w in ("cr1", "cr2"):
             assert abs(r[w]["crit"] - gold[f"c0_{w}_crit"][i]) <= 1e-8 * e2
-            assert rel(np.sort(np.diag(r[w]["ee"])), np.sort(np.diag(gold[f"c0_{w}_ee"][i]))) <= 1e-6
+            assert abs(r[w]["ee"][:3, :3].sum() - gold["c0_ee"][i][:3, :3].sum()) <= 1e-6 * np.abs(gold["c0_ee"][i]).max()
+            assert rel(np.linalg.norm(r[w]["ee"]), np.linalg.norm(gold["c0_ee"][i])) <= 1e-6
 
 
 def test_c1_matches_oracle(dtc, gold, cases):

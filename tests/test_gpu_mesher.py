@@ -72,3 +72,32 @@ def test_solve_with_device_mesher(dtc):
         if a["status"] == 0:
             assert np.abs(a["c"] - b["c"]).max() <= 1e-9 * np.abs(b["c"]).max()
             assert np.abs(a["displ"] - b["displ"]).max() <= 1e-9 * np.abs(b["displ"]).max()
+
+
+@pytest.mark.parametrize("nen", [8, 20])
+def test_device_mesher_macro_order2(dtc, nen):
+    """The 60 prescribed values per constrained DOF of macro order 2, from the device mesher's
+    plans, equal the host planner's (tests/test_mesher.py pins those to the oracle); and a solve
+    with the device mesher gives the host-mesher solve's 60 x 60 leaves."""
+    rng = np.random.default_rng(211 + nen)
+    doms = []
+    for _ in range(20):
+        L = rng.integers(2, 9, size=3)
+        phi = (rng.random((L[2], L[1], L[0])) < 0.6).astype(np.int16) * 1000
+        doms.append(dtc.Domain(phi, elem_type=nen, delta=0.05, xa_n=tuple(int(v) for v in rng.integers(1, 40, 3))))
+    with dtc.Solver() as s:
+        dev = s.mesh_batch(doms, macro_order=2)
+    for d, m in zip(doms, dev):
+        ref = dtc.mesh_domain(d, macro_order=2)
+        same(m, ref)
+        assert m["bnode_vals"].shape == (60, 3 * m["nb"])
+    syn = dtc.synth
+    sd = [dtc.Domain(syn.bone_volume((8, 8, 8), b, syn.seed_for(8, 90 + i)), elem_type=nen, E=syn.E_CONST, nu=syn.NU,
+                     delta=syn.DELTA) for i, b in enumerate((0.35, 0.5))]
+    out = {}
+    for dm in (False, True):
+        with dtc.Solver(precision="fp64", rtol=1e-10, rotation_search=False, device_mesher=dm, macro_order=2) as s:
+            out[dm] = s.solve(sd)
+    for a, b in zip(out[True], out[False]):
+        assert a["status"] == b["status"] == 0
+        assert np.abs(a["kmacro"] - b["kmacro"]).max() <= 1e-9 * np.abs(b["kmacro"]).max()
