@@ -601,10 +601,12 @@ def main():
             "rtol": rt, "max_rel_err": ej, "speedup_over_fp64_from_precision": fp64_ms / mj_ms,
             "speedup_from_multigrid_and_estimator": mj_ms / step_ms}
     peak, src = measured_peaks()
-    # dominant kernel: one extra, untimed-for-the-metric step with CUDA-event timing per launch
+    # dominant kernel: extra, untimed-for-the-metric steps with CUDA-event timing per launch (the
+    # second solve of the handle: one-time allocations and the tuner's timings behind it)
     with dtc.Solver(precision="mixed", rtol=rtol_of["mixed"], max_it=args.max_it, rotation_search=False,
                     device=local, profile_kernels=True, estimator=args.estimator,
                     inner_precond=args.precond, mixed_matvec=args.matvec) as prof:
+        prof.solve(doms)
         prof.solve(doms)
         ks = prof.kernel_stats()
     host = {k: ks.pop(k) for k in list(ks) if k.startswith("host_")}   # host phases, wall ms

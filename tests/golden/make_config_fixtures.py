@@ -8,8 +8,11 @@ dtc_b200.synth and compare against them.  Cases:
        CR1/CR2 rotation search;
   c1 : 4 HEX08 domains of 32^3 drawn like the headline batch (BV/TV 0.10-0.40, per-voxel E);
   c2 : 4 HEX20 domains of 24^3 (BV/TV 0.25, per-voxel E), the subset of the HEX20 workload.
+With --me2 it writes tests/golden/config_parity_me2.npz instead:
+  me2: macro order 2 (60 load cases) on the first 4 c0 domains (HEX08, 20^3, constant E) and on
+       2 HEX20 domains of 12^3 (per-voxel E).
 
-    python tests/golden/make_config_fixtures.py [--threads N]
+    python tests/golden/make_config_fixtures.py [--threads N] [--me2]
 """
 import argparse
 import sys
@@ -23,6 +26,7 @@ sys.path.insert(0, str(ROOT))
 import __graft_entry__ as ge  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "config_parity.npz"
+OUT_ME2 = Path(__file__).resolve().parent / "config_parity_me2.npz"
 
 
 def c0_domains(syn):
@@ -38,6 +42,10 @@ def c1_cases(syn, n=4):
 
 def c2_cases(syn, n=4):
     return [syn.bone_volume((24, 24, 24), 0.25, syn.seed_for(2, i)) for i in range(n)]
+
+
+def me2_hex20_cases(syn, n=2):
+    return [syn.bone_volume((12, 12, 12), 0.3, syn.seed_for(2, 900 + i)) for i in range(n)]
 
 
 def pack(prefix, results, out):
@@ -60,12 +68,25 @@ def pack(prefix, results, out):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--me2", action="store_true")
     a = ap.parse_args()
     dtc = ge.load_package()
     orc = ge.load_oracle()
     syn = dtc.synth
     out = {}
     t0 = time.time()
+    if a.me2:
+        parts = c0_domains(syn)[:4]
+        doms = [orc.Domain(sub, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, xa_n=xa, macro_order=2)
+                for _, xa, sub in parts]
+        pack("me2", orc.solve_batch(doms, nthreads=a.threads), out)
+        doms = [orc.Domain(g, nen=20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, macro_order=2,
+                           E_voxel=syn.modulus_of_gray(g)) for g in me2_hex20_cases(syn)]
+        pack("me2h20", orc.solve_batch(doms, nthreads=a.threads), out)
+        print(f"me2 done {time.time() - t0:.0f} s", flush=True)
+        np.savez_compressed(OUT_ME2, **out)
+        print("wrote", OUT_ME2)
+        return
     parts = c0_domains(syn)
     doms = [orc.Domain(sub, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, rtol=1e-10, xa_n=xa, rotation=True)
             for _, xa, sub in parts]

@@ -5,7 +5,9 @@ tests/golden/config_parity.npz (made by tests/golden/make_config_fixtures.py, wh
 defines the inputs rebuilt here from their seeds):
   c0 : 27 HEX08 domains of 20^3 from a 62^3 volume, constant E, rotation search;
   c1 : 4 HEX08 domains of 32^3 drawn like the headline batch, per-voxel E;
-  c2 : 4 HEX20 domains of 24^3, per-voxel E.
+  c2 : 4 HEX20 domains of 24^3, per-voxel E;
+and, in tests/golden/config_parity_me2.npz (the same script with --me2), macro order 2 (60 load
+cases) on the first 4 c0 domains and on 2 HEX20 domains of 12^3.
 Tolerances (normwise relative on C, ff, K_macro): FP64 path 1e-6, mixed path 1e-5.
 Counts and indices (ne, nn, nb; rotation argmin indices and refinement depth) must be equal.
 """
@@ -37,7 +39,8 @@ def cases(dtc):
     m = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(m)
     syn = dtc.synth
-    return {"c0": m.c0_domains(syn), "c1": m.c1_cases(syn), "c2": m.c2_cases(syn)}
+    return {"c0": m.c0_domains(syn), "c1": m.c1_cases(syn), "c2": m.c2_cases(syn),
+            "me2h20": m.me2_hex20_cases(syn)}
 
 
 def check_tensors(res, gold, key, tol, counts=True):
@@ -77,6 +80,24 @@ def test_c0_fp64_matches_oracle(dtc, gold, cases):
             assert abs(r[w]["crit"] - gold[f"c0_{w}_crit"][i]) <= 1e-8 * e2
             assert abs(r[w]["ee"][:3, :3].sum() - gold["c0_ee"][i][:3, :3].sum()) <= 1e-6 * np.abs(gold["c0_ee"][i]).max()
             assert rel(np.linalg.norm(r[w]["ee"]), np.linalg.norm(gold["c0_ee"][i])) <= 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_macro_order2_matches_oracle(dtc, cases, precision):
+    """Macro order 2 at c0's domain size (and HEX20 micro elements): C, ff(60 x 60), K_macro."""
+    g2 = np.load(GOLDEN / "config_parity_me2.npz")
+    syn = dtc.synth
+    kw = dict(precision=precision, rotation_search=False, macro_order=2)
+    if precision == "mixed":
+        kw.update(inner_precond="mg", estimator="energy")
+    tol = TOL_FP64 if precision == "fp64" else TOL_MIXED
+    doms = [dtc.Domain(sub, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA, xa_n=xa) for _, xa, sub in cases["c0"][:4]]
+    with dtc.Solver(rtol=1e-10, **kw) as s:
+        check_tensors(s.solve(doms), g2, "me2", tol)
+    doms = [dtc.Domain(g, elem_type=dtc.HEX20, E=syn.E_CONST, nu=syn.NU, delta=syn.DELTA,
+                       E_voxel=syn.modulus_of_gray(g)) for g in cases["me2h20"]]
+    with dtc.Solver(rtol=1e-10, **kw) as s:
+        check_tensors(s.solve(doms), g2, "me2h20", tol)
 
 
 def test_c1_matches_oracle(dtc, gold, cases):
