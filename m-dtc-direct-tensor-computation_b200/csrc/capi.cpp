@@ -339,8 +339,12 @@ dtc_status dtc_solve_batch(dtc_handle* h, const dtc_domain_in* in, int64_t n, dt
     }
     st.rc = DeviceSolver::prepare(st.tasks, h->opt, in[0].nu, st.batch, st.msg);
     // the voxel factors go to the device now, overlapping the solve of the pass before (the
-    // adjoint keeps the buffers of the pass solved last: it uploads with the solve)
-    if (st.rc == DTC_OK && !keep) st.rc = h->solver.upload_voxels(st.batch.get(), st.msg);
+    // adjoint keeps the buffers of the pass solved last: it uploads with the solve); if the
+    // pinned staging cannot be had, the pass uploads them with its solve instead
+    if (st.rc == DTC_OK && !keep) {
+      std::string ignored;
+      h->solver.upload_voxels(st.batch.get(), ignored);
+    }
   };
   // the host stage may run on a worker thread: an exception there becomes the pass's status
   auto host_stage = [&](size_t c, Stage& st) {

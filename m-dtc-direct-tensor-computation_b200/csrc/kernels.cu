@@ -2764,32 +2764,39 @@ int DeviceSolver::solve(std::vector<DomainTask>& tasks, const dtc_options& opt, 
 int DeviceSolver::upload_voxels(HostBatch* hb, std::string& msg) {
   if (!hb || hb->nen == 0 || hb->svox.empty()) return DTC_OK;
   Impl& I = *impl_;
-  DTC_CUDA(cudaSetDevice(I.device));
-  if (!I.up_stream) {
-    DTC_CUDA(cudaStreamCreateWithFlags(&I.up_stream, cudaStreamNonBlocking));
-    DTC_CUDA(cudaEventCreateWithFlags(&I.up_ev[0], cudaEventDisableTiming));
-    DTC_CUDA(cudaEventCreateWithFlags(&I.up_ev[1], cudaEventDisableTiming));
-  }
-  const int k = I.up_next;
-  const size_t n = hb->svox.size();
-  // the slot's last reader, the pass before the one now solving, has finished; its copy too
-  DTC_CUDA(cudaEventSynchronize(I.up_ev[k]));
-  if (I.up_cap[k] < n) {
-    if (I.up_pin[k]) cudaFreeHost(I.up_pin[k]);
-    if (I.up_dev[k]) cudaFree(I.up_dev[k]);
-    I.up_pin[k] = nullptr;
-    I.up_dev[k] = nullptr;
-    I.up_cap[k] = 0;
-    DTC_CUDA(cudaMallocHost(&I.up_pin[k], sizeof(float) * n));
-    DTC_CUDA(cudaMalloc(&I.up_dev[k], sizeof(float) * n));
-    I.up_cap[k] = n;
-  }
-  std::memcpy(I.up_pin[k], hb->svox.data(), sizeof(float) * n);
-  DTC_CUDA(cudaMemcpyAsync(I.up_dev[k], I.up_pin[k], sizeof(float) * n, cudaMemcpyHostToDevice, I.up_stream));
-  DTC_CUDA(cudaEventRecord(I.up_ev[k], I.up_stream));
-  hb->up_slot = k;
-  I.up_next = 1 - k;
-  return DTC_OK;
+  auto stage = [&]() -> int {
+    DTC_CUDA(cudaSetDevice(I.device));
+    if (!I.up_stream) {
+      DTC_CUDA(cudaStreamCreateWithFlags(&I.up_stream, cudaStreamNonBlocking));
+      DTC_CUDA(cudaEventCreateWithFlags(&I.up_ev[0], cudaEventDisableTiming));
+      DTC_CUDA(cudaEventCreateWithFlags(&I.up_ev[1], cudaEventDisableTiming));
+    }
+    const int k = I.up_next;
+    const size_t n = hb->svox.size();
+    // the slot's last reader, the pass before the one now solving, has finished; its copy too
+    DTC_CUDA(cudaEventSynchronize(I.up_ev[k]));
+    if (I.up_cap[k] < n) {
+      if (I.up_pin[k]) cudaFreeHost(I.up_pin[k]);
+      if (I.up_dev[k]) cudaFree(I.up_dev[k]);
+      I.up_pin[k] = nullptr;
+      I.up_dev[k] = nullptr;
+      I.up_cap[k] = 0;
+      DTC_CUDA(cudaMallocHost(&I.up_pin[k], sizeof(float) * n));
+      DTC_CUDA(cudaMalloc(&I.up_dev[k], sizeof(float) * n));
+      I.up_cap[k] = n;
+    }
+    std::memcpy(I.up_pin[k], hb->svox.data(), sizeof(float) * n);
+    DTC_CUDA(cudaMemcpyAsync(I.up_dev[k], I.up_pin[k], sizeof(float) * n, cudaMemcpyHostToDevice, I.up_stream));
+    DTC_CUDA(cudaEventRecord(I.up_ev[k], I.up_stream));
+    hb->up_slot = k;
+    I.up_next = 1 - k;
+    return DTC_OK;
+  };
+  const int rc = stage();
+  // a failed allocation leaves a (non-sticky) last error behind: clear it, so that the next
+  // launch check does not report it for a kernel
+  if (rc != DTC_OK) cudaGetLastError();
+  return rc;
 }
 
 void DeviceSolver::clear_kept() {

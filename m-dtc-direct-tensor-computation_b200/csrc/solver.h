@@ -123,7 +123,8 @@ class DeviceSolver {
   // Copy a prepared pass's voxel factors to the device through pinned memory on a stream of
   // their own, so that the copy overlaps the solve of the pass before; its solve then waits
   // for the copy instead of uploading them.  Call from one host thread at a time, after
-  // prepare and before solve of that pass, while at most one other pass is in flight.
+  // prepare and before solve of that pass, while at most one other pass is in flight.  On an
+  // error the batch is left as it was (its solve uploads the factors itself).
   int upload_voxels(HostBatch* batch, std::string& msg);
   // Adjoint: dL/dE_voxel for the domains of the last solve (kept displacements).
   // grad_on_device: grad_e[i] are device pointers on this solver's device (filled by device
