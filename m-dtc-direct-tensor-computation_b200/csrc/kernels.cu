@@ -723,12 +723,13 @@ __global__ void __launch_bounds__(kThreads) k_residual_norm(const Tile* __restri
   if (threadIdx.x < 8) atomicAdd(acc_zz + col, s1);
 }
 
-// r32 = (float) r64 for columns still refining, 0 otherwise; x32 = p32 = 0
+// r32 = (float) (sgn * r64) for columns still refining, 0 otherwise; x32 = p32 = 0 (sgn = -1 when
+// r64 holds K X rather than the residual -(K X))
 __global__ void __launch_bounds__(kThreads) k_start_inner(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                           const uint8_t* __restrict__ flags,
                                                           const double* __restrict__ r64, float* __restrict__ r32,
                                                           float* __restrict__ x32, float* __restrict__ p32,
-                                                          const ColState* __restrict__ ost) {
+                                                          const ColState* __restrict__ ost, double sgn) {
   const int* dom_active = nullptr;
   DTC_TILE_PROLOGUE
   if (!rowok) return;
@@ -741,7 +742,7 @@ __global__ void __launch_bounds__(kThreads) k_start_inner(const Tile* __restrict
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t k = vec_index(n, c, lc);
-      r32[k] = on ? (float)r64[k] : 0.0f;
+      r32[k] = on ? (float)(sgn * r64[k]) : 0.0f;
       x32[k] = 0.0f;
       p32[k] = 0.0f;
     }
@@ -2558,6 +2559,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       ++L;
     }
     if ((e = launch_check(msg))) return e;
+    bool kx_all = false;   // R64 holds K X on every node for the final X (mixed refinement)
     if (!mixed) {
       // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
       DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
@@ -2581,10 +2583,19 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       int64_t inner_budget = opt.max_it;
       for (int step = 0; step <= max_refine; ++step) {
         DTC_CUDA(cudaMemsetAsync(I.bufs[bZz], 0, sizeof(double) * ncol, s));
-        if (nti) {
+        // from the second check on, K X over every node: its interior part is minus the residual
+        // and, once the loop stops (X is final then), it is the reaction force of every node
+        kx_all = step > 0 && nta > 0;
+        if (kx_all) {
+          apply_k<double, NEN, true, false>(W, dd, I.svox(), fl, X, R64, 1.0, nullptr, nullptr, s);
+          ++L;
+        } else if (nti) {
           apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s);
+          ++L;
+        }
+        if (nti) {
           k_residual_norm<<<gi, kThreads, 0, s>>>(ti, dd, fl, B<double>(I, bDinv64), R64, B<double>(I, bZz));
-          L += 2;
+          ++L;
         }
         k_outer_check<<<ndom, 32, 0, s>>>(ost, B<double>(I, bZz), B<double>(I, bTarget), B<int>(I, bDomAct), opt.rtol,
                                           step == 0);
@@ -2595,7 +2606,11 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
         DTC_CUDA(cudaMemcpyAsync(&h_count, I.bufs[bCount], sizeof(int), cudaMemcpyDeviceToHost, s));
         DTC_CUDA(cudaStreamSynchronize(s));
         if (h_count == 0 || step == max_refine || inner_budget <= 0) break;
-        if (nti) { k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32), ost); ++L; }
+        if (nti) {
+          k_start_inner<<<gi, kThreads, 0, s>>>(ti, dd, fl, R64, B<float>(I, bR32), B<float>(I, bX32), B<float>(I, bP32),
+                                                ost, kx_all ? -1.0 : 1.0);
+          ++L;
+        }
         DTC_CUDA(cudaMemsetAsync(I.bufs[bW32], 0, vbytes32, s));
         if (use_mg)
           e = run_cg_mg<NEN>(I, ndom, W, mgd, B<float>(I, bX32), B<float>(I, bR32), B<float>(I, bP32), B<float>(I, bW32),
@@ -2615,10 +2630,14 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
         if ((e = launch_check(msg))) return e;
       }
     }
-    // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff)
-    DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
+    // reactions F = K X on all nodes (AA_org * u, :1092-1123) and their projection (ff); the
+    // mixed loop's last check already computed them for the final X (readers use active nodes only)
+    if (!kx_all) DTC_CUDA(cudaMemsetAsync(R64, 0, vbytes64, s));
     if (nta) {
-      apply_k<double, NEN, true, false>(W, dd, I.svox(), fl, X, R64, 1.0, nullptr, nullptr, s);
+      if (!kx_all) {
+        apply_k<double, NEN, true, false>(W, dd, I.svox(), fl, X, R64, 1.0, nullptr, nullptr, s);
+        ++L;
+      }
       if (energy) {
         k_energy_gram<<<ga, kThreads, 0, s>>>(ta, dd, fl, X, R64, B<double>(I, bFf), ldg, kNLC * cp, kNLC * cp);
         for (int q = 0; q < cp; ++q) {   // u_q . K u_cp against the kept solutions of earlier passes
@@ -2633,7 +2652,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
         k_project<20><<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf), cp * kNLC);
       else
         k_project<8><<<ga, kThreads, 0, s>>>(ta, dd, fl, R64, B<double>(I, bFf), 0);
-      L += 2;
+      ++L;
     }
     if ((e = launch_check(msg))) return e;
     DTC_CUDA(cudaMemcpyAsync(cs.data() + ncol * cp, ost, sizeof(ColState) * ncol, cudaMemcpyDeviceToHost, s));
