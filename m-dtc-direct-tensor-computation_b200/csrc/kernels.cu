@@ -215,7 +215,9 @@ template <> struct Win<float, true> : Win<float, false> {
 
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
-// node of the grid (reaction forces).
+// node of the grid (reaction forces).  bnd_only: u vanishes off the domain box (the boundary
+// values before the first solve) and y is zero on entry; a row whose neighbour rows lie
+// inside the box then only has nonzero output at x = 1 and x = n0 - 2, and computes only those.
 // MINB: CTAs per SM the register allocation is sized for; FP32 4 (at most 128 registers) or 5,
 // FP64 1 (255) or 3 (168), chosen per batch class by the sweep autotuner
 template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 4 : 1)>
@@ -223,7 +225,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
                                                                           const DomDev* __restrict__ doms,
                                                      const float* __restrict__ svox, const T* __restrict__ u,
                                                      T* __restrict__ y, double scale, double* __restrict__ acc,
-                                                     const int* __restrict__ dom_active) {
+                                                     const int* __restrict__ dom_active, int bnd_only) {
   __shared__ double red[32];
   const Tile t = tiles[blockIdx.x / 3];
   if (dom_active && !dom_active[t.dom]) return;
@@ -233,19 +235,25 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   const int lo = ALL ? 0 : 1;
   const int xhi = ALL ? D.n[0] - 1 : D.n[0] - 2, yhi = ALL ? D.n[1] - 1 : D.n[1] - 2, zhi = ALL ? D.n[2] - 1 : D.n[2] - 2;
+  // nodes x0 .. xe of the row, x0 from the tile start
+  int x0 = t.x0, xe = min(xhi, t.x0 + kTileX - 1);
+  if (!ALL && bnd_only && yy >= 2 && yy <= D.n[1] - 3 && zz >= 2 && zz <= D.n[2] - 3) {
+    const bool has_lo = x0 <= 1 && 1 <= xe, has_hi = x0 <= D.n[0] - 2 && D.n[0] - 2 <= xe;
+    if (has_lo && !has_hi) xe = 1;
+    else if (has_hi && !has_lo) x0 = D.n[0] - 2;
+    else if (!has_lo) xe = x0 - 1;   // neither: nothing to compute on this row
+  }
   double dot = 0.0;
-  if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi) {
+  if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi && x0 <= xe) {
     Win<T, sizeof(T) == 4> W;
     float sv[2][2];
     T cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
-    W.template start<ALL>(u, D, t.x0 - 1, yy, zz, lc);
-    load_voxels<ALL>(sv, svox, D, t.x0 - 1, yy, zz);
+    W.template start<ALL>(u, D, x0 - 1, yy, zz, lc);
+    load_voxels<ALL>(sv, svox, D, x0 - 1, yy, zz);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
     W.template apply<true>(sv, cur, nxt);
 #pragma unroll 1
-    for (int i = 0; i < kTileX; ++i) {
-      const int x = t.x0 + i;
-      if (x > xhi) break;
+    for (int x = x0; x <= xe; ++x) {
       W.template advance<ALL>(u, D, x + 1, yy, zz, lc);
       load_voxels<ALL>(sv, svox, D, x, yy, zz);
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
@@ -1080,18 +1088,18 @@ struct Work {
 // y = scale * K u on the interior (ALL = false) or every node; DOT: acc[col] += u . y.
 template <typename T, int NEN, bool ALL, bool DOT>
 void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* fl, const T* u, T* y, double scale,
-             double* acc, const int* act, cudaStream_t s) {
+             double* acc, const int* act, cudaStream_t s, int bnd_only = 0) {
   if constexpr (NEN == 8) {
     const int64_t nt = ALL ? W.nta : W.nti;
     if (nt <= 0) return;
     const unsigned g = (unsigned)(3 * nt);
     const Tile* tl = ALL ? W.ta : W.ti;
     if constexpr (sizeof(T) == 4) {
-      if (W.minb32 == 5) k_matvec<T, ALL, DOT, 5><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
-      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
+      if (W.minb32 == 5) k_matvec<T, ALL, DOT, 5><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
+      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
     } else {
-      if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
-      else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act);
+      if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
+      else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
     }
   } else {
     const T* ke;
@@ -2564,7 +2572,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       // b = -(K X)_interior with X = boundary values only (RHS of all 24 load cases, :674-951)
       DTC_CUDA(cudaMemsetAsync(I.bufs[bP64], 0, vbytes64, s));
       DTC_CUDA(cudaMemsetAsync(I.bufs[bW64], 0, vbytes64, s));
-      apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s);
+      apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s, 1);
       ++L;
       if ((e = run_cg<double, false, NEN>(I, ndom, W, X, R64, B<double>(I, bP64), B<double>(I, bW64), B<double>(I, bDinv64),
                               opt.rtol, nullptr, opt.max_it, L, msg)))
@@ -2589,8 +2597,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
         if (kx_all) {
           apply_k<double, NEN, true, false>(W, dd, I.svox(), fl, X, R64, 1.0, nullptr, nullptr, s);
           ++L;
-        } else if (nti) {
-          apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s);
+        } else if (nti) {   // first check: X holds the boundary values only, R64 is zero
+          apply_k<double, NEN, false, false>(W, dd, I.svox(), fl, X, R64, -1.0, nullptr, nullptr, s, 1);
           ++L;
         }
         if (nti) {
