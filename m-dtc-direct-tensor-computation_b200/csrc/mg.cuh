@@ -74,10 +74,9 @@ __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __rest
     load_voxels_f(sv, svox, D, t.x0 - 1, yy, zz);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
     W.apply<true>(sv, cur, nxt);
+    const int xe = min(D.n[0] - 2, t.x0 + kTileX - 1);
 #pragma unroll 1
-    for (int i = 0; i < kTileX; ++i) {
-      const int x = t.x0 + i;
-      if (x > D.n[0] - 2) break;
+    for (int x = t.x0; x <= xe; ++x) {
       W.advance<false>(u, D, x + 1, yy, zz, lc);
       load_voxels_f(sv, svox, D, x, yy, zz);
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
