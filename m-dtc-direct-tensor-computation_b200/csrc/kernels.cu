@@ -185,11 +185,35 @@ __device__ __forceinline__ void slab_rp(const float (&P0)[3][3][3], const float 
 // slab on packed FMAs (slab_rp); otherwise scalar FMAs (FP64, and the FP32 reference form).
 template <typename T, bool PACKED = false> struct Win {
   T P0[3][3][3], P1[3][3][3];
+  // unguarded sweeps: the row's values at plane x+1 (the plane loaded last) for its load case,
+  // and the offsets of the neighbour rows in y and z (one 64-bit pointer, 32-bit offsets)
+  const T* row = nullptr;
+  int sy = 0, sz = 0;
+  __device__ __forceinline__ void load_rel(T (&pl)[3][3][3], const T* __restrict__ p) const {
+#pragma unroll
+    for (int py = 0; py < 3; ++py)
+#pragma unroll
+      for (int pz = 0; pz < 3; ++pz) {
+        const T* q = p + (py - 1) * sy + (pz - 1) * sz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pl[py][pz][c] = __ldg(q + c * kNLC);
+      }
+  }
   template <bool GUARD>
   __device__ __forceinline__ void start(const T* __restrict__ u, const DomDev& D, int x, int y, int z, int lc) {
-    load_plane<T, GUARD>(P0, u, D, x, y, z, lc);
-    load_plane<T, GUARD>(P1, u, D, x + 1, y, z, lc);
+    if constexpr (GUARD) {
+      load_plane<T, true>(P0, u, D, x, y, z, lc);
+      load_plane<T, true>(P1, u, D, x + 1, y, z, lc);
+    } else {
+      sy = D.n[0] * (3 * kNLC);
+      sz = D.n[0] * D.n[1] * (3 * kNLC);
+      row = u + vec_index(node_index(D, x, y, z), 0, lc);
+      load_rel(P0, row);
+      row += 3 * kNLC;
+      load_rel(P1, row);
+    }
   }
+  // next plane x (= the previous one + 1)
   template <bool GUARD>
   __device__ __forceinline__ void advance(const T* __restrict__ u, const DomDev& D, int x, int y, int z, int lc) {
 #pragma unroll
@@ -198,13 +222,38 @@ template <typename T, bool PACKED = false> struct Win {
       for (int pz = 0; pz < 3; ++pz)
 #pragma unroll
         for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
-    load_plane<T, GUARD>(P1, u, D, x, y, z, lc);
+    if constexpr (GUARD) {
+      load_plane<T, true>(P1, u, D, x, y, z, lc);
+    } else {
+      row += 3 * kNLC;
+      load_rel(P1, row);
+    }
   }
   template <bool FIRST>
   __device__ __forceinline__ void apply(const float (&sv)[2][2], T (&cur)[3], T (&nxt)[3]) const {
     slab<T, FIRST>(P0, P1, sv, cur, nxt);
   }
   __device__ __forceinline__ T centre(int c) const { return P0[1][1][c]; }
+  // unguarded sweeps: index of the centre node's first value (plane x) in the vector u
+  __device__ __forceinline__ int64_t centre_index(const T* __restrict__ u) const { return (row - u) - 3 * kNLC; }
+};
+
+// The 4 voxels of an interior node row between planes x and x+1 (unguarded sweeps): a pointer
+// that advances by one voxel per plane, 32-bit offsets of the y and z neighbours.
+struct VoxRow {
+  const float* p;
+  int sy, sz;
+  __device__ __forceinline__ void start(const float* __restrict__ svox, const DomDev& D, int vx, int y, int z) {
+    sy = D.L[0];
+    sz = D.L[0] * D.L[1];
+    p = svox + D.vox_off + vx + (int64_t)D.L[0] * ((y - 1) + (int64_t)D.L[1] * (z - 1));
+  }
+  __device__ __forceinline__ void load(float (&sp)[2][2]) const {
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) sp[b][c] = __ldg(p + b * sy + c * sz);
+  }
 };
 template <> struct Win<float, true> : Win<float, false> {
   template <bool FIRST>
@@ -246,22 +295,33 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
   double dot = 0.0;
   if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi && x0 <= xe) {
     Win<T, sizeof(T) == 4> W;
+    VoxRow V;
     float sv[2][2];
     T cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
     W.template start<ALL>(u, D, x0 - 1, yy, zz, lc);
-    load_voxels<ALL>(sv, svox, D, x0 - 1, yy, zz);
+    if constexpr (ALL) {
+      load_voxels<true>(sv, svox, D, x0 - 1, yy, zz);
+    } else {
+      V.start(svox, D, x0 - 1, yy, zz);
+      V.load(sv);
+    }
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
     W.template apply<true>(sv, cur, nxt);
 #pragma unroll 1
     for (int x = x0; x <= xe; ++x) {
       W.template advance<ALL>(u, D, x + 1, yy, zz, lc);
-      load_voxels<ALL>(sv, svox, D, x, yy, zz);
+      if constexpr (ALL) {
+        load_voxels<true>(sv, svox, D, x, yy, zz);
+      } else {
+        ++V.p;
+        V.load(sv);
+      }
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
       for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = T(0); }
       W.template apply<false>(sv, cur, nxt);
       if (anyp | anyc) {
-        const int64_t b = vec_index(node_index(D, x, yy, zz), 0, lc);
+        const int64_t b = ALL ? vec_index(node_index(D, x, yy, zz), 0, lc) : W.centre_index(u);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const T v = (T)(scale * D.scale * (double)cur[c]);

@@ -38,15 +38,6 @@ enum { kMgRes = 0, kMgPost = 1 };
 constexpr int kListShift = 40;
 constexpr int64_t kListNodeMask = (int64_t(1) << kListShift) - 1;
 
-__device__ __forceinline__ void load_voxels_f(float (&sp)[2][2], const float* __restrict__ svox, const DomDev& D, int vx,
-                                              int y, int z) {
-#pragma unroll
-  for (int b = 0; b < 2; ++b)
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-      sp[b][c] = __ldg(svox + D.vox_off + vx + (int64_t)D.L[0] * ((y - 1 + b) + (int64_t)D.L[1] * (z - 1 + c)));
-}
-
 // Residual / smoother on one level's interior tiles (the slab sweep of k_matvec).
 //   kMgRes : y = b - K u
 //   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
@@ -68,24 +59,26 @@ __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __rest
   double szz = 0.0, szr = 0.0;
   if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
     Win<float, true> W;
+    VoxRow V;
     float sv[2][2];
     float cur[3] = {0.f, 0.f, 0.f}, nxt[3] = {0.f, 0.f, 0.f};
     W.start<false>(u, D, t.x0 - 1, yy, zz, lc);
-    load_voxels_f(sv, svox, D, t.x0 - 1, yy, zz);
+    V.start(svox, D, t.x0 - 1, yy, zz);
+    V.load(sv);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
     W.apply<true>(sv, cur, nxt);
     const int xe = min(D.n[0] - 2, t.x0 + kTileX - 1);
 #pragma unroll 1
     for (int x = t.x0; x <= xe; ++x) {
       W.advance<false>(u, D, x + 1, yy, zz, lc);
-      load_voxels_f(sv, svox, D, x, yy, zz);
+      ++V.p;
+      V.load(sv);
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
       for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = 0.f; }
       W.apply<false>(sv, cur, nxt);
       if (anyp | anyc) {
-        const int64_t n = node_index(D, x, yy, zz);
-        const int64_t k0 = vec_index(n, 0, lc);
+        const int64_t k0 = W.centre_index(u);
         float res[3], bc[3], v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -97,7 +90,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __rest
           for (int c = 0; c < 3; ++c) v[c] = res[c];
         } else {
           float dz[3];
-          block_jacobi(binv, n, omega, res, dz);
+          block_jacobi(binv, node_index(D, x, yy, zz), omega, res, dz);
 #pragma unroll
           for (int c = 0; c < 3; ++c) v[c] = W.centre(c) + dz[c];
         }
