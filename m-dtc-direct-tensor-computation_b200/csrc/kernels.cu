@@ -1501,7 +1501,8 @@ struct MgDev {
   int minb_res = 4, minb_post = 4;   // HEX08 fine-level residual / post-smoothing sweeps: CTAs per SM
 };
 
-// The fine-level HEX08 residual and post-smoothing sweeps with the tuned register budget.
+// The HEX08 residual and post-smoothing sweeps with the tuned register budget (the fine
+// level's choice, used on the coarse levels too).
 template <int MODE, bool DOT>
 void launch_mg_matvec(int minb, unsigned g, cudaStream_t s, const Tile* t, const DomDev* d, const float* sv,
                       const float* bi, const float* b, const float* u, float* y, float om, double* a1, double* a2,
@@ -1562,7 +1563,7 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   float* cur = t;                  // the smoothed iterate
   float* rbuf = z;                 // the residual handed to the restriction
   if (twice) {
-    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
     ++launches;
     cur = z;
     rbuf = t;
@@ -1579,7 +1580,7 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   } else if (fine) {
     launch_mg_matvec<kMgRes, false>(M.minb_res, g, s, tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   } else {
-    k_mg_matvec<kMgRes, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
+    launch_mg_matvec<kMgRes, false>(M.minb_res, g, s, tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   }
   if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
@@ -1617,11 +1618,11 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
     launch_mg_matvec<kMgPost, true>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
   else if (twice) {
     // z holds the corrected iterate: t = z + w D^-1 (b - K z), then z = t + w D^-1 (b - K t)
-    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, z, t, P.omega, nullptr, nullptr, act);
-    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, z, t, P.omega, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
     ++launches;
   } else
-    k_mg_matvec<kMgPost, false><<<g, kThreads, 0, s>>>(tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
   if (fine) I.end(kcMgPost, q, mb + vb + vb / 12, mf);     // t in, z out (mb), b in, D^-1
   if (!fine) I.end(kcMgCoarse, q1, 0, 0);
   launches += 2;
