@@ -13,7 +13,8 @@
 // Work is cut into tiles of 8 x 4 x 4 nodes; a CTA of 128 threads handles one tile for
 // 8 of the 24 load cases (1-D grid, the three load-case groups of a tile adjacent), each
 // thread one (y,z) row of the tile and one load case, sweeping x with a 2-plane register
-// window (the slab sweep of the HEX08 operator).  HEX20 uses voxel bricks (ebe.cuh); the
+// window (the slab sweep of the HEX08 operator; the SIMT sweeps take their own lists of
+// kSweepX-long rows, which halves the start-up of the window per node).  HEX20 uses voxel bricks (ebe.cuh); the
 // multigrid CG vectors use a flat list of active interior nodes (mg.cuh).
 #pragma once
 #include <cstdint>
@@ -22,6 +23,7 @@ namespace dtc {
 
 constexpr int kNLC = 24;          // load cases of the linear macro element
 constexpr int kTileX = 8, kTileY = 4, kTileZ = 4;
+constexpr int kSweepX = 16;       // nodes per row of the SIMT slab sweeps (own tile lists: two tiles in x)
 constexpr int kLcGroup = 8;       // load cases per CTA
 constexpr int kThreads = 128;     // 8 load cases x 16 rows
 

@@ -264,7 +264,8 @@ template <> struct Win<float, true> : Win<float, false> {
 
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
-// node of the grid (reaction forces).  bnd_only: u vanishes off the domain box (the boundary
+// node of the grid (reaction forces).  xlen: nodes per row of the tile list (kTileX or
+// kSweepX).  bnd_only: u vanishes off the domain box (the boundary
 // values before the first solve) and y is zero on entry; a row whose neighbour rows lie
 // inside the box then only has nonzero output at x = 1 and x = n0 - 2, and computes only those.
 // MINB: CTAs per SM the register allocation is sized for; FP32 4 (at most 128 registers) or 5,
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
                                                                           const DomDev* __restrict__ doms,
                                                      const float* __restrict__ svox, const T* __restrict__ u,
                                                      T* __restrict__ y, double scale, double* __restrict__ acc,
-                                                     const int* __restrict__ dom_active, int bnd_only) {
+                                                     const int* __restrict__ dom_active, int bnd_only, int xlen) {
   __shared__ double red[32];
   const Tile t = tiles[blockIdx.x / 3];
   if (dom_active && !dom_active[t.dom]) return;
@@ -285,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
   const int lo = ALL ? 0 : 1;
   const int xhi = ALL ? D.n[0] - 1 : D.n[0] - 2, yhi = ALL ? D.n[1] - 1 : D.n[1] - 2, zhi = ALL ? D.n[2] - 1 : D.n[2] - 2;
   // nodes x0 .. xe of the row, x0 from the tile start
-  int x0 = t.x0, xe = min(xhi, t.x0 + kTileX - 1);
+  int x0 = t.x0, xe = min(xhi, t.x0 + xlen - 1);
   if (!ALL && bnd_only && yy >= 2 && yy <= D.n[1] - 3 && zz >= 2 && zz <= D.n[2] - 3) {
     const bool has_lo = x0 <= 1 && 1 <= xe, has_hi = x0 <= D.n[0] - 2 && D.n[0] - 2 <= xe;
     if (has_lo && !has_hi) xe = 1;
@@ -959,8 +960,8 @@ struct DeviceSolver::Impl {
   cudaStream_t stream = nullptr;
   // persistent buffers grown on demand
   std::vector<std::pair<void**, size_t>> owned;
-  void* bufs[64] = {nullptr};
-  size_t caps[64] = {0};
+  void* bufs[80] = {nullptr};
+  size_t caps[80] = {0};
   // what the solves of the last batch kept for the adjoint: per chunk the domains (node and
   // voxel offsets of that chunk), their batch positions, and the FP64 displacements, on the
   // device for the chunk solved last (its buffers are still live) or copied to the host
@@ -1035,8 +1036,9 @@ enum Buf { bDoms, bTilesI, bTilesA, bSvox, bFlags, bDinv64, bDinv32, bX, bR64, b
            bSt, bOst, bPw, bZz, bZr, bDomAct, bCount, bFf, bTarget, bErr, bBinv32, bBricksI, bBricksA, bZ32, bT32,
            bMgDoms, bMgTiles, bMgSvox, bMgFlags, bMgDinv64, bMgDinv32, bMgBinv32, bMgB, bMgT, bMgZ, bMgMinv, bMgList,
            bAdjG, bAdjV, bAdjBlk, bAdjGrad, bAdjDoms, bAdjX, bAdjSvox, bKe20, bKe20tc, bNodesI, bDirF, bAlphaF,
-           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bMgNodes, bMgNodesC, bXkeep, bNumBufs };
-static_assert(bNumBufs <= 64, "buffer table");
+           bTilesIc, bNodesIc, bBricksIc, bMgTilesC, bMgListC, bCompactCnt, bMgNodes, bMgNodesC, bXkeep, bTilesW,
+           bTilesWc, bNumBufs };
+static_assert(bNumBufs <= 80, "buffer table");
 static_assert(bSvox == 3, "DeviceSolver::Impl::svox() reads bufs[3]");
 
 int ensure(DeviceSolver::Impl& I, int which, size_t bytes, std::string& msg) {
@@ -1143,6 +1145,8 @@ struct Work {
   int* err;             // mbarrier time-out flag of the tensor-core kernels
   int minb32 = 4;       // HEX08 slab sweeps: CTAs per SM of the FP32 CG application (4 or 5)
   int minb64 = 1;       //                    and of every FP64 application (1 or 3)
+  const Tile* tw = nullptr;   // interior sweep tiles (rows of kSweepX nodes) of the slab sweeps
+  int64_t ntw = 0;
 };
 
 // y = scale * K u on the interior (ALL = false) or every node; DOT: acc[col] += u . y.
@@ -1150,16 +1154,18 @@ template <typename T, int NEN, bool ALL, bool DOT>
 void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* fl, const T* u, T* y, double scale,
              double* acc, const int* act, cudaStream_t s, int bnd_only = 0) {
   if constexpr (NEN == 8) {
-    const int64_t nt = ALL ? W.nta : W.nti;
+    // interior: the sweep tiles (rows of kSweepX nodes); every node: the node tiles
+    const int64_t nt = ALL ? W.nta : W.ntw;
     if (nt <= 0) return;
     const unsigned g = (unsigned)(3 * nt);
-    const Tile* tl = ALL ? W.ta : W.ti;
+    const Tile* tl = ALL ? W.ta : W.tw;
+    const int xl = ALL ? kTileX : kSweepX;
     if constexpr (sizeof(T) == 4) {
-      if (W.minb32 == 5) k_matvec<T, ALL, DOT, 5><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
-      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
+      if (W.minb32 == 5) k_matvec<T, ALL, DOT, 5><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
+      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
     } else {
-      if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
-      else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only);
+      if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
+      else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
     }
   } else {
     const T* ke;
@@ -1189,6 +1195,7 @@ struct MgPlan {
   std::vector<DomDev> doms;                         // nlev * ndom, level-major
   std::vector<Tile> tiles;
   std::vector<int64_t> sm_off, sm_n, in_off, in_n, all_off, all_n;
+  std::vector<int64_t> sw_off, sw_n;                // smoothing tiles as rows of kSweepX nodes (slab sweeps)
   std::vector<int> lists;
   std::vector<int64_t> list_off, list_n;
   std::vector<int64_t> nodes_l;                     // levels >= 1: active interior nodes, (domain << kListShift) | node
@@ -1317,8 +1324,9 @@ void coarse_inverse(const DomDev& D, const float* sv, const double* kh, float* o
     }
 }
 
-// Build the hierarchy on the host from the fine voxel factors.  fine_i: interior tiles of the
-// fine level (level-0 smoothing tiles are those of domains with a coarser level).
+// Build the hierarchy on the host from the fine voxel factors.  fine_i / fine_w: interior node
+// tiles / sweep tiles of the fine level (level-0 smoothing tiles are those of domains with a
+// coarser level).
 // Levels from this one down smooth twice per visit (pre and post): on 256 x 32^3 and on an
 // uneven batch (16^3-64^3) ~3.5% less solve time than once everywhere; twice already on
 // level 1 costs more than the iterations it saves.
@@ -1330,7 +1338,7 @@ constexpr int kMgTwiceFrom = 2;
 // grids are halved as for HEX08.  Every domain's levels are built on their own host thread,
 // then concatenated in domain order (the layout does not depend on the thread count).
 void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<float>& svox0,
-              const std::vector<Tile>& fine_i, double nu, int nen, int threads) {
+              const std::vector<Tile>& fine_i, const std::vector<Tile>& fine_w, double nu, int nen, int threads) {
   const int ndom = (int)doms0.size();
   double kh[576];
   voxel_stiffness(8, nu, kh);
@@ -1358,7 +1366,7 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
   struct Level {
     DomDev C;
     std::vector<float> sv;
-    std::vector<Tile> t_in, t_sm, t_all;
+    std::vector<Tile> t_in, t_sm, t_all, t_sw;
     std::vector<int32_t> n_in;   // active interior nodes (index inside the level's grid)
   };
   std::vector<std::vector<Level>> lev(ndom);
@@ -1397,10 +1405,10 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
               for (int b = 0; b < 2; ++b)
                 for (int a = 0; a < 2; ++a) act[(x + a) + (size_t)nx * ((y + b) + (size_t)ny * (z + c))] = 1;
           }
-      auto any = [&](int x0, int y0, int z0, int lo, int hx, int hy, int hz) {
+      auto any = [&](int x0, int y0, int z0, int lo, int hx, int hy, int hz, int sx = kTileX) {
         for (int z = std::max(z0, lo); z < std::min(z0 + kTileZ, hz + 1); ++z)
           for (int y = std::max(y0, lo); y < std::min(y0 + kTileY, hy + 1); ++y)
-            for (int x = std::max(x0, lo); x < std::min(x0 + kTileX, hx + 1); ++x)
+            for (int x = std::max(x0, lo); x < std::min(x0 + sx, hx + 1); ++x)
               if (act[x + (size_t)nx * (y + (size_t)ny * z)]) return true;
         return false;
       };
@@ -1417,6 +1425,12 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
           for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
             if (any(x0, y0, z0, 0, nx - 1, ny - 1, nz - 1))
               Lv.t_all.push_back(Tile{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+      if (nlev[d] > l + 1)
+        for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
+          for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
+            for (int x0 = 1; x0 <= nx - 2; x0 += kSweepX)
+              if (any(x0, y0, z0, 1, nx - 2, ny - 2, nz - 2, kSweepX))
+                Lv.t_sw.push_back(Tile{d, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
       for (int z = 1; z < nz - 1; ++z)
         for (int y = 1; y < ny - 1; ++y)
           for (int x = 1; x < nx - 1; ++x) {
@@ -1436,6 +1450,7 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
   P.nlev = nl;
   P.doms.assign((size_t)nl * ndom, DomDev{});
   P.sm_off.assign(nl, 0); P.sm_n.assign(nl, 0); P.in_off.assign(nl, 0); P.in_n.assign(nl, 0);
+  P.sw_off.assign(nl, 0); P.sw_n.assign(nl, 0);
   P.all_off.assign(nl, 0); P.all_n.assign(nl, 0); P.list_off.assign(nl, 0); P.list_n.assign(nl, 0);
   P.nl_off.assign(nl, 0); P.nl_n.assign(nl, 0);
   P.tiles.clear(); P.lists.clear(); P.svox.clear(); P.nodes_l.clear(); P.nodes = 0;
@@ -1443,6 +1458,9 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
   P.sm_off[0] = 0;
   for (const Tile& t : fine_i) if (nlev[t.dom] > 1) P.tiles.push_back(t);
   P.sm_n[0] = (int64_t)P.tiles.size();
+  P.sw_off[0] = (int64_t)P.tiles.size();
+  for (const Tile& t : fine_w) if (nlev[t.dom] > 1) P.tiles.push_back(t);
+  P.sw_n[0] = (int64_t)P.tiles.size() - P.sw_off[0];
   for (int l = 1; l < nl; ++l) {
     for (int d = 0; d < ndom; ++d) {
       if (nlev[d] <= l) continue;
@@ -1462,6 +1480,7 @@ void build_mg(MgPlan& P, const std::vector<DomDev>& doms0, const std::vector<flo
     append(&Level::t_sm, P.sm_off[l], P.sm_n[l]);
     append(&Level::t_in, P.in_off[l], P.in_n[l]);
     append(&Level::t_all, P.all_off[l], P.all_n[l]);
+    append(&Level::t_sw, P.sw_off[l], P.sw_n[l]);
     P.nl_off[l] = (int64_t)P.nodes_l.size();
     for (int d = 0; d < ndom; ++d)
       if (nlev[d] > l)
@@ -1503,12 +1522,14 @@ struct MgDev {
 
 // The HEX08 residual and post-smoothing sweeps with the tuned register budget (the fine
 // level's choice, used on the coarse levels too).
+// t: sweep tiles (rows of kSweepX nodes), g = 3 x their number.
 template <int MODE, bool DOT>
 void launch_mg_matvec(int minb, unsigned g, cudaStream_t s, const Tile* t, const DomDev* d, const float* sv,
                       const float* bi, const float* b, const float* u, float* y, float om, double* a1, double* a2,
                       const int* act) {
-  if (minb == 5) k_mg_matvec<MODE, DOT, 5><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act);
-  else k_mg_matvec<MODE, DOT, 4><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act);
+  if (g == 0) return;
+  if (minb == 5) k_mg_matvec<MODE, DOT, 5><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act, kSweepX);
+  else k_mg_matvec<MODE, DOT, 4><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act, kSweepX);
 }
 
 // t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_flat)
@@ -1545,6 +1566,8 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   }
   const Tile* tsm = M.tiles + P.sm_off[l];
   const unsigned g = (unsigned)(3 * nsm);
+  const Tile* tsw = M.tiles + P.sw_off[l];        // the slab sweeps' rows of kSweepX nodes
+  const unsigned gw = (unsigned)(3 * P.sw_n[l]);
   int q = -1;
   if (!(fine && t_ready)) {
     q = fine ? I.begin(0) : -1;
@@ -1563,7 +1586,7 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   float* cur = t;                  // the smoothed iterate
   float* rbuf = z;                 // the residual handed to the restriction
   if (twice) {
-    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, gw, s, tsw, dl, sv, bi, b, t, z, om, nullptr, nullptr, act);
     ++launches;
     cur = z;
     rbuf = t;
@@ -1578,9 +1601,9 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   } else if (fine && I.tensor_matvec) {
     launch_sweep_tc(kTcRes, tsm, nsm, dl, sv, fl, bi, b, cur, rbuf, 1.0f, om, nullptr, nullptr, act, M.err, s);
   } else if (fine) {
-    launch_mg_matvec<kMgRes, false>(M.minb_res, g, s, tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
+    launch_mg_matvec<kMgRes, false>(M.minb_res, gw, s, tsw, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   } else {
-    launch_mg_matvec<kMgRes, false>(M.minb_res, g, s, tsm, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
+    launch_mg_matvec<kMgRes, false>(M.minb_res, gw, s, tsw, dl, sv, bi, b, cur, rbuf, om, nullptr, nullptr, act);
   }
   if (fine) I.end(kcMgResidual, q, mb + vb, mf);          // t in, r out (mb), b in
   const DomDev* dc = M.doms + (size_t)(l + 1) * M.ndom;
@@ -1615,14 +1638,14 @@ void mg_vcycle(DeviceSolver::Impl& I, const MgDev& M, int l, const float* r0, do
   } else if (l == 0 && I.tensor_matvec)
     launch_sweep_tc(kTcPost, tsm, nsm, dl, sv, fl, bi, b, t, z, 1.0f, P.omega0, zz, zr, act, M.err, s);
   else if (l == 0)
-    launch_mg_matvec<kMgPost, true>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
+    launch_mg_matvec<kMgPost, true>(M.minb_post, gw, s, tsw, dl, sv, bi, b, t, z, P.omega0, zz, zr, act);
   else if (twice) {
     // z holds the corrected iterate: t = z + w D^-1 (b - K z), then z = t + w D^-1 (b - K t)
-    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, z, t, P.omega, nullptr, nullptr, act);
-    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, gw, s, tsw, dl, sv, bi, b, z, t, P.omega, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, gw, s, tsw, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
     ++launches;
   } else
-    launch_mg_matvec<kMgPost, false>(M.minb_post, g, s, tsm, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
+    launch_mg_matvec<kMgPost, false>(M.minb_post, gw, s, tsw, dl, sv, bi, b, t, z, P.omega, nullptr, nullptr, act);
   if (fine) I.end(kcMgPost, q, mb + vb + vb / 12, mf);     // t in, z out (mb), b in, D^-1
   if (!fine) I.end(kcMgCoarse, q1, 0, 0);
   launches += 2;
@@ -1712,10 +1735,11 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   cudaStream_t s = I.stream;
   static const MgPlan kNoLevels;
   const MgPlan& P = M ? *M->P : kNoLevels;
-  const int nseg = 3 + 4 * P.nlev;
+  const int nseg = 4 + 5 * P.nlev;
   int e;
   if ((e = ensure(I, bCompactCnt, sizeof(int) * nseg, msg))) return e;
   if ((e = ensure(I, bTilesIc, sizeof(Tile) * std::max<int64_t>(W.nti, 1), msg))) return e;
+  if ((e = ensure(I, bTilesWc, sizeof(Tile) * std::max<int64_t>(W.ntw, 1), msg))) return e;
   if ((e = ensure(I, bNodesIc, sizeof(int64_t) * std::max<int64_t>(W.nnodes, 1), msg))) return e;
   if ((e = ensure(I, bBricksIc, sizeof(Tile) * std::max<int64_t>(W.nbi, 1), msg))) return e;
   if ((e = ensure(I, bMgTilesC, sizeof(Tile) * std::max<size_t>(P.tiles.size(), 1), msg))) return e;
@@ -1724,6 +1748,7 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   int* cnt = B<int>(I, bCompactCnt);
   DTC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * nseg, s));
   Tile* tc = B<Tile>(I, bTilesIc);
+  Tile* wc = B<Tile>(I, bTilesWc);
   int64_t* nc = B<int64_t>(I, bNodesIc);
   Tile* bc = B<Tile>(I, bBricksIc);
   Tile* mt = B<Tile>(I, bMgTilesC);
@@ -1732,11 +1757,13 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   launch_compact(W.ti, W.nti, act, tc, cnt + 0, s);
   launch_compact(W.nodes, W.nnodes, act, nc, cnt + 1, s);
   launch_compact(W.bi, W.nbi, act, bc, cnt + 2, s);
+  launch_compact(W.tw, W.ntw, act, wc, cnt + 3, s);
   for (int l = 0; l < P.nlev; ++l) {
-    launch_compact(M->tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 3 + 4 * l, s);
-    launch_compact(M->tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 4 + 4 * l, s);
-    launch_compact(M->lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 5 + 4 * l, s);
-    launch_compact(M->nodes + P.nl_off[l], P.nl_n[l], act, mn + P.nl_off[l], cnt + 6 + 4 * l, s);
+    launch_compact(M->tiles + P.sm_off[l], P.sm_n[l], act, mt + P.sm_off[l], cnt + 4 + 5 * l, s);
+    launch_compact(M->tiles + P.in_off[l], P.in_n[l], act, mt + P.in_off[l], cnt + 5 + 5 * l, s);
+    launch_compact(M->lists + P.list_off[l], P.list_n[l], act, ml + P.list_off[l], cnt + 6 + 5 * l, s);
+    launch_compact(M->nodes + P.nl_off[l], P.nl_n[l], act, mn + P.nl_off[l], cnt + 7 + 5 * l, s);
+    launch_compact(M->tiles + P.sw_off[l], P.sw_n[l], act, mt + P.sw_off[l], cnt + 8 + 5 * l, s);
   }
   launches += nseg;
   if ((e = launch_check(msg))) return e;
@@ -1746,6 +1773,7 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
   Wc.ti = tc; Wc.nti = h[0];
   Wc.nodes = nc; Wc.nnodes = h[1];
   Wc.bi = bc; Wc.nbi = h[2];
+  Wc.tw = wc; Wc.ntw = h[3];
   if (M) {
     Mc->bricks0 = bc; Mc->nbricks0 = h[2];
     Mc->nodes0 = nc; Mc->nnodes0 = h[1];
@@ -1753,10 +1781,11 @@ int compact_lists(DeviceSolver::Impl& I, const Work& W, const MgDev* M, const in
     Mc->lists = ml;
     Mc->nodes = mn;
     for (int l = 0; l < P.nlev; ++l) {
-      Pc->sm_n[l] = h[3 + 4 * l];
-      Pc->in_n[l] = h[4 + 4 * l];
-      Pc->list_n[l] = h[5 + 4 * l];
-      Pc->nl_n[l] = h[6 + 4 * l];
+      Pc->sm_n[l] = h[4 + 5 * l];
+      Pc->in_n[l] = h[5 + 5 * l];
+      Pc->list_n[l] = h[6 + 5 * l];
+      Pc->nl_n[l] = h[7 + 5 * l];
+      Pc->sw_n[l] = h[8 + 5 * l];
     }
   }
   return DTC_OK;
@@ -1853,6 +1882,7 @@ int run_cg_mg(DeviceSolver::Impl& I, int ndom, const Work& W, const MgDev& M, fl
   MgPlan Pc;   // offsets and counts of the multigrid lists (no bulk data)
   Pc.nlev = M.P->nlev; Pc.omega = M.P->omega; Pc.omega0 = M.P->omega0;
   Pc.sm_off = M.P->sm_off; Pc.sm_n = M.P->sm_n; Pc.in_off = M.P->in_off; Pc.in_n = M.P->in_n;
+  Pc.sw_off = M.P->sw_off; Pc.sw_n = M.P->sw_n;
   Pc.list_off = M.P->list_off; Pc.list_n = M.P->list_n;
   Pc.nl_off = M.P->nl_off; Pc.nl_n = M.P->nl_n;
   MgDev Mc = M;
@@ -2051,6 +2081,8 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, co
   double* zz = B<double>(I, bZz);
   double* zr = B<double>(I, bZr);
   const unsigned g = (unsigned)(3 * nsm);
+  const Tile* tsw = M.tiles + M.P->sw_off[0];
+  const unsigned gw = (unsigned)(3 * M.P->sw_n[0]);
   TuneResult r{0, {0.f, 0.f}};
   int e;
   for (int cand = 0; cand < 2; ++cand) {
@@ -2063,8 +2095,8 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, co
           launch_ebe_tc(M.bricks0, M.nbricks0, M.doms0, M.svox0, M.flags0, W.ke20tc, M.t0, M.z0, -1.0, nullptr,
                         nullptr, M.err, s);
       } else if (cand == 0) {
-        k_mg_matvec<kMgPost, true, 4><<<g, kThreads, 0, s>>>(tsm, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0,
-                                                             M.P->omega0, zz, zr, nullptr);
+        launch_mg_matvec<kMgPost, true>(4, gw, s, tsw, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0, zz,
+                                        zr, nullptr);
       } else {
         launch_sweep_tc(kTcPost, tsm, nsm, M.doms0, M.svox0, M.flags0, M.binv0, b, M.t0, M.z0, 1.0f, M.P->omega0, zz,
                         zr, nullptr, M.err, s);
@@ -2079,14 +2111,14 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, co
     for (int v = 0; v < 2; ++v) {
       const int minb = 4 + v;
       auto res = [&]() {
-        launch_mg_matvec<kMgRes, false>(minb, g, s, tsm, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0,
+        launch_mg_matvec<kMgRes, false>(minb, gw, s, tsw, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0,
                                         nullptr, nullptr, nullptr);
       };
       if ((e = time_launches(s, res, r.shape_ms[0][v], msg))) return e;
       if (v == 1) {
         auto post = [&]() {
-          launch_mg_matvec<kMgPost, true>(minb, g, s, tsm, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0, zz,
-                                          zr, nullptr);
+          launch_mg_matvec<kMgPost, true>(minb, gw, s, tsw, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0,
+                                          zz, zr, nullptr);
         };
         if ((e = time_launches(s, post, r.shape_ms[1][v], msg))) return e;
       }
@@ -2148,6 +2180,7 @@ struct HostBatch {
   std::vector<int64_t> tidx;   // tasks solved in this pass
   std::vector<DomDev> doms;
   std::vector<Tile> tiles_i, tiles_a, bricks_i, bricks_a;
+  std::vector<Tile> tiles_w;   // interior sweep tiles (rows of kSweepX nodes)
   std::vector<int64_t> nodes_i;
   std::vector<float> svox;
   int64_t node_total = 0;
@@ -2187,7 +2220,7 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
   // per domain: voxel factors, node activity and work lists (host threads)
   struct Packed {
     DomDev D;
-    std::vector<Tile> ti, ta, bi, ba;
+    std::vector<Tile> ti, ta, bi, ba, tw;
     std::vector<int64_t> ni;
     double vec = 0, mv = 0, fl = 0;
   };
@@ -2263,6 +2296,12 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
         for (int x0 = 1; x0 <= nx - 2; x0 += kTileX)
           if (any_active(x0, y0, z0, kTileX, kTileY, kTileZ, 1, nx - 2, ny - 2, nz - 2))
             out.ti.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
+    // sweep tiles (the slab sweeps over the interior): rows of kSweepX nodes
+    for (int z0 = 1; z0 <= nz - 2; z0 += kTileZ)
+      for (int y0 = 1; y0 <= ny - 2; y0 += kTileY)
+        for (int x0 = 1; x0 <= nx - 2; x0 += kSweepX)
+          if (any_active(x0, y0, z0, kSweepX, kTileY, kTileZ, 1, nx - 2, ny - 2, nz - 2))
+            out.tw.push_back(Tile{dom, (int16_t)x0, (int16_t)y0, (int16_t)z0, 0});
     for (int z0 = 0; z0 <= nz - 1; z0 += kTileZ)
       for (int y0 = 0; y0 <= ny - 1; y0 += kTileY)
         for (int x0 = 0; x0 <= nx - 1; x0 += kTileX)
@@ -2287,6 +2326,7 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
     doms.push_back(q.D);
     tiles_i.insert(tiles_i.end(), q.ti.begin(), q.ti.end());
     tiles_a.insert(tiles_a.end(), q.ta.begin(), q.ta.end());
+    hb.tiles_w.insert(hb.tiles_w.end(), q.tw.begin(), q.tw.end());
     bricks_i.insert(bricks_i.end(), q.bi.begin(), q.bi.end());
     bricks_a.insert(bricks_a.end(), q.ba.begin(), q.ba.end());
     nodes_i.insert(nodes_i.end(), q.ni.begin(), q.ni.end());
@@ -2298,7 +2338,7 @@ int prepare_nen(std::vector<DomainTask>& tasks, const dtc_options& opt, double n
   // multigrid plan of the mixed inner solve (HEX08 levels; HEX20 starts with p-coarsening)
   if (opt.precision == DTC_PREC_MIXED && opt.inner_precond == 2 && !tiles_i.empty()) {
     const auto tb = std::chrono::steady_clock::now();
-    build_mg(hb.mg, doms, svox, tiles_i, nu, NEN, opt.host_threads);
+    build_mg(hb.mg, doms, svox, tiles_i, hb.tiles_w, nu, NEN, opt.host_threads);
     hb.has_mg = true;
     hb.ms_mg = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
   }
@@ -2400,6 +2440,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   if ((e = ensure(I, bDoms, sizeof(DomDev) * ndom, msg))) return e;
   if ((e = ensure(I, bTilesI, sizeof(Tile) * std::max<int64_t>(nti, 1), msg))) return e;
   if ((e = ensure(I, bTilesA, sizeof(Tile) * std::max<int64_t>(nta, 1), msg))) return e;
+  const int64_t ntw = (int64_t)hb.tiles_w.size();
+  if ((e = ensure(I, bTilesW, sizeof(Tile) * std::max<int64_t>(ntw, 1), msg))) return e;
   if ((e = ensure(I, bBricksI, sizeof(Tile) * std::max<int64_t>(nbi, 1), msg))) return e;
   if ((e = ensure(I, bBricksA, sizeof(Tile) * std::max<int64_t>(nba, 1), msg))) return e;
   I.svox_dev = nullptr;
@@ -2449,6 +2491,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   DTC_CUDA(cudaMemcpyAsync(I.bufs[bDoms], doms.data(), sizeof(DomDev) * ndom, cudaMemcpyHostToDevice, s));
   if (nti) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesI], tiles_i.data(), sizeof(Tile) * nti, cudaMemcpyHostToDevice, s));
   if (nta) DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesA], tiles_a.data(), sizeof(Tile) * nta, cudaMemcpyHostToDevice, s));
+  if (ntw)
+    DTC_CUDA(cudaMemcpyAsync(I.bufs[bTilesW], hb.tiles_w.data(), sizeof(Tile) * ntw, cudaMemcpyHostToDevice, s));
   if (nbi) DTC_CUDA(cudaMemcpyAsync(I.bufs[bBricksI], bricks_i.data(), sizeof(Tile) * nbi, cudaMemcpyHostToDevice, s));
   if ((e = ensure(I, bNodesI, sizeof(int64_t) * std::max<size_t>(nodes_i.size(), 1), msg))) return e;
   if (!nodes_i.empty())
@@ -2480,6 +2524,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
   Work W{ti, ta, B<Tile>(I, bBricksI), B<Tile>(I, bBricksA), nti, nta, nbi, nba,
                B<int64_t>(I, bNodesI), (int64_t)nodes_i.size(), ke64,
                ke64 ? reinterpret_cast<const float*>(ke64 + 3600) : nullptr, ke20tc, B<int>(I, bErr)};
+  W.tw = B<Tile>(I, bTilesW);
+  W.ntw = ntw;
   const DomDev* dd = B<DomDev>(I, bDoms);
   uint8_t* fl = B<uint8_t>(I, bFlags);
   double* X = B<double>(I, bX);
@@ -2506,7 +2552,7 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
       mgp = std::move(hb.mg);
     } else {
       const auto tb = std::chrono::steady_clock::now();
-      build_mg(mgp, doms, svox, tiles_i, nu, NEN, opt.host_threads);
+      build_mg(mgp, doms, svox, tiles_i, hb.tiles_w, nu, NEN, opt.host_threads);
       stats_.kc[kcHostMgBuild].ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
       stats_.kc[kcHostMgBuild].launches += 1;
     }

@@ -41,14 +41,15 @@ constexpr int64_t kListNodeMask = (int64_t(1) << kListShift) - 1;
 // Residual / smoother on one level's interior tiles (the slab sweep of k_matvec).
 //   kMgRes : y = b - K u
 //   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
-// MINB: CTAs per SM the register allocation is sized for (4: at most 128 registers; 5: 102)
+// MINB: CTAs per SM the register allocation is sized for (4: at most 128 registers; 5: 102);
+// xlen: nodes per row of the tile list (kSweepX)
 template <int MODE, bool DOT, int MINB = 4>
 __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                         const float* __restrict__ svox,
                                                         const float* __restrict__ binv, const float* __restrict__ b,
                                                         const float* __restrict__ u, float* __restrict__ y, float omega,
                                                         double* __restrict__ acc_zz, double* __restrict__ acc_zr,
-                                                        const int* __restrict__ dom_active) {
+                                                        const int* __restrict__ dom_active, int xlen) {
   __shared__ double red[32];
   const Tile t = tiles[blockIdx.x / 3];
   if (dom_active && !dom_active[t.dom]) return;
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __rest
     V.load(sv);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
     W.apply<true>(sv, cur, nxt);
-    const int xe = min(D.n[0] - 2, t.x0 + kTileX - 1);
+    const int xe = min(D.n[0] - 2, t.x0 + xlen - 1);
 #pragma unroll 1
     for (int x = t.x0; x <= xe; ++x) {
       W.advance<false>(u, D, x + 1, yy, zz, lc);
