@@ -29,14 +29,13 @@ TARGET = 1e-5
 # the loosest one whose tensors stay within TARGET / 2 of an FP64 rtol-1e-10 solve on a sample
 LADDER = [float(f"{m}e-{k}") for k in range(3, 10) for m in (5, 3, 2, 1)][3:]
 # rtol at which the reference algorithm (reaction projection, FP64) meets TARGET/2 on this
-# workload: what the plain FP64 GPU arm calibrates to on the 512 x 32^3 batch (3e-7, measured);
+# workload: what the plain FP64 GPU arm calibrates to on the 512 x 32^3 batch (5e-7, measured);
 # the host-only reference arm cannot calibrate itself
-REF_RTOL = 3e-7
+REF_RTOL = 5e-7
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the fine
 # sweeps, measured on 16 domains of 32^3 (profiles/k_matvec_k_mg_matvec_f32_16x32cubed.md: the
-# CG application before the register budgets were tuned, the residual at 5 CTAs per SM and the
-# post-smoothing at 4 with them)
-DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 0.96, "mg_residual_f32": 1.50, "mg_postsmooth_f32": 1.54}
+# three sweeps at 5 CTAs per SM over 16-node rows)
+DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 1.01, "mg_residual_f32": 1.56, "mg_postsmooth_f32": 1.59}
 # FP32 SIMT FMA peak, nominal: 148 SMs x 128 lanes x 2 flop x 1.965 GHz (the sweeps run on the
 # FMA pipe, not on tensor cores; the measured peaks cover HBM and bf16 tensor only)
 FP32_NOMINAL_TFLOPS = 74.4
