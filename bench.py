@@ -618,8 +618,8 @@ def main():
         us = {k[len("autotune_"):]: 1e3 * v["ms_total"] / max(v["launches"], 1) for k, v in tune.items()}
         autotune = {"timed_us_per_launch": us,
                     "pick": "tensor" if us.get("tc_sweep", 1e30) < us.get("simt_sweep", 1e30) else "simt",
-                    "note": "simt_sweep / tc_sweep: fine post-smoothing; *_4cta / *_5cta: the SIMT residual, "
-                            "post-smoothing and CG-application sweeps at 4 or 5 CTAs per SM; f64_*: the FP64 "
+                    "note": "simt_sweep / tc_sweep: fine post-smoothing; *_6cta / *_8cta: the SIMT residual, "
+                            "post-smoothing and CG-application sweeps at 6 or 8 CTAs per SM; f64_*: the FP64 "
                             "sweep at 1 or 3 CTAs per SM"}
     top = max((k for k in ks if ks[k]["bytes_per_launch"] > 0), key=lambda k: ks[k]["ms_total"])
     kt = ks[top]

@@ -80,7 +80,7 @@ typedef struct dtc_options {
                               1 = tcgen05 tensor cores (3xTF32 split, FP32-level accuracy),
                               2 = autotuned: multigrid solves time both kernels of the fine-level
                               operator on the batch's own tiles and keep the faster; for the HEX08
-                              SIMT sweeps also the register budget (4 or 5 CTAs per SM) of each of
+                              SIMT sweeps also the register budget (6 or 8 CTAs per SM) of each of
                               the residual, post-smoothing and CG-application sweeps, and for
                               every HEX08 solve that of the FP64 sweep (1 or 3 CTAs per SM);
                               cached per device and size class (dtc_get_kernel_stats lists the

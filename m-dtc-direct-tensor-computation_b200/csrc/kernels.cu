@@ -135,55 +135,57 @@ __device__ __forceinline__ void load_voxels(float (&sp)[2][2], const float* __re
 // FP32 slab on packed two-lane FMAs (sm_100 FFMA2).  A voxel of the row feeds two output rows
 // r of the thread's nodes: the corner at plane x (l0, node x) and the corner at plane x+1 (l1,
 // node x+1); one packed FMA applies both rows' entries of a column to one broadcast input value
-// (lane x: node x, lane y: node x+1), halving the FMA instructions of the scalar slab.  The table
-// holds the two rows' entries side by side, per voxel slot (b, c) of the row.
+// (lane x: node x, lane y: node x+1), halving the FMA instructions of the scalar slab (voxel_rp).
+// The table holds the two rows' entries side by side, per voxel slot (b, c) of the row.
 __constant__ float2 c_khat32r2[4 * 3 * 24];   // [2b + c][r][col] = (Khat[3 l0 + r, col], Khat[3 l1 + r, col])
 
+// Voxel-outer FP32 slab (the FP32 sweeps): the kept voxel (b, c) of the row between planes x
+// (rp: the row's values at plane x for its load case) and x+1 reads its own 8 corners' 24 values
+// (mostly L1 hits: neighbouring rows and voxels share them) and applies them with packed FMAs.
+// No node plane stays in registers between steps, which keeps a thread at 64-80 registers (6 or
+// 8 CTAs per SM) where the two-plane register window needed ~100.
 template <bool FIRST>
-__device__ __forceinline__ void slab_rp(const float (&P0)[3][3][3], const float (&P1)[3][3][3], const float (&sv)[2][2],
-                                        float (&cur)[3], float (&nxt)[3]) {
-  if (FIRST) {
-    slab<float, true>(P0, P1, sv, cur, nxt);
-    return;
+__device__ __forceinline__ void voxel_rp(const float* __restrict__ rp, int sy, int sz, int b, int c, float s,
+                                         float (&cur)[3], float (&nxt)[3]) {
+  float2 acc[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) acc[r] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int mz = 0; mz < 2; ++mz)
+#pragma unroll
+    for (int my = 0; my < 2; ++my)
+#pragma unroll
+      for (int mx = 0; mx < 2; ++mx) {
+        const int lm = corner_local(mx, my, mz);
+        const float* q = rp + mx * (3 * kNLC) + (b - 1 + my) * sy + (c - 1 + mz) * sz;
+#pragma unroll
+        for (int cj = 0; cj < 3; ++cj) {
+          const float v = __ldg(q + cj * kNLC);
+          const float2 vv = make_float2(v, v);
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+            acc[r] = __ffma2_rn(c_khat32r2[((2 * b + c) * 3 + r) * 24 + 3 * lm + cj], vv, acc[r]);
+        }
+      }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    if (!FIRST) cur[r] = fmaf(s, acc[r].x, cur[r]);
+    nxt[r] = fmaf(s, acc[r].y, nxt[r]);
   }
+}
+template <bool FIRST>
+__device__ __forceinline__ void row_slab(const float* __restrict__ rp, int sy, int sz, const float (&sv)[2][2],
+                                         float (&cur)[3], float (&nxt)[3]) {
 #pragma unroll
   for (int b = 0; b < 2; ++b)
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const float s = sv[b][c];
-      if (s != 0.0f) {
-        float2 acc[3];
-#pragma unroll
-        for (int r = 0; r < 3; ++r) acc[r] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int mz = 0; mz < 2; ++mz)
-#pragma unroll
-          for (int my = 0; my < 2; ++my)
-#pragma unroll
-            for (int mx = 0; mx < 2; ++mx) {
-              const int lm = corner_local(mx, my, mz);
-#pragma unroll
-              for (int cj = 0; cj < 3; ++cj) {
-                const float v = mx ? P1[b + my][c + mz][cj] : P0[b + my][c + mz][cj];
-                const float2 vv = make_float2(v, v);
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-                  acc[r] = __ffma2_rn(c_khat32r2[((2 * b + c) * 3 + r) * 24 + 3 * lm + cj], vv, acc[r]);
-              }
-            }
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-          cur[r] = fmaf(s, acc[r].x, cur[r]);
-          nxt[r] = fmaf(s, acc[r].y, nxt[r]);
-        }
-      }
-    }
+    for (int c = 0; c < 2; ++c)
+      if (sv[b][c] != 0.0f) voxel_rp<FIRST>(rp, sy, sz, b, c, sv[b][c], cur, nxt);
 }
 
-// Two-plane register window of the slab sweeps: load the first two planes, advance by one
-// plane, apply the slab between them, read the centre value of plane x.  PACKED: the FP32
-// slab on packed FMAs (slab_rp); otherwise scalar FMAs (FP64, and the FP32 reference form).
-template <typename T, bool PACKED = false> struct Win {
+// Two-plane register window of the FP64 slab sweeps: load the first two planes, advance by one
+// plane, apply the slab between them (scalar FMAs), read the centre value of plane x.
+template <typename T> struct Win {
   T P0[3][3][3], P1[3][3][3];
   // unguarded sweeps: the row's values at plane x+1 (the plane loaded last) for its load case,
   // and the offsets of the neighbour rows in y and z (one 64-bit pointer, 32-bit offsets)
@@ -255,12 +257,6 @@ struct VoxRow {
       for (int c = 0; c < 2; ++c) sp[b][c] = __ldg(p + b * sy + c * sz);
   }
 };
-template <> struct Win<float, true> : Win<float, false> {
-  template <bool FIRST>
-  __device__ __forceinline__ void apply(const float (&sv)[2][2], float (&cur)[3], float (&nxt)[3]) const {
-    slab_rp<FIRST>(P0, P1, sv, cur, nxt);
-  }
-};
 
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
@@ -268,9 +264,9 @@ template <> struct Win<float, true> : Win<float, false> {
 // kSweepX).  bnd_only: u vanishes off the domain box (the boundary
 // values before the first solve) and y is zero on entry; a row whose neighbour rows lie
 // inside the box then only has nonzero output at x = 1 and x = n0 - 2, and computes only those.
-// MINB: CTAs per SM the register allocation is sized for; FP32 4 (at most 128 registers) or 5,
+// MINB: CTAs per SM the register allocation is sized for; FP32 6 (at most 80 registers) or 8 (64),
 // FP64 1 (255) or 3 (168), chosen per batch class by the sweep autotuner
-template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 4 : 1)>
+template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 6 : 1)>
 __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restrict__ tiles,
                                                                           const DomDev* __restrict__ doms,
                                                      const float* __restrict__ svox, const T* __restrict__ u,
@@ -294,8 +290,40 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
     else if (!has_lo) xe = x0 - 1;   // neither: nothing to compute on this row
   }
   double dot = 0.0;
-  if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi && x0 <= xe) {
-    Win<T, sizeof(T) == 4> W;
+  if constexpr (!ALL && sizeof(T) == 4) {
+    if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi && x0 <= xe) {
+      const int sy = D.n[0] * (3 * kNLC), sz = D.n[0] * D.n[1] * (3 * kNLC);
+      const float* rp = u + vec_index(node_index(D, x0 - 1, yy, zz), 0, lc);   // plane x0 - 1
+      VoxRow V;
+      float sv[2][2];
+      float cur[3] = {0.f, 0.f, 0.f}, nxt[3] = {0.f, 0.f, 0.f};
+      V.start(svox, D, x0 - 1, yy, zz);
+      V.load(sv);
+      bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
+      row_slab<true>(rp, sy, sz, sv, cur, nxt);
+#pragma unroll 1
+      for (int x = x0; x <= xe; ++x) {
+        rp += 3 * kNLC;   // plane x
+        ++V.p;
+        V.load(sv);
+        const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = 0.f; }
+        row_slab<false>(rp, sy, sz, sv, cur, nxt);
+        if (anyp | anyc) {
+          const int64_t b = rp - u;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float v = (float)(scale * D.scale * (double)cur[c]);
+            y[b + c * kNLC] = v;
+            if (DOT) dot += (double)__ldg(rp + c * kNLC) * (double)v;
+          }
+        }
+        anyp = anyc;
+      }
+    }
+  } else if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi && x0 <= xe) {
+    Win<T> W;
     VoxRow V;
     float sv[2][2];
     T cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
@@ -1143,7 +1171,7 @@ struct Work {
   const float* ke32;
   const float* ke20tc;  // HEX20 FP32 applications on tcgen05: split matrix in the B layout, else null
   int* err;             // mbarrier time-out flag of the tensor-core kernels
-  int minb32 = 4;       // HEX08 slab sweeps: CTAs per SM of the FP32 CG application (4 or 5)
+  int minb32 = 6;       // HEX08 slab sweeps: CTAs per SM of the FP32 CG application (6 or 8)
   int minb64 = 1;       //                    and of every FP64 application (1 or 3)
   const Tile* tw = nullptr;   // interior sweep tiles (rows of kSweepX nodes) of the slab sweeps
   int64_t ntw = 0;
@@ -1161,8 +1189,8 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
     const Tile* tl = ALL ? W.ta : W.tw;
     const int xl = ALL ? kTileX : kSweepX;
     if constexpr (sizeof(T) == 4) {
-      if (W.minb32 == 5) k_matvec<T, ALL, DOT, 5><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
-      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
+      if (W.minb32 == 8) k_matvec<T, ALL, DOT, 8><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
+      else k_matvec<T, ALL, DOT, 6><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
     } else {
       if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
       else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
@@ -1517,7 +1545,7 @@ struct MgDev {
   const float* ke32;     // HEX20 unit element matrix (FP32)
   const float* ke20tc;   // its tensor-core operand, or null (brick SIMT kernel)
   int* err;
-  int minb_res = 4, minb_post = 4;   // HEX08 fine-level residual / post-smoothing sweeps: CTAs per SM
+  int minb_res = 6, minb_post = 6;   // HEX08 residual / post-smoothing sweeps: CTAs per SM (6 or 8)
 };
 
 // The HEX08 residual and post-smoothing sweeps with the tuned register budget (the fine
@@ -1528,8 +1556,8 @@ void launch_mg_matvec(int minb, unsigned g, cudaStream_t s, const Tile* t, const
                       const float* bi, const float* b, const float* u, float* y, float om, double* a1, double* a2,
                       const int* act) {
   if (g == 0) return;
-  if (minb == 5) k_mg_matvec<MODE, DOT, 5><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act, kSweepX);
-  else k_mg_matvec<MODE, DOT, 4><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act, kSweepX);
+  if (minb == 8) k_mg_matvec<MODE, DOT, 8><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act, kSweepX);
+  else k_mg_matvec<MODE, DOT, 6><<<g, kThreads, 0, s>>>(t, d, sv, bi, b, u, y, om, a1, a2, act, kSweepX);
 }
 
 // t_ready: the fine-level t = omega D^-1 r0 was already written (by k_update_flat)
@@ -1990,10 +2018,10 @@ struct TuneKey {
 };
 struct TuneResult {
   int pick;            // 0 = SIMT, 1 = tensor cores
-  float ms[2];         // the timed launches of each candidate (post-smoothing; SIMT at 4 CTAs/SM)
+  float ms[2];         // the timed launches of each candidate (post-smoothing; SIMT at 6 CTAs/SM)
   // HEX08 SIMT slab sweeps: CTAs per SM of the residual, post-smoothing and CG application
-  // sweeps, and the timed launches at 4 and 5 CTAs per SM (index 0 / 1)
-  int minb[3] = {4, 4, 4};
+  // sweeps, and the timed launches at 6 and 8 CTAs per SM (index 0 / 1)
+  int minb[3] = {6, 6, 6};
   float shape_ms[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
 };
 std::mutex g_tune_mu;
@@ -2052,7 +2080,7 @@ TuneKey tune_key(int device, int nen, const std::vector<DomDev>& doms, const std
 // by CUDA-event timings on the batch's own tiles and vectors:
 //  * HEX08: the SIMT slab sweep or the tcgen05 sweep (timed on the post-smoothing sweep); for
 //    the SIMT sweep also the register budget of each of its three kernels -- residual,
-//    post-smoothing, CG application -- at 4 CTAs per SM (128 registers) or 5 (102);
+//    post-smoothing, CG application -- at 6 CTAs per SM (80 registers) or 8 (64);
 //  * HEX20: the SIMT brick kernel or the tcgen05 brick kernel (the operator of the residual and
 //    post-smoothing steps and of the CG application).
 int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, const std::vector<DomDev>& doms,
@@ -2106,10 +2134,10 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, co
   }
   r.pick = r.ms[1] < r.ms[0] ? 1 : 0;
   if (nen == 8 && r.pick == 0) {
-    // register budgets of the three SIMT sweeps (the post-smoothing at 4 CTAs/SM is ms[0])
+    // register budgets of the three SIMT sweeps (the post-smoothing at 6 CTAs/SM is ms[0])
     r.shape_ms[1][0] = r.ms[0];
     for (int v = 0; v < 2; ++v) {
-      const int minb = 4 + v;
+      const int minb = v == 0 ? 6 : 8;
       auto res = [&]() {
         launch_mg_matvec<kMgRes, false>(minb, gw, s, tsw, M.doms0, M.svox0, M.binv0, b, M.t0, M.z0, M.P->omega0,
                                         nullptr, nullptr, nullptr);
@@ -2129,7 +2157,7 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, co
       };
       if ((e = time_launches(s, apply, r.shape_ms[2][v], msg))) return e;
     }
-    for (int k = 0; k < 3; ++k) r.minb[k] = r.shape_ms[k][1] < r.shape_ms[k][0] ? 5 : 4;
+    for (int k = 0; k < 3; ++k) r.minb[k] = r.shape_ms[k][1] < r.shape_ms[k][0] ? 8 : 6;
   }
   adopt(r);
   std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -2356,9 +2384,9 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
                                              "project_f64", "mg_jacobi_f32", "mg_residual_f32",
                                              "mg_postsmooth_f32", "mg_transfer_f32", "mg_coarse_levels_f32",
                                              "rotation_search_f64", "autotune_simt_sweep", "autotune_tc_sweep",
-                                             "autotune_res_sweep_4cta", "autotune_res_sweep_5cta",
-                                             "autotune_post_sweep_5cta", "autotune_apply_sweep_4cta",
-                                             "autotune_apply_sweep_5cta", "autotune_f64_sweep_1cta",
+                                             "autotune_res_sweep_6cta", "autotune_res_sweep_8cta",
+                                             "autotune_post_sweep_8cta", "autotune_apply_sweep_6cta",
+                                             "autotune_apply_sweep_8cta", "autotune_f64_sweep_1cta",
                                              "autotune_f64_sweep_3cta", "host_pack", "host_multigrid_build"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;

@@ -41,9 +41,9 @@ constexpr int64_t kListNodeMask = (int64_t(1) << kListShift) - 1;
 // Residual / smoother on one level's interior tiles (the slab sweep of k_matvec).
 //   kMgRes : y = b - K u
 //   kMgPost: y = u + omega D^-1 (b - K u);  DOT: zz += y.y, zr += y.b per (domain, load case)
-// MINB: CTAs per SM the register allocation is sized for (4: at most 128 registers; 5: 102);
+// MINB: CTAs per SM the register allocation is sized for (6: at most 80 registers; 8: 64);
 // xlen: nodes per row of the tile list (kSweepX)
-template <int MODE, bool DOT, int MINB = 4>
+template <int MODE, bool DOT, int MINB = 6>
 __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __restrict__ tiles, const DomDev* __restrict__ doms,
                                                         const float* __restrict__ svox,
                                                         const float* __restrict__ binv, const float* __restrict__ b,
@@ -59,27 +59,27 @@ __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __rest
   const int yy = t.y0 + (row & 3), zz = t.z0 + (row >> 2);
   double szz = 0.0, szr = 0.0;
   if (yy >= 1 && yy <= D.n[1] - 2 && zz >= 1 && zz <= D.n[2] - 2) {
-    Win<float, true> W;
+    const int sy = D.n[0] * (3 * kNLC), sz = D.n[0] * D.n[1] * (3 * kNLC);
+    const float* rp = u + vec_index(node_index(D, t.x0 - 1, yy, zz), 0, lc);   // plane x0 - 1
     VoxRow V;
     float sv[2][2];
     float cur[3] = {0.f, 0.f, 0.f}, nxt[3] = {0.f, 0.f, 0.f};
-    W.start<false>(u, D, t.x0 - 1, yy, zz, lc);
     V.start(svox, D, t.x0 - 1, yy, zz);
     V.load(sv);
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
-    W.apply<true>(sv, cur, nxt);
+    row_slab<true>(rp, sy, sz, sv, cur, nxt);
     const int xe = min(D.n[0] - 2, t.x0 + xlen - 1);
 #pragma unroll 1
     for (int x = t.x0; x <= xe; ++x) {
-      W.advance<false>(u, D, x + 1, yy, zz, lc);
+      rp += 3 * kNLC;   // plane x
       ++V.p;
       V.load(sv);
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
       for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = 0.f; }
-      W.apply<false>(sv, cur, nxt);
+      row_slab<false>(rp, sy, sz, sv, cur, nxt);
       if (anyp | anyc) {
-        const int64_t k0 = W.centre_index(u);
+        const int64_t k0 = rp - u;
         float res[3], bc[3], v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_mg_matvec(const Tile* __rest
           float dz[3];
           block_jacobi(binv, node_index(D, x, yy, zz), omega, res, dz);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) v[c] = W.centre(c) + dz[c];
+          for (int c = 0; c < 3; ++c) v[c] = __ldg(rp + c * kNLC) + dz[c];
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
