@@ -34,8 +34,9 @@ LADDER = [float(f"{m}e-{k}") for k in range(3, 10) for m in (5, 3, 2, 1)][3:]
 REF_RTOL = 5e-7
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the fine
 # sweeps, measured on 16 domains of 32^3 (profiles/k_matvec_k_mg_matvec_f32_16x32cubed.md: the
-# three sweeps at 5 CTAs per SM over 16-node rows)
-DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 1.01, "mg_residual_f32": 1.56, "mg_postsmooth_f32": 1.59}
+# voxel-outer sweeps at their tuned 6 or 8 CTAs per SM; below 1 where part of the input vector
+# was still in L2)
+DRAM_PER_ALGORITHMIC_BYTE = {"matvec_f32": 0.46, "mg_residual_f32": 0.97, "mg_postsmooth_f32": 1.01}
 # FP32 SIMT FMA peak, nominal: 148 SMs x 128 lanes x 2 flop x 1.965 GHz (the sweeps run on the
 # FMA pipe, not on tensor cores; the measured peaks cover HBM and bf16 tensor only)
 FP32_NOMINAL_TFLOPS = 74.4
