@@ -621,7 +621,7 @@ def main():
                     "pick": "tensor" if us.get("tc_sweep", 1e30) < us.get("simt_sweep", 1e30) else "simt",
                     "note": "simt_sweep / tc_sweep: fine post-smoothing; *_6cta / *_8cta: the SIMT residual, "
                             "post-smoothing and CG-application sweeps at 6 or 8 CTAs per SM; f64_*: the FP64 "
-                            "sweep at 1 or 3 CTAs per SM"}
+                            "sweep at 4 or 6 CTAs per SM"}
     top = max((k for k in ks if ks[k]["bytes_per_launch"] > 0), key=lambda k: ks[k]["ms_total"])
     kt = ks[top]
     t_launch = kt["ms_total"] / kt["launches"] / 1e3

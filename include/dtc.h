@@ -82,7 +82,7 @@ typedef struct dtc_options {
                               operator on the batch's own tiles and keep the faster; for the HEX08
                               SIMT sweeps also the register budget (6 or 8 CTAs per SM) of each of
                               the residual, post-smoothing and CG-application sweeps, and for
-                              every HEX08 solve that of the FP64 sweep (1 or 3 CTAs per SM);
+                              every HEX08 solve that of the FP64 sweep (4 or 6 CTAs per SM);
                               cached per device and size class (dtc_get_kernel_stats lists the
                               timings as autotune_* classes) */
   int32_t inner_precond;   /* preconditioner of the FP32 inner solve: 0 = Jacobi (as PETSc's

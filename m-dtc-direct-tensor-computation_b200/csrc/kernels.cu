@@ -49,73 +49,12 @@ template <> struct KhatC<double> {
 };
 
 // -------------------------------------------------------------------------------------
-// HEX08: matrix-free K*u on one node tile (the default SIMT operator of the corner grid).
-// A thread owns one (y, z) row of the tile for one load case and sweeps x.  Between node
-// planes x and x+1 lie the 4 voxels (x, y-1..y, z-1..z) of the row; each kept voxel
-// contributes s_v * Khat[rows of its corner, :] * u_v to node x (corner with offset 0 in x)
-// and to node x+1 (offset 1), both from one read of its 8 corner values held in the two
-// plane registers P0 (plane x) and P1 (plane x+1).  FIRST: the slab left of the tile, whose
-// contribution to the first node only is needed.
-template <typename T, bool FIRST>
-__device__ __forceinline__ void slab(const T (&P0)[3][3][3], const T (&P1)[3][3][3], const float (&sv)[2][2],
-                                     T (&cur)[3], T (&nxt)[3]) {
-#pragma unroll
-  for (int b = 0; b < 2; ++b)
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const float s = sv[b][c];
-      if (s != 0.0f) {
-        const int l0 = corner_local(0, 1 - b, 1 - c), l1 = corner_local(1, 1 - b, 1 - c);
-        T t0 = 0, t1 = 0, t2 = 0, q0 = 0, q1 = 0, q2 = 0;
-#pragma unroll
-        for (int mz = 0; mz < 2; ++mz)
-#pragma unroll
-          for (int my = 0; my < 2; ++my)
-#pragma unroll
-            for (int mx = 0; mx < 2; ++mx) {
-              const int lm = corner_local(mx, my, mz);
-#pragma unroll
-              for (int cj = 0; cj < 3; ++cj) {
-                const T v = mx ? P1[b + my][c + mz][cj] : P0[b + my][c + mz][cj];
-                const int col = 24 * (3 * lm + cj);
-                if (!FIRST) {
-                  t0 = fma(KhatC<T>::at(col + 3 * l0 + 0), v, t0);
-                  t1 = fma(KhatC<T>::at(col + 3 * l0 + 1), v, t1);
-                  t2 = fma(KhatC<T>::at(col + 3 * l0 + 2), v, t2);
-                }
-                q0 = fma(KhatC<T>::at(col + 3 * l1 + 0), v, q0);
-                q1 = fma(KhatC<T>::at(col + 3 * l1 + 1), v, q1);
-                q2 = fma(KhatC<T>::at(col + 3 * l1 + 2), v, q2);
-              }
-            }
-        const T ts = (T)s;
-        if (!FIRST) {
-          cur[0] = fma(ts, t0, cur[0]);
-          cur[1] = fma(ts, t1, cur[1]);
-          cur[2] = fma(ts, t2, cur[2]);
-        }
-        nxt[0] = fma(ts, q0, nxt[0]);
-        nxt[1] = fma(ts, q1, nxt[1]);
-        nxt[2] = fma(ts, q2, nxt[2]);
-      }
-    }
-}
-
-template <typename T, bool GUARD>
-__device__ __forceinline__ void load_plane(T (&pl)[3][3][3], const T* __restrict__ u, const DomDev& D, int x, int y,
-                                           int z, int lc) {
-#pragma unroll
-  for (int py = 0; py < 3; ++py)
-#pragma unroll
-    for (int pz = 0; pz < 3; ++pz) {
-      const int yy = y + py - 1, zz = z + pz - 1;
-      bool ok = true;
-      if (GUARD) ok = (x >= 0 && x < D.n[0] && yy >= 0 && yy < D.n[1] && zz >= 0 && zz < D.n[2]);
-      const int64_t base = ok ? vec_index(node_index(D, x, yy, zz), 0, lc) : 0;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) pl[py][pz][c] = ok ? __ldg(u + base + c * kNLC) : T(0);
-    }
-}
+// HEX08: matrix-free K*u on node rows (the default SIMT operator of the corner grid).  A thread
+// owns one (y, z) row of a tile for one load case and sweeps x.  Between node planes x and x+1
+// lie the 4 voxels (x, y-1..y, z-1..z) of the row; each kept voxel contributes
+// s_v * Khat[rows of its corner, :] * u_v to node x (corner with offset 0 in x) and to node x+1
+// (offset 1), both from one read of its 8 corner values (voxel_rp / voxel_rd below).  FIRST: the
+// slab left of the tile, whose contribution to the first node only is needed.
 
 template <bool GUARD>
 __device__ __forceinline__ void load_voxels(float (&sp)[2][2], const float* __restrict__ svox, const DomDev& D, int vx,
@@ -143,7 +82,7 @@ __constant__ float2 c_khat32r2[4 * 3 * 24];   // [2b + c][r][col] = (Khat[3 l0 +
 // (rp: the row's values at plane x for its load case) and x+1 reads its own 8 corners' 24 values
 // (mostly L1 hits: neighbouring rows and voxels share them) and applies them with packed FMAs.
 // No node plane stays in registers between steps, which keeps a thread at 64-80 registers (6 or
-// 8 CTAs per SM) where the two-plane register window needed ~100.
+// 8 CTAs per SM) where a window of two node planes in registers needed ~100.
 template <bool FIRST>
 __device__ __forceinline__ void voxel_rp(const float* __restrict__ rp, int sy, int sz, int b, int c, float s,
                                          float (&cur)[3], float (&nxt)[3]) {
@@ -183,62 +122,57 @@ __device__ __forceinline__ void row_slab(const float* __restrict__ rp, int sy, i
       if (sv[b][c] != 0.0f) voxel_rp<FIRST>(rp, sy, sz, b, c, sv[b][c], cur, nxt);
 }
 
-// Two-plane register window of the FP64 slab sweeps: load the first two planes, advance by one
-// plane, apply the slab between them (scalar FMAs), read the centre value of plane x.
-template <typename T> struct Win {
-  T P0[3][3][3], P1[3][3][3];
-  // unguarded sweeps: the row's values at plane x+1 (the plane loaded last) for its load case,
-  // and the offsets of the neighbour rows in y and z (one 64-bit pointer, 32-bit offsets)
-  const T* row = nullptr;
-  int sy = 0, sz = 0;
-  __device__ __forceinline__ void load_rel(T (&pl)[3][3][3], const T* __restrict__ p) const {
+// Voxel-outer FP64 slab (scalar FMAs, the summation order of slab): the kept voxel (b, c) of
+// the row between planes x and x+1 reads its 8 corners' values from u, kb being the index of the
+// row's value at plane x for its load case (negative when the row starts left of the grid: a
+// voxel inside the grid has all its corners inside it, so only kept voxels' corners are read).
+template <bool FIRST>
+__device__ __forceinline__ void voxel_rd(const double* __restrict__ u, int64_t kb, int sy, int sz, int b, int c,
+                                         float s, double (&cur)[3], double (&nxt)[3]) {
+  const int l0 = corner_local(0, 1 - b, 1 - c), l1 = corner_local(1, 1 - b, 1 - c);
+  double t0 = 0, t1 = 0, t2 = 0, q0 = 0, q1 = 0, q2 = 0;
+#pragma unroll 1
+  for (int mz = 0; mz < 2; ++mz)
 #pragma unroll
-    for (int py = 0; py < 3; ++py)
+    for (int my = 0; my < 2; ++my)
 #pragma unroll
-      for (int pz = 0; pz < 3; ++pz) {
-        const T* q = p + (py - 1) * sy + (pz - 1) * sz;
+      for (int mx = 0; mx < 2; ++mx) {
+        const int lm = corner_local(mx, my, mz);
+        const int64_t k = kb + mx * (3 * kNLC) + (b - 1 + my) * sy + (c - 1 + mz) * sz;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) pl[py][pz][c] = __ldg(q + c * kNLC);
+        for (int cj = 0; cj < 3; ++cj) {
+          const double v = __ldg(u + k + cj * kNLC);
+          const int col = 24 * (3 * lm + cj);
+          if (!FIRST) {
+            t0 = fma(KhatC<double>::at(col + 3 * l0 + 0), v, t0);
+            t1 = fma(KhatC<double>::at(col + 3 * l0 + 1), v, t1);
+            t2 = fma(KhatC<double>::at(col + 3 * l0 + 2), v, t2);
+          }
+          q0 = fma(KhatC<double>::at(col + 3 * l1 + 0), v, q0);
+          q1 = fma(KhatC<double>::at(col + 3 * l1 + 1), v, q1);
+          q2 = fma(KhatC<double>::at(col + 3 * l1 + 2), v, q2);
+        }
       }
+  const double ts = (double)s;
+  if (!FIRST) {
+    cur[0] = fma(ts, t0, cur[0]);
+    cur[1] = fma(ts, t1, cur[1]);
+    cur[2] = fma(ts, t2, cur[2]);
   }
-  template <bool GUARD>
-  __device__ __forceinline__ void start(const T* __restrict__ u, const DomDev& D, int x, int y, int z, int lc) {
-    if constexpr (GUARD) {
-      load_plane<T, true>(P0, u, D, x, y, z, lc);
-      load_plane<T, true>(P1, u, D, x + 1, y, z, lc);
-    } else {
-      sy = D.n[0] * (3 * kNLC);
-      sz = D.n[0] * D.n[1] * (3 * kNLC);
-      row = u + vec_index(node_index(D, x, y, z), 0, lc);
-      load_rel(P0, row);
-      row += 3 * kNLC;
-      load_rel(P1, row);
-    }
-  }
-  // next plane x (= the previous one + 1)
-  template <bool GUARD>
-  __device__ __forceinline__ void advance(const T* __restrict__ u, const DomDev& D, int x, int y, int z, int lc) {
+  nxt[0] = fma(ts, q0, nxt[0]);
+  nxt[1] = fma(ts, q1, nxt[1]);
+  nxt[2] = fma(ts, q2, nxt[2]);
+}
+template <bool FIRST>
+__device__ __forceinline__ void row_slab_d(const double* __restrict__ u, int64_t kb, int sy, int sz,
+                                           const float (&sv)[2][2], double (&cur)[3], double (&nxt)[3]) {
 #pragma unroll
-    for (int py = 0; py < 3; ++py)
+  for (int b = 0; b < 2; ++b)
 #pragma unroll
-      for (int pz = 0; pz < 3; ++pz)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) P0[py][pz][c] = P1[py][pz][c];
-    if constexpr (GUARD) {
-      load_plane<T, true>(P1, u, D, x, y, z, lc);
-    } else {
-      row += 3 * kNLC;
-      load_rel(P1, row);
-    }
-  }
-  template <bool FIRST>
-  __device__ __forceinline__ void apply(const float (&sv)[2][2], T (&cur)[3], T (&nxt)[3]) const {
-    slab<T, FIRST>(P0, P1, sv, cur, nxt);
-  }
-  __device__ __forceinline__ T centre(int c) const { return P0[1][1][c]; }
-  // unguarded sweeps: index of the centre node's first value (plane x) in the vector u
-  __device__ __forceinline__ int64_t centre_index(const T* __restrict__ u) const { return (row - u) - 3 * kNLC; }
-};
+    for (int c = 0; c < 2; ++c)
+      if (sv[b][c] != 0.0f) voxel_rd<FIRST>(u, kb, sy, sz, b, c, sv[b][c], cur, nxt);
+}
+
 
 // The 4 voxels of an interior node row between planes x and x+1 (unguarded sweeps): a pointer
 // that advances by one voxel per plane, 32-bit offsets of the y and z neighbours.
@@ -265,7 +199,7 @@ struct VoxRow {
 // values before the first solve) and y is zero on entry; a row whose neighbour rows lie
 // inside the box then only has nonzero output at x = 1 and x = n0 - 2, and computes only those.
 // MINB: CTAs per SM the register allocation is sized for; FP32 6 (at most 80 registers) or 8 (64),
-// FP64 1 (255) or 3 (168), chosen per batch class by the sweep autotuner
+// FP64 4 (128) or 6 (80), chosen per batch class by the sweep autotuner
 template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 6 : 1)>
 __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restrict__ tiles,
                                                                           const DomDev* __restrict__ doms,
@@ -323,11 +257,13 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
       }
     }
   } else if (yy >= lo && yy <= yhi && zz >= lo && zz <= zhi && x0 <= xe) {
-    Win<T> W;
+    // FP64: voxel-outer slab; ALL rows may lie on the domain box, where only the voxel factors
+    // need guards (out-of-grid voxels read as void)
+    const int sy = D.n[0] * (3 * kNLC), sz = D.n[0] * D.n[1] * (3 * kNLC);
+    int64_t kx = vec_index(node_index(D, x0 - 1, yy, zz), 0, lc);   // plane x0 - 1 of the row
     VoxRow V;
     float sv[2][2];
-    T cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
-    W.template start<ALL>(u, D, x0 - 1, yy, zz, lc);
+    double cur[3] = {0, 0, 0}, nxt[3] = {0, 0, 0};
     if constexpr (ALL) {
       load_voxels<true>(sv, svox, D, x0 - 1, yy, zz);
     } else {
@@ -335,10 +271,10 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
       V.load(sv);
     }
     bool anyp = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
-    W.template apply<true>(sv, cur, nxt);
+    row_slab_d<true>(u, kx, sy, sz, sv, cur, nxt);
 #pragma unroll 1
     for (int x = x0; x <= xe; ++x) {
-      W.template advance<ALL>(u, D, x + 1, yy, zz, lc);
+      kx += 3 * kNLC;   // plane x
       if constexpr (ALL) {
         load_voxels<true>(sv, svox, D, x, yy, zz);
       } else {
@@ -347,15 +283,14 @@ __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restric
       }
       const bool anyc = (sv[0][0] != 0.f) | (sv[0][1] != 0.f) | (sv[1][0] != 0.f) | (sv[1][1] != 0.f);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = T(0); }
-      W.template apply<false>(sv, cur, nxt);
+      for (int c = 0; c < 3; ++c) { cur[c] = nxt[c]; nxt[c] = 0.0; }
+      row_slab_d<false>(u, kx, sy, sz, sv, cur, nxt);
       if (anyp | anyc) {
-        const int64_t b = ALL ? vec_index(node_index(D, x, yy, zz), 0, lc) : W.centre_index(u);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const T v = (T)(scale * D.scale * (double)cur[c]);
-          y[b + c * kNLC] = v;
-          if (DOT) dot += (double)W.centre(c) * (double)v;
+          const double v = scale * D.scale * cur[c];
+          y[kx + c * kNLC] = v;
+          if (DOT) dot += __ldg(u + kx + c * kNLC) * v;
         }
       }
       anyp = anyc;
@@ -1172,7 +1107,7 @@ struct Work {
   const float* ke20tc;  // HEX20 FP32 applications on tcgen05: split matrix in the B layout, else null
   int* err;             // mbarrier time-out flag of the tensor-core kernels
   int minb32 = 6;       // HEX08 slab sweeps: CTAs per SM of the FP32 CG application (6 or 8)
-  int minb64 = 1;       //                    and of every FP64 application (1 or 3)
+  int minb64 = 4;       //                    and of every FP64 application (4 or 6)
   const Tile* tw = nullptr;   // interior sweep tiles (rows of kSweepX nodes) of the slab sweeps
   int64_t ntw = 0;
 };
@@ -1192,8 +1127,8 @@ void apply_k(const Work& W, const DomDev* dd, const float* svox, const uint8_t* 
       if (W.minb32 == 8) k_matvec<T, ALL, DOT, 8><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
       else k_matvec<T, ALL, DOT, 6><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
     } else {
-      if (W.minb64 == 3) k_matvec<T, ALL, DOT, 3><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
-      else k_matvec<T, ALL, DOT, 1><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
+      if (W.minb64 == 6) k_matvec<T, ALL, DOT, 6><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
+      else k_matvec<T, ALL, DOT, 4><<<g, kThreads, 0, s>>>(tl, dd, svox, u, y, scale, acc, act, bnd_only, xl);
     }
   } else {
     const T* ke;
@@ -2166,7 +2101,7 @@ int autotune_sweep(DeviceSolver::Impl& I, SolverStats& st, Work& W, MgDev& M, co
 }
 
 // The register budget of the HEX08 FP64 slab sweep (outer residual, reactions, plain FP64 CG):
-// 1 CTA per SM (255 registers) or 3 (168), timed on the batch's interior tiles (X -> R64, which
+// 4 CTAs per SM (128 registers) or 6 (80), timed on the batch's interior tiles (X -> R64, which
 // the solve overwrites next), cached per class like the FP32 choice.
 struct Tune64 { int minb; float ms[2]; };
 std::map<TuneKey, Tune64> g_tune64;
@@ -2174,7 +2109,7 @@ std::map<TuneKey, Tune64> g_tune64;
 int autotune_fp64(DeviceSolver::Impl& I, SolverStats& st, Work& W, const std::vector<DomDev>& doms,
                   const std::vector<float>& svox, const double* X, double* R64, std::string& msg) {
   const TuneKey key = tune_key(I.device, 8, doms, svox);
-  Tune64 r{1, {0.f, 0.f}};
+  Tune64 r{4, {0.f, 0.f}};
   bool cached = false;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -2184,14 +2119,14 @@ int autotune_fp64(DeviceSolver::Impl& I, SolverStats& st, Work& W, const std::ve
   if (!cached && W.nti > 0) {
     for (int v = 0; v < 2; ++v) {
       Work Wv = W;
-      Wv.minb64 = v == 0 ? 1 : 3;
+      Wv.minb64 = v == 0 ? 4 : 6;
       auto launch = [&]() {
         apply_k<double, 8, false, false>(Wv, B<DomDev>(I, bDoms), I.svox(), B<uint8_t>(I, bFlags), X, R64,
                                          -1.0, nullptr, nullptr, I.stream);
       };
       if (int e = time_launches(I.stream, launch, r.ms[v], msg)) return e;
     }
-    r.minb = r.ms[1] < r.ms[0] ? 3 : 1;
+    r.minb = r.ms[1] < r.ms[0] ? 6 : 4;
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune64[key] = r;
   }
@@ -2386,8 +2321,8 @@ int solve_nen(DeviceSolver::Impl& I, SolverStats& stats_, std::vector<DomainTask
                                              "rotation_search_f64", "autotune_simt_sweep", "autotune_tc_sweep",
                                              "autotune_res_sweep_6cta", "autotune_res_sweep_8cta",
                                              "autotune_post_sweep_8cta", "autotune_apply_sweep_6cta",
-                                             "autotune_apply_sweep_8cta", "autotune_f64_sweep_1cta",
-                                             "autotune_f64_sweep_3cta", "host_pack", "host_multigrid_build"};
+                                             "autotune_apply_sweep_8cta", "autotune_f64_sweep_4cta",
+                                             "autotune_f64_sweep_6cta", "host_pack", "host_multigrid_build"};
   for (int c = 0; c < kcNumClasses; ++c) stats_.kc[c].name = kNames[c];
   I.stats = &stats_;
   I.profile = opt.profile_kernels != 0;
