@@ -174,8 +174,8 @@ __device__ __forceinline__ void row_slab_d(const double* __restrict__ u, int64_t
 }
 
 
-// The 4 voxels of an interior node row between planes x and x+1 (unguarded sweeps): a pointer
-// that advances by one voxel per plane, 32-bit offsets of the y and z neighbours.
+// The 4 voxels of an interior node row between planes x and x+1 (the sweeps over interior
+// rows): a pointer that advances by one voxel per plane, 32-bit offsets of the y and z neighbours.
 struct VoxRow {
   const float* p;
   int sy, sz;
@@ -194,13 +194,14 @@ struct VoxRow {
 
 // y = scale * K u on the tile's nodes.  ALL = false: interior nodes only (inputs are
 // in-bounds without guards), optional dot accumulation acc[col] += u.y.  ALL = true: every
-// node of the grid (reaction forces).  xlen: nodes per row of the tile list (kTileX or
+// node of the grid (reaction forces; only the voxel factors need guards, since a voxel inside the
+// grid has all its corners inside it).  FP32 rows use voxel_rp, FP64 rows voxel_rd.  xlen: nodes per row of the tile list (kTileX or
 // kSweepX).  bnd_only: u vanishes off the domain box (the boundary
 // values before the first solve) and y is zero on entry; a row whose neighbour rows lie
 // inside the box then only has nonzero output at x = 1 and x = n0 - 2, and computes only those.
 // MINB: CTAs per SM the register allocation is sized for; FP32 6 (at most 80 registers) or 8 (64),
 // FP64 4 (128) or 6 (80), chosen per batch class by the sweep autotuner
-template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 6 : 1)>
+template <typename T, bool ALL, bool DOT, int MINB = (sizeof(T) == 4 ? 6 : 4)>
 __global__ void __launch_bounds__(kThreads, MINB) k_matvec(const Tile* __restrict__ tiles,
                                                                           const DomDev* __restrict__ doms,
                                                      const float* __restrict__ svox, const T* __restrict__ u,
